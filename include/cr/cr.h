@@ -1,0 +1,337 @@
+/*
+ * cr.h — C ABI of the B200 point-cloud compute rasteriser.
+ *
+ * This header is the drop-in boundary for the batch-oriented point-cloud
+ * rasteriser of Satin-ComputeRasteriser.  It replaces the Swift/Metal plugin
+ * surface of that package:
+ *
+ *   reference (Swift / Metal)                          C ABI here
+ *   -----------------------------------------------    ---------------------------
+ *   ComputeRasteriserTypes.h:11-63 (shared structs)    cr_raster_batch, cr_raster_file,
+ *                                                      cr_raster_pixel, cr_visible_batch,
+ *                                                      cr_dispatch_args
+ *   ComputeRasteriserTypes.swift:26-142 (config)        cr_config
+ *   ComputeRasteriserPointCloud.swift:23-40 (capacity)  cr_capacity
+ *   ComputeRasteriserPointCloud.swift:202-547 (pool)    cr_cloud_*
+ *   ComputeRasteriser.swift:201-296 (update/encode)     cr_cloud_update_files, cr_render
+ *   ComputeRasteriser.swift:766-838 (per-size buffers)  cr_frame_*
+ *   ComputeRasteriser.swift:609-670 (pickPointIndex)    cr_pick
+ *   GPUPacker.swift:140-392 (pack / packChunk)          cr_pack
+ *
+ * Conventions
+ *   - Every entry point returns a cr_status; CR_OK is 0.  The thread-local
+ *     detail of the last failure is available from cr_last_error_detail().
+ *   - Sizes are element counts unless a name says bytes.
+ *   - Host pointers are borrowed for the duration of the call only.
+ *   - Device memory is owned by the library (context, cloud, frame objects).
+ *   - Each context owns one CUDA stream; every call that launches work
+ *     enqueues it on that stream.  Read-back calls synchronise the stream.
+ *   - Calls on one context (and the objects created from it) are not
+ *     re-entrant: serialise them on the host, as the reference serialises
+ *     its render loop on one thread.
+ *   - Matrices are column-major float[16] (m[col*4 + row]), the simd_float4x4
+ *     layout the reference passes to its shaders.
+ */
+#ifndef CR_CR_H
+#define CR_CR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define CR_API __declspec(dllexport)
+#else
+#define CR_API __attribute__((visibility("default")))
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Constants (ComputeRasteriserTypes.h:4-9, ComputeRasteriserTypes.swift:4-6) */
+/* ------------------------------------------------------------------------ */
+#define CR_THREADS_PER_GROUP 128
+#define CR_DEFAULT_POINTS_PER_BATCH (CR_THREADS_PER_GROUP * 80) /* 10240 */
+#define CR_MASK_10BIT 1023u
+#define CR_MAX_DEPTH 0xffffffffu
+#define CR_INVALID_INDEX 0xffffffffu
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum cr_status {
+    CR_OK = 0,
+    CR_ERR_INVALID_ARGUMENT = 1, /* null handle, bad size, bad enum          */
+    CR_ERR_OUT_OF_MEMORY = 2,    /* device or pinned allocation failed      */
+    CR_ERR_CUDA = 3,             /* a CUDA runtime call failed               */
+    CR_ERR_UNSUPPORTED = 4,      /* feature flag outside the hot path is set */
+    CR_ERR_CAPACITY = 5,         /* slot pool or fixed buffer too small      */
+    CR_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up       */
+    CR_ERR_NO_DEVICE = 7,        /* no CUDA device / library not usable      */
+    CR_ERR_INTERNAL = 8
+} cr_status;
+
+/* ------------------------------------------------------------------------ */
+/* Shared GPU structs, byte-identical to ComputeRasteriserTypes.h:11-63.     */
+/* ------------------------------------------------------------------------ */
+
+/* RasterBatch (ComputeRasteriserTypes.h:11-33): one slot of the pool.
+ * lodCum01..67 hold eight cumulative uint16 LOD counts, two per word (low
+ * level in the low half).  lodCum67 == 0 marks a legacy (unbucketed) batch. */
+typedef struct cr_raster_batch {
+    int32_t state; /* 0 = slot not resident */
+    float minX, minY, minZ;
+    float maxX, maxY, maxZ;
+    uint32_t numPoints;
+    uint32_t firstPoint;
+    uint32_t fileIndex;
+    uint32_t lodCum01, lodCum23, lodCum45, lodCum67;
+    uint32_t padding7, padding8;
+} cr_raster_batch;
+
+/* RasterFile (ComputeRasteriserTypes.h:35-40): per-file transforms. */
+typedef struct cr_raster_file {
+    float transform[16];        /* viewProjection * world              */
+    float transformFrustum[16]; /* frustum matrix * world              */
+    float world[16];            /* model * file world                  */
+    float prevTransform[16];    /* previous frame's viewProjection*world */
+} cr_raster_file;
+
+/* RasterPixel (ComputeRasteriserTypes.h:42-50): the HQS accumulator of one
+ * pixel as the reference lays it out.  Frames store the same quantities as
+ * structure-of-arrays planes; cr_frame_read_pixels re-interleaves them. */
+typedef struct cr_raster_pixel {
+    uint32_t depth;
+    uint32_t red, green, blue, count;
+    uint32_t weight;
+    uint32_t padding[2];
+} cr_raster_pixel;
+
+/* VisibleBatch (ComputeRasteriserTypes.h:52-57): one cull survivor. */
+typedef struct cr_visible_batch {
+    uint32_t batchIndex;
+    int32_t level;
+    float lodThreshold;
+    uint32_t activePoints;
+} cr_visible_batch;
+
+/* CRDispatchArgs (ComputeRasteriserTypes.h:59-63). */
+typedef struct cr_dispatch_args {
+    uint32_t threadgroupsX, threadgroupsY, threadgroupsZ;
+} cr_dispatch_args;
+
+/* ------------------------------------------------------------------------ */
+/* Configuration (ComputeRasteriserConfiguration, ComputeRasteriserTypes.swift:26-142) */
+/* ------------------------------------------------------------------------ */
+typedef enum cr_mode {
+    CR_MODE_HIGH_QUALITY_AVERAGE = 0, /* .highQualityAverage */
+    CR_MODE_NEAREST_POINT = 1         /* .nearestPoint        */
+} cr_mode;
+
+typedef enum cr_point_size_mode {
+    CR_POINT_SIZE_SCREEN_SPACE = 0,
+    CR_POINT_SIZE_WORLD_SPACE = 1
+} cr_point_size_mode;
+
+/* Field names and defaults follow ComputeRasteriserConfiguration.init
+ * (ComputeRasteriserTypes.swift:97-119); booleans are int32 0/1.
+ * applyDisplacement, applyTint, tintAlphaIsCoverage and motionBlur > 0 are
+ * user-programmable effects outside this library; cr_render returns
+ * CR_ERR_UNSUPPORTED when any of them is set. */
+typedef struct cr_config {
+    int32_t mode;              /* cr_mode,             default HQS  */
+    float depthTolerance;      /* default 0.01                      */
+    float backgroundColor[4];  /* default (0,0,0,0)                 */
+    int32_t enableFrustumCulling; /* default 1                      */
+    int32_t lodBias;           /* default 0                         */
+    int32_t enableCLOD;        /* default 1                         */
+    int32_t enableLODDither;   /* default 1                         */
+    int32_t holeFillIterations; /* default 0                        */
+    int32_t colorizeChunks;    /* default 0                         */
+    int32_t colorizeOverdraw;  /* default 0                         */
+    int32_t pointSizeMode;     /* cr_point_size_mode, default screen */
+    float minimumPointSize;    /* default 1                         */
+    float maximumPointSize;    /* default 1                         */
+    float pointSizeScale;      /* default 1                         */
+    int32_t applyDisplacement; /* default 0 (unsupported if set)    */
+    int32_t applyTint;         /* default 0 (unsupported if set)    */
+    int32_t tintAlphaIsCoverage; /* default 0 (unsupported if set)  */
+    int32_t writesSceneDepth;  /* default 1 (composite only)        */
+    float motionBlur;          /* default 0 (unsupported if > 0)    */
+    int32_t motionBlurSamples; /* default 8                         */
+    float motionBlurMaxSpread; /* default 64                        */
+} cr_config;
+
+/* Camera as the reference's processors receive it: Satin
+ * camera.viewMatrix and camera.projectionMatrix (ComputeRasteriser.swift:208-213). */
+typedef struct cr_camera {
+    float view[16];
+    float projection[16];
+} cr_camera;
+
+/* ComputeRasteriserCapacity (ComputeRasteriserPointCloud.swift:23-40). */
+typedef struct cr_capacity {
+    uint32_t maxResidentBatches;
+    uint32_t pointsPerBatch;
+} cr_capacity;
+
+typedef struct cr_cloud_info {
+    cr_capacity capacity;
+    uint32_t residentBatchCount; /* slots with state != 0          */
+    uint64_t pointCount;         /* sum of resident numPoints      */
+    uint32_t freeSlotCount;
+    uint32_t fileCount;
+} cr_cloud_info;
+
+typedef struct cr_context cr_context;
+typedef struct cr_cloud cr_cloud;
+typedef struct cr_frame cr_frame;
+
+/* ------------------------------------------------------------------------ */
+/* Errors and versions                                                       */
+/* ------------------------------------------------------------------------ */
+CR_API const char *cr_status_string(cr_status status);
+/* Detail of the last failure on the calling thread ("" if none). */
+CR_API const char *cr_last_error_detail(void);
+/* Layout self-description, for bindings that mirror the structs:
+ * sizes[0..4] = sizeof batch, file, pixel, visible, dispatch args. */
+CR_API cr_status cr_layout_sizes(uint32_t sizes[5]);
+/* ComputeRasteriserConfiguration() defaults. */
+CR_API cr_status cr_config_default(cr_config *out);
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------ */
+CR_API cr_status cr_context_create(int device, cr_context **out);
+CR_API cr_status cr_context_destroy(cr_context *ctx);
+/* Wait for all work queued on the context's stream. */
+CR_API cr_status cr_context_synchronize(cr_context *ctx);
+/* The context's cudaStream_t, as an opaque pointer. */
+CR_API cr_status cr_context_stream(cr_context *ctx, void **stream_out);
+
+/* ------------------------------------------------------------------------ */
+/* Point cloud slot pool (ComputeRasteriserPointCloud)                       */
+/* ------------------------------------------------------------------------ */
+/* init(context:capacity:files:originShift:label:)  — ComputeRasteriserPointCloud.swift:202-218.
+ * files may be NULL with nfiles == 0, which installs one identity RasterFile. */
+CR_API cr_status cr_cloud_create(cr_context *ctx, cr_capacity capacity,
+                                 const cr_raster_file *files, uint32_t nfiles,
+                                 cr_cloud **out);
+CR_API cr_status cr_cloud_destroy(cr_cloud *cloud);
+/* reallocate(to:files:) — ComputeRasteriserPointCloud.swift:519-530: new
+ * capacity, all slots empty. */
+CR_API cr_status cr_cloud_reallocate(cr_cloud *cloud, cr_capacity capacity,
+                                     const cr_raster_file *files, uint32_t nfiles);
+/* Replace the file table without touching slots (replacePackedPointCloud's
+ * fitting branch, ComputeRasteriserPointCloud.swift:256-259). */
+CR_API cr_status cr_cloud_set_files(cr_cloud *cloud, const cr_raster_file *files,
+                                    uint32_t nfiles);
+/* addBatches(...) — ComputeRasteriserPointCloud.swift:410-452.  Each input
+ * batch names a run [firstPoint, firstPoint+numPoints) of the host arrays;
+ * it is copied into a free slot (LIFO free list), its firstPoint rebased to
+ * slot*pointsPerBatch and its state set to 1.  slots_out (n entries) receives
+ * the chosen slot of each batch.  points_len is the element count of every
+ * host array (bounds check).  CR_ERR_CAPACITY if fewer than n slots are free
+ * or a batch exceeds pointsPerBatch. */
+CR_API cr_status cr_cloud_add_batches(cr_cloud *cloud,
+                                      const uint32_t *xyz_low, const uint32_t *xyz_med,
+                                      const uint32_t *xyz_high, const uint32_t *colors,
+                                      const uint8_t *levels, uint64_t points_len,
+                                      const cr_raster_batch *batches, uint32_t n,
+                                      int commit, int32_t *slots_out);
+/* removeBatches(slots:commit:) — ComputeRasteriserPointCloud.swift:460-473. */
+CR_API cr_status cr_cloud_remove_batches(cr_cloud *cloud, const int32_t *slots, uint32_t n,
+                                         int commit);
+/* commitBatchUpdates() — ComputeRasteriserPointCloud.swift:481-483 (uploads
+ * the dirty slot range of the host batch mirror). */
+CR_API cr_status cr_cloud_commit(cr_cloud *cloud);
+/* clearAllBatches() — ComputeRasteriserPointCloud.swift:367-377. */
+CR_API cr_status cr_cloud_clear(cr_cloud *cloud);
+/* updateFiles(viewProjection:modelMatrix:frustumTransform:prevViewProjection:)
+ * — ComputeRasteriserPointCloud.swift:487-515.  frustum and prev_vp may be NULL. */
+CR_API cr_status cr_cloud_update_files(cr_cloud *cloud, const float vp[16],
+                                       const float model[16], const float *frustum,
+                                       const float *prev_vp);
+CR_API cr_status cr_cloud_info_get(const cr_cloud *cloud, cr_cloud_info *out);
+/* Host mirror of the file table as last written by cr_cloud_update_files. */
+CR_API cr_status cr_cloud_read_files(const cr_cloud *cloud, cr_raster_file *out, uint32_t n);
+/* Device batch table, slots [first, first+n). */
+CR_API cr_status cr_cloud_read_batches(cr_cloud *cloud, cr_raster_batch *out, uint32_t first,
+                                       uint32_t n);
+/* Device point arrays, points [first, first+n); any output may be NULL. */
+CR_API cr_status cr_cloud_read_points(cr_cloud *cloud, uint64_t first, uint64_t n,
+                                      uint32_t *xyz_low, uint32_t *xyz_med, uint32_t *xyz_high,
+                                      uint32_t *colors, uint8_t *levels);
+/* Cull output of the last frame that rendered this cloud (cloud.visibleBatchesBuffer):
+ * count_out receives the survivor count; up to cap records are copied. */
+CR_API cr_status cr_cloud_read_visible(cr_cloud *cloud, cr_visible_batch *out, uint32_t cap,
+                                       uint32_t *count_out);
+
+/* ------------------------------------------------------------------------ */
+/* Frames: per-viewport device resources (ComputeRasteriser.swift:766-838)   */
+/* ------------------------------------------------------------------------ */
+CR_API cr_status cr_frame_create(cr_context *ctx, int width, int height, cr_frame **out);
+CR_API cr_status cr_frame_destroy(cr_frame *frame);
+
+/* One frame: ComputeRasteriser.update + encode (ComputeRasteriser.swift:201-296).
+ * Uses each cloud's file table as last set by cr_cloud_update_files.
+ *   HQS:     clear -> [cull] -> [depth] -> [colour] over all clouds, phase-major
+ *            -> resolve -> hole fill (ComputeRasteriser.swift:322-456, 298-320)
+ *   nearest: first cloud with resident batches only: clear winner -> cull ->
+ *            nearest depth/index -> nearest resolve -> hole fill
+ *            (ComputeRasteriser.swift:483-522) */
+CR_API cr_status cr_render(cr_context *ctx, cr_frame *frame, cr_cloud *const *clouds,
+                           uint32_t nclouds, const cr_config *config, const cr_camera *camera);
+
+/* Read-backs (synchronise the context stream). */
+CR_API cr_status cr_frame_read_rgba8(cr_frame *frame, uint8_t *out /* w*h*4 */);
+CR_API cr_status cr_frame_read_depth_f32(cr_frame *frame, float *out /* w*h */);
+CR_API cr_status cr_frame_read_pixels(cr_frame *frame, cr_raster_pixel *out /* w*h */);
+CR_API cr_status cr_frame_read_nearest_depth(cr_frame *frame, uint32_t *out /* w*h */);
+CR_API cr_status cr_frame_read_nearest_index(cr_frame *frame, uint32_t *out /* w*h */);
+/* Rows [row0, row0+nrows) of the nearest index plane (pick band read-back). */
+CR_API cr_status cr_frame_read_nearest_index_rows(cr_frame *frame, int row0, int nrows,
+                                                  uint32_t *out);
+
+/* pickPointIndex(atNDC:in:camera:searchRadius:) — ComputeRasteriser.swift:609-670.
+ * Runs cull + nearest depth/index for one cloud into the frame's nearest
+ * planes, reads back the band of rows within search_radius of the pixel
+ * under ndc (y up) and returns the nearest non-sentinel pixel's point index.
+ * found_out = 0 when nothing lies within the radius. */
+CR_API cr_status cr_pick(cr_context *ctx, cr_frame *frame, cr_cloud *cloud, const float ndc[2],
+                         const cr_config *config, const cr_camera *camera, int search_radius,
+                         uint32_t *index_out, int *found_out);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+/* Layout checks mirroring LayoutTests.swift:5-26. */
+#ifdef __cplusplus
+static_assert(sizeof(cr_raster_batch) == 64, "RasterBatch stride");
+static_assert(offsetof(cr_raster_batch, state) == 0, "RasterBatch.state");
+static_assert(offsetof(cr_raster_batch, minX) == 4, "RasterBatch.minX");
+static_assert(offsetof(cr_raster_batch, maxZ) == 24, "RasterBatch.maxZ");
+static_assert(offsetof(cr_raster_batch, numPoints) == 28, "RasterBatch.numPoints");
+static_assert(offsetof(cr_raster_batch, firstPoint) == 32, "RasterBatch.firstPoint");
+static_assert(offsetof(cr_raster_batch, fileIndex) == 36, "RasterBatch.fileIndex");
+static_assert(sizeof(cr_raster_file) == 256, "RasterFile stride");
+static_assert(sizeof(cr_raster_pixel) == 32, "RasterPixel stride");
+static_assert(sizeof(cr_visible_batch) == 16, "VisibleBatch stride");
+static_assert(sizeof(cr_dispatch_args) == 12, "CRDispatchArgs stride");
+#else
+_Static_assert(sizeof(cr_raster_batch) == 64, "RasterBatch stride");
+_Static_assert(offsetof(cr_raster_batch, state) == 0, "RasterBatch.state");
+_Static_assert(offsetof(cr_raster_batch, minX) == 4, "RasterBatch.minX");
+_Static_assert(offsetof(cr_raster_batch, maxZ) == 24, "RasterBatch.maxZ");
+_Static_assert(offsetof(cr_raster_batch, numPoints) == 28, "RasterBatch.numPoints");
+_Static_assert(offsetof(cr_raster_batch, firstPoint) == 32, "RasterBatch.firstPoint");
+_Static_assert(offsetof(cr_raster_batch, fileIndex) == 36, "RasterBatch.fileIndex");
+_Static_assert(sizeof(cr_raster_file) == 256, "RasterFile stride");
+_Static_assert(sizeof(cr_raster_pixel) == 32, "RasterPixel stride");
+_Static_assert(sizeof(cr_visible_batch) == 16, "VisibleBatch stride");
+_Static_assert(sizeof(cr_dispatch_args) == 12, "CRDispatchArgs stride");
+#endif
+
+#endif /* CR_CR_H */
