@@ -280,6 +280,7 @@ bool cull_one(const orc_cloud &c, uint32_t gid, const orc_config &cfg, const flo
         const uint32_t words[4] = {b.lodCum01, b.lodCum23, b.lodCum45, b.lodCum67};
         const uint32_t word = words[lmax >> 1];
         active = (lmax & 1) ? (word >> 16) : (word & 0xffffu);
+        active = std::min(active, b.numPoints);  // malformed counts stay inside the slot
     }
     if (active == 0u) return false;
     out.batchIndex = gid;

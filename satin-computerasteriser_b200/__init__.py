@@ -1,0 +1,559 @@
+"""B200 point-cloud compute rasteriser — host mirror of Satin-ComputeRasteriser's API.
+
+The classes here mirror the reference's Swift surface for the render path
+(same names, argument meaning and error behaviour) on top of the C ABI in
+``include/cr/cr.h``:
+
+  ComputeRasteriserConfiguration  ComputeRasteriserTypes.swift:26-142
+  ComputeRasteriserCapacity       ComputeRasteriserPointCloud.swift:23-40
+  ComputeRasteriserPointCloud     ComputeRasteriserPointCloud.swift:59-678
+  ComputeRasteriser               ComputeRasteriser.swift:5-888
+  PackedPointCloud                ComputeRasteriserTypes.swift:269-320
+
+Swift preconditions become ``CRError`` exceptions.  All GPU work runs in
+``_lib/libsatincr.so`` (CUDA, sm_100a); nothing here computes pixels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field, fields
+
+import numpy as np
+
+from . import _native as N
+from ._native import (BATCH_DTYPE, FILE_DTYPE, PIXEL_DTYPE, VISIBLE_DTYPE, CRError)
+
+__all__ = ["Context", "ComputeRasteriserConfiguration", "ComputeRasteriserCapacity",
+           "ComputeRasteriserPointCloud", "ComputeRasteriser", "PackedPointCloud",
+           "PerspectiveCamera", "CRError", "BATCH_DTYPE", "FILE_DTYPE", "PIXEL_DTYPE",
+           "VISIBLE_DTYPE", "computeRasteriserThreadsPerGroup", "MODE_HQS", "MODE_NEAREST",
+           "identity_files", "matrix_multiply"]
+
+computeRasteriserThreadsPerGroup = 128
+MODE_HQS = 0      # ComputeRasteriserMode.highQualityAverage
+MODE_NEAREST = 1  # ComputeRasteriserMode.nearestPoint
+SCREEN_SPACE = 0  # PointSizeMode.screenSpace
+WORLD_SPACE = 1   # PointSizeMode.worldSpace
+
+
+def _mat16(m) -> np.ndarray:
+    """A 4x4 matrix as the column-major float[16] the ABI takes.
+
+    Accepts a flat 16-vector (already column-major) or a 4x4 array in
+    row-major math notation (m[row][col]), which is transposed."""
+    a = np.asarray(m, dtype=np.float32)
+    if a.shape == (4, 4):
+        a = a.T
+    return np.ascontiguousarray(a.reshape(16))
+
+
+def matrix_multiply(a, b) -> np.ndarray:
+    """a * b for column-major float[16] matrices with the library's fixed
+    operation order (rows summed k = 0..3 left to right, no FMA)."""
+    a, b = _mat16(a), _mat16(b)
+    out = np.zeros(16, np.float32)
+    for c in range(4):
+        for r in range(4):
+            s = np.float32(a[r] * b[c * 4 + 0]) + np.float32(a[4 + r] * b[c * 4 + 1])
+            s = np.float32(s) + np.float32(a[8 + r] * b[c * 4 + 2])
+            s = np.float32(s) + np.float32(a[12 + r] * b[c * 4 + 3])
+            out[c * 4 + r] = s
+    return out
+
+
+def identity_files(n: int = 1) -> np.ndarray:
+    """RasterFile() defaults (ComputeRasteriserTypes.swift:235-244): identity matrices."""
+    f = np.zeros(n, FILE_DTYPE)
+    eye = np.eye(4, dtype=np.float32).reshape(16)
+    for k in FILE_DTYPE.names:
+        f[k][:] = eye
+    return f
+
+
+class Context:
+    """Device + stream (the role of Satin's Context / MTLCommandQueue)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        N.check(N.lib().cr_context_create(device, C.byref(self._h)))
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def synchronize(self):
+        N.check(N.lib().cr_context_synchronize(self._h))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        N.check(N.lib().cr_context_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def close(self):
+        if self._h:
+            N.lib().cr_context_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class ComputeRasteriserConfiguration:
+    """ComputeRasteriserConfiguration (ComputeRasteriserTypes.swift:26-142), same defaults."""
+    mode: int = MODE_HQS
+    depthTolerance: float = 0.01
+    backgroundColor: tuple = (0.0, 0.0, 0.0, 0.0)
+    enableFrustumCulling: bool = True
+    lodBias: int = 0
+    enableCLOD: bool = True
+    enableLODDither: bool = True
+    holeFillIterations: int = 0
+    colorizeChunks: bool = False
+    colorizeOverdraw: bool = False
+    pointSizeMode: int = SCREEN_SPACE
+    minimumPointSize: float = 1.0
+    maximumPointSize: float = 1.0
+    pointSizeScale: float = 1.0
+    applyDisplacement: bool = False
+    applyTint: bool = False
+    tintAlphaIsCoverage: bool = False
+    writesSceneDepth: bool = True
+    motionBlur: float = 0.0
+    motionBlurSamples: int = 8
+    motionBlurMaxSpread: float = 64.0
+
+    def to_c(self) -> N.cr_config:
+        c = N.cr_config()
+        for f in fields(self):
+            v = getattr(self, f.name)
+            if f.name == "backgroundColor":
+                c.backgroundColor[:] = [float(x) for x in v]
+            elif isinstance(getattr(c, f.name), float):
+                setattr(c, f.name, float(v))
+            else:
+                setattr(c, f.name, int(v))
+        return c
+
+
+@dataclass(frozen=True)
+class ComputeRasteriserCapacity:
+    """ComputeRasteriserCapacity (ComputeRasteriserPointCloud.swift:23-40)."""
+    maxResidentBatches: int
+    pointsPerBatch: int = computeRasteriserThreadsPerGroup * 80
+
+    def __post_init__(self):
+        if self.maxResidentBatches <= 0:
+            raise CRError(1, "maxResidentBatches must be positive")
+        if self.pointsPerBatch <= 0:
+            raise CRError(1, "pointsPerBatch must be positive")
+
+    @property
+    def maxResidentPoints(self) -> int:
+        return self.maxResidentBatches * self.pointsPerBatch
+
+    def to_c(self) -> N.cr_capacity:
+        return N.cr_capacity(self.maxResidentBatches, self.pointsPerBatch)
+
+
+@dataclass
+class PackedPointCloud:
+    """PackedPointCloud (ComputeRasteriserTypes.swift:269-320) as numpy arrays."""
+    batches: np.ndarray
+    files: np.ndarray
+    xyzLow: np.ndarray
+    xyzMed: np.ndarray
+    xyzHigh: np.ndarray
+    colors: np.ndarray
+    levels: np.ndarray
+    boundsMin: np.ndarray = field(default_factory=lambda: np.zeros(3, np.float32))
+    boundsMax: np.ndarray = field(default_factory=lambda: np.zeros(3, np.float32))
+    orderedPositions: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float32))
+    sourceIndices: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
+
+    @property
+    def pointCount(self) -> int:
+        return len(self.colors)
+
+    @property
+    def batchCount(self) -> int:
+        return len(self.batches)
+
+
+class ComputeRasteriserPointCloud:
+    """ComputeRasteriserPointCloud (ComputeRasteriserPointCloud.swift:59-678).
+
+    A fixed-size slot pool on the device: per-point xyzLow/Med/High, colours
+    and levels, one RasterBatch per slot, and the per-file transform table.
+    """
+
+    def __init__(self, context: Context, capacity: ComputeRasteriserCapacity | None = None,
+                 files=None, packed: PackedPointCloud | None = None,
+                 label: str = "ComputeRasteriserPointCloud"):
+        self.context = context
+        self.label = label
+        self.visible = True
+        self.worldMatrix = np.eye(4, dtype=np.float32).reshape(16)
+        if packed is not None and capacity is None:
+            # Convenience init (ComputeRasteriserPointCloud.swift:222-236).
+            ppb = int(packed.batches["numPoints"].max()) if packed.batchCount else \
+                computeRasteriserThreadsPerGroup * 80
+            capacity = ComputeRasteriserCapacity(max(1, packed.batchCount), max(1, ppb))
+            files = packed.files
+        if capacity is None:
+            raise CRError(1, "capacity or packed is required")
+        files = identity_files() if files is None else np.ascontiguousarray(files, FILE_DTYPE)
+        self._h = C.c_void_p()
+        N.check(N.lib().cr_cloud_create(context.handle, capacity.to_c(), N.ptr(files), len(files),
+                                        C.byref(self._h)))
+        self._capacity = capacity
+        if packed is not None and packed.batchCount > 0:
+            self._upload_packed(packed)
+
+    # --- Satin Object transform (position only, enough for the render path) ---
+    @property
+    def position(self):
+        return tuple(self.worldMatrix[12:15])
+
+    @position.setter
+    def position(self, p):
+        m = np.eye(4, dtype=np.float32).reshape(16)
+        m[12:15] = np.asarray(p, np.float32)
+        self.worldMatrix = m
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _info(self) -> N.cr_cloud_info:
+        info = N.cr_cloud_info()
+        N.check(N.lib().cr_cloud_info_get(self._h, C.byref(info)))
+        return info
+
+    @property
+    def capacity(self) -> ComputeRasteriserCapacity:
+        return self._capacity
+
+    @property
+    def batchCount(self) -> int:
+        return self._capacity.maxResidentBatches
+
+    @property
+    def residentBatchCount(self) -> int:
+        return self._info().residentBatchCount
+
+    @property
+    def pointCount(self) -> int:
+        return self._info().pointCount
+
+    @property
+    def freeSlotCount(self) -> int:
+        return self._info().freeSlotCount
+
+    def addBatches(self, positionsXYZLow, positionsXYZMed, positionsXYZHigh, colors, levels,
+                   batches, commit: bool = True) -> list[int]:
+        """addBatches (ComputeRasteriserPointCloud.swift:410-452)."""
+        low = np.ascontiguousarray(positionsXYZLow, np.uint32)
+        med = np.ascontiguousarray(positionsXYZMed, np.uint32)
+        high = np.ascontiguousarray(positionsXYZHigh, np.uint32)
+        col = np.ascontiguousarray(colors, np.uint32)
+        lv = np.ascontiguousarray(levels, np.uint8)
+        b = np.ascontiguousarray(batches, BATCH_DTYPE)
+        n = min(len(low), len(med), len(high), len(col), len(lv))
+        slots = np.zeros(max(len(b), 1), np.int32)
+        N.check(N.lib().cr_cloud_add_batches(self._h, N.ptr(low), N.ptr(med), N.ptr(high),
+                                             N.ptr(col), N.ptr(lv), n, N.ptr(b), len(b),
+                                             int(commit), N.ptr(slots)))
+        return slots[:len(b)].tolist()
+
+    def removeBatches(self, slots, commit: bool = True):
+        """removeBatches (ComputeRasteriserPointCloud.swift:460-473)."""
+        s = np.ascontiguousarray(slots, np.int32)
+        N.check(N.lib().cr_cloud_remove_batches(self._h, N.ptr(s), len(s), int(commit)))
+
+    def commitBatchUpdates(self):
+        N.check(N.lib().cr_cloud_commit(self._h))
+
+    def clearAllBatches(self):
+        N.check(N.lib().cr_cloud_clear(self._h))
+
+    def replacePackedPointCloud(self, packed: PackedPointCloud):
+        """replacePackedPointCloud (ComputeRasteriserPointCloud.swift:246-264)."""
+        needed = max(1, packed.batchCount)
+        ppb = int(packed.batches["numPoints"].max()) if packed.batchCount else \
+            self._capacity.pointsPerBatch
+        files = np.ascontiguousarray(packed.files, FILE_DTYPE)
+        if needed > self._capacity.maxResidentBatches or ppb > self._capacity.pointsPerBatch:
+            cap = ComputeRasteriserCapacity(needed, max(ppb, self._capacity.pointsPerBatch))
+            N.check(N.lib().cr_cloud_reallocate(self._h, cap.to_c(), N.ptr(files), len(files)))
+            self._capacity = cap
+        else:
+            N.check(N.lib().cr_cloud_set_files(self._h, N.ptr(files), len(files)))
+            self.clearAllBatches()
+        if packed.batchCount > 0:
+            self._upload_packed(packed)
+
+    def _upload_packed(self, packed: PackedPointCloud):
+        self.addBatches(packed.xyzLow, packed.xyzMed, packed.xyzHigh, packed.colors,
+                        packed.levels, packed.batches)
+
+    def updateFiles(self, viewProjection, modelMatrix, frustumTransform=None,
+                    prevViewProjection=None):
+        """updateFiles (ComputeRasteriserPointCloud.swift:487-515)."""
+        vp, mm = _mat16(viewProjection), _mat16(modelMatrix)
+        fr = None if frustumTransform is None else _mat16(frustumTransform)
+        pv = None if prevViewProjection is None else _mat16(prevViewProjection)
+        N.check(N.lib().cr_cloud_update_files(self._h, N.ptr(vp), N.ptr(mm), N.ptr(fr),
+                                              N.ptr(pv)))
+
+    # --- read-backs (for tests and tools) ---
+    def files(self) -> np.ndarray:
+        out = np.zeros(self._info().fileCount, FILE_DTYPE)
+        N.check(N.lib().cr_cloud_read_files(self._h, N.ptr(out), len(out)))
+        return out
+
+    def batches(self, first: int = 0, n: int | None = None) -> np.ndarray:
+        n = self.batchCount - first if n is None else n
+        out = np.zeros(max(n, 0), BATCH_DTYPE)
+        N.check(N.lib().cr_cloud_read_batches(self._h, N.ptr(out), first, n))
+        return out
+
+    def points(self, first: int = 0, n: int | None = None) -> dict:
+        n = self._capacity.maxResidentPoints - first if n is None else n
+        out = {k: np.zeros(n, np.uint32) for k in ("xyzLow", "xyzMed", "xyzHigh", "colors")}
+        out["levels"] = np.zeros(n, np.uint8)
+        N.check(N.lib().cr_cloud_read_points(self._h, first, n, N.ptr(out["xyzLow"]),
+                                             N.ptr(out["xyzMed"]), N.ptr(out["xyzHigh"]),
+                                             N.ptr(out["colors"]), N.ptr(out["levels"])))
+        return out
+
+    def visibleBatches(self) -> np.ndarray:
+        out = np.zeros(self.batchCount, VISIBLE_DTYPE)
+        count = C.c_uint32()
+        N.check(N.lib().cr_cloud_read_visible(self._h, N.ptr(out), len(out), C.byref(count)))
+        return out[:count.value].copy()
+
+    def close(self):
+        if self._h:
+            N.lib().cr_cloud_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Frame:
+    def __init__(self, context: Context, width: int, height: int):
+        self.context = context
+        self.width, self.height = width, height
+        self._h = C.c_void_p()
+        N.check(N.lib().cr_frame_create(context.handle, width, height, C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            N.lib().cr_frame_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PerspectiveCamera:
+    """A Satin-style perspective camera: right-handed view (looks down -Z) and
+    a reverse-Z projection for Metal's [0, 1] clip depth (near -> 1, far -> 0)."""
+
+    def __init__(self, position=(0.0, 0.0, 5.0), near: float = 0.1, far: float = 100.0,
+                 fov: float = 45.0, aspect: float = 1.0):
+        self.position = np.asarray(position, np.float64)
+        self.near, self.far, self.fov, self.aspect = near, far, fov, aspect
+        self.target = np.zeros(3)
+        self.up = np.array([0.0, 1.0, 0.0])
+
+    def lookAt(self, target, up=(0.0, 1.0, 0.0)):
+        self.target = np.asarray(target, np.float64)
+        self.up = np.asarray(up, np.float64)
+
+    @property
+    def viewMatrix(self) -> np.ndarray:
+        f = self.target - self.position
+        f = f / np.linalg.norm(f)
+        s = np.cross(f, self.up)
+        s = s / np.linalg.norm(s)
+        u = np.cross(s, f)
+        m = np.eye(4)
+        m[0, :3], m[1, :3], m[2, :3] = s, u, -f
+        m[0, 3], m[1, 3], m[2, 3] = -s @ self.position, -u @ self.position, f @ self.position
+        return _mat16(m)
+
+    @property
+    def projectionMatrix(self) -> np.ndarray:
+        t = 1.0 / math.tan(math.radians(self.fov) * 0.5)
+        n, fa = self.near, self.far
+        m = np.zeros((4, 4))
+        m[0, 0] = t / self.aspect
+        m[1, 1] = t
+        m[2, 2] = n / (fa - n)
+        m[2, 3] = fa * n / (fa - n)
+        m[3, 2] = -1.0
+        return _mat16(m)
+
+
+def _camera_c(camera) -> N.cr_camera:
+    c = N.cr_camera()
+    c.view[:] = _mat16(camera.viewMatrix).tolist()
+    c.projection[:] = _mat16(camera.projectionMatrix).tolist()
+    return c
+
+
+class ComputeRasteriser:
+    """ComputeRasteriser (ComputeRasteriser.swift:5-888): the per-frame render API.
+
+    ``update`` sets the camera and refreshes every visible cloud's file
+    table; ``encode`` enqueues the frame (HQS or nearest, then hole fill).
+    Outputs are device buffers read back with ``outputRGBA8`` and friends.
+    Per-viewport buffers are cached for the four most recent sizes
+    (ComputeRasteriser.swift:43-53, 766-838).
+    """
+    resourceCacheCap = 4
+
+    def __init__(self, context: Context, label: str = "ComputeRasteriser"):
+        self.context = context
+        self.label = label
+        self.configuration = ComputeRasteriserConfiguration()
+        self.visible = True
+        self._clouds: list[ComputeRasteriserPointCloud] = []
+        self._cache: dict[tuple, _Frame] = {}
+        self._lru: list[tuple] = []
+        self._frame: _Frame | None = None
+        self._camera = None
+        self._prev_vp: dict[int, np.ndarray] = {}
+
+    def addPointCloud(self, cloud: ComputeRasteriserPointCloud) -> ComputeRasteriserPointCloud:
+        self._clouds.append(cloud)
+        return cloud
+
+    def removePointCloud(self, cloud: ComputeRasteriserPointCloud):
+        self._clouds = [c for c in self._clouds if c is not cloud]
+
+    @property
+    def pointClouds(self):
+        return list(self._clouds)
+
+    @property
+    def visiblePointClouds(self):
+        return [c for c in self._clouds if c.visible]
+
+    def resize(self, size):
+        w, h = int(size[0]), int(size[1])
+        if w <= 0 or h <= 0:
+            return
+        key = (w, h)
+        frame = self._cache.get(key)
+        if frame is None:
+            while len(self._lru) >= self.resourceCacheCap:
+                old = self._lru.pop(0)
+                self._cache.pop(old).close()
+            frame = _Frame(self.context, w, h)
+            self._cache[key] = frame
+        if key in self._lru:
+            self._lru.remove(key)
+        self._lru.append(key)
+        self._frame = frame
+
+    @property
+    def viewportSize(self):
+        return None if self._frame is None else (self._frame.width, self._frame.height)
+
+    def update(self, camera, viewport=None):
+        """update(renderContext:camera:viewport:index:) (ComputeRasteriser.swift:201-268)."""
+        if not self.visible:
+            return
+        if viewport is not None:
+            w, h = int(viewport[-2]), int(viewport[-1])
+            if self.viewportSize != (w, h):
+                self.resize((w, h))
+        self._camera = camera
+        vp = matrix_multiply(camera.projectionMatrix, camera.viewMatrix)
+        prev = self._prev_vp.get(id(camera), vp)
+        for cloud in self.visiblePointClouds:
+            cloud.updateFiles(vp, cloud.worldMatrix, prevViewProjection=prev)
+        self._prev_vp[id(camera)] = vp
+
+    def encode(self):
+        """encode(_:) (ComputeRasteriser.swift:277-296)."""
+        if not self.visible or self._frame is None or self._camera is None:
+            return
+        clouds = self.visiblePointClouds
+        arr = (C.c_void_p * max(len(clouds), 1))(*[c.handle.value for c in clouds])
+        cfg = self.configuration.to_c()
+        cam = _camera_c(self._camera)
+        N.check(N.lib().cr_render(self.context.handle, self._frame.handle, arr, len(clouds),
+                                  C.byref(cfg), C.byref(cam)))
+
+    # --- outputs (row 0 = top of the viewport) ---
+    def outputRGBA8(self) -> np.ndarray:
+        f = self._require_frame()
+        out = np.zeros((f.height, f.width, 4), np.uint8)
+        N.check(N.lib().cr_frame_read_rgba8(f.handle, N.ptr(out)))
+        return out
+
+    def depthTexture(self) -> np.ndarray:
+        f = self._require_frame()
+        out = np.zeros((f.height, f.width), np.float32)
+        N.check(N.lib().cr_frame_read_depth_f32(f.handle, N.ptr(out)))
+        return out
+
+    def pixels(self) -> np.ndarray:
+        f = self._require_frame()
+        out = np.zeros((f.height, f.width), PIXEL_DTYPE)
+        N.check(N.lib().cr_frame_read_pixels(f.handle, N.ptr(out)))
+        return out
+
+    def nearestDepths(self) -> np.ndarray:
+        f = self._require_frame()
+        out = np.zeros((f.height, f.width), np.uint32)
+        N.check(N.lib().cr_frame_read_nearest_depth(f.handle, N.ptr(out)))
+        return out
+
+    def nearestIndices(self) -> np.ndarray:
+        f = self._require_frame()
+        out = np.zeros((f.height, f.width), np.uint32)
+        N.check(N.lib().cr_frame_read_nearest_index(f.handle, N.ptr(out)))
+        return out
+
+    def pickPointIndex(self, atNDC, cloud: ComputeRasteriserPointCloud, camera,
+                       searchRadius: int = 10):
+        """pickPointIndex(atNDC:in:camera:searchRadius:) (ComputeRasteriser.swift:609-670)."""
+        if self._frame is None or cloud.residentBatchCount == 0:
+            return None
+        vp = matrix_multiply(camera.projectionMatrix, camera.viewMatrix)
+        cloud.updateFiles(vp, cloud.worldMatrix)
+        ndc = np.asarray(atNDC, np.float32)
+        cfg = self.configuration.to_c()
+        cam = _camera_c(camera)
+        idx = C.c_uint32()
+        found = C.c_int()
+        N.check(N.lib().cr_pick(self.context.handle, self._frame.handle, cloud.handle,
+                                N.ptr(ndc), C.byref(cfg), C.byref(cam), int(searchRadius),
+                                C.byref(idx), C.byref(found)))
+        return int(idx.value) if found.value else None
+
+    def _require_frame(self) -> _Frame:
+        if self._frame is None:
+            raise CRError(1, "no viewport: call resize or update first")
+        return self._frame

@@ -1,0 +1,876 @@
+// capi.cpp — the C ABI (include/cr/cr.h): context, slot pool, frames, and
+// the pass sequencing of ComputeRasteriser.encode.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cr_internal.h"
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+namespace cri {
+static thread_local std::string g_detail;
+
+void set_error(const std::string &detail) { g_detail = detail; }
+
+cr_status fail(cr_status st, const std::string &detail) {
+    g_detail = detail;
+    return st;
+}
+
+cr_status cuda_fail(cudaError_t e, const char *what) {
+    g_detail = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    if (e == cudaErrorMemoryAllocation) return CR_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ||
+        e == cudaErrorInvalidDevice)
+        return CR_ERR_NO_DEVICE;
+    return CR_ERR_CUDA;
+}
+}  // namespace cri
+
+using cri::fail;
+
+namespace {
+
+constexpr size_t kPointPad = 64;  // slack past the last slot for 16-byte vector loads
+
+// Host 4x4 product with the library's operation order (no contraction:
+// this file is compiled with -ffp-contract=off).
+void mat4mul(const float *a, const float *b, float *out) {
+    float r[16];
+    for (int c = 0; c < 4; ++c)
+        for (int row = 0; row < 4; ++row)
+            r[c * 4 + row] = ((a[0 * 4 + row] * b[c * 4 + 0] + a[1 * 4 + row] * b[c * 4 + 1]) +
+                              a[2 * 4 + row] * b[c * 4 + 2]) +
+                             a[3 * 4 + row] * b[c * 4 + 3];
+    std::memcpy(out, r, sizeof(r));
+}
+
+cr_raster_file identity_file() {
+    cr_raster_file f;
+    std::memset(&f, 0, sizeof(f));
+    for (int i = 0; i < 4; ++i) {
+        f.transform[i * 5] = 1.0f;
+        f.transformFrustum[i * 5] = 1.0f;
+        f.world[i * 5] = 1.0f;
+        f.prevTransform[i * 5] = 1.0f;
+    }
+    return f;
+}
+
+template <typename T>
+cr_status dalloc(T **p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return cri::cuda_fail(e, "cudaMalloc");
+    }
+    return CR_OK;
+}
+
+template <typename T>
+void dfree(T *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void free_cloud_buffers(cr_cloud *c) {
+    dfree(c->d_low);
+    dfree(c->d_med);
+    dfree(c->d_high);
+    dfree(c->d_colors);
+    dfree(c->d_levels);
+    dfree(c->d_batches);
+    dfree(c->d_files);
+    dfree(c->d_visible);
+    dfree(c->d_cull_tmp);
+    dfree(c->d_cull_cta);
+    dfree(c->d_counters);
+}
+
+void mark_dirty(cr_cloud *c, int64_t lo, int64_t hi) {
+    if (lo < c->dirty_lo) c->dirty_lo = lo;
+    if (hi > c->dirty_hi) c->dirty_hi = hi;
+}
+
+// flushBatchMirror (ComputeRasteriserPointCloud.swift:629-644).
+cr_status flush_mirror(cr_cloud *c) {
+    if (c->dirty_lo > c->dirty_hi) return CR_OK;
+    const int64_t lo = std::max<int64_t>(0, c->dirty_lo);
+    const int64_t hi = std::min<int64_t>(c->dirty_hi, (int64_t)c->mirror.size() - 1);
+    c->dirty_lo = INT64_MAX;
+    c->dirty_hi = -1;
+    if (lo > hi) return CR_OK;
+    CR_CUDA(cudaMemcpyAsync(c->d_batches + lo, c->mirror.data() + lo,
+                            (size_t)(hi - lo + 1) * sizeof(cr_raster_batch),
+                            cudaMemcpyHostToDevice, c->ctx->stream));
+    return CR_OK;
+}
+
+cr_status upload_files(cr_cloud *c, const std::vector<cr_raster_file> &files) {
+    if (files.empty()) return CR_OK;
+    if (files.size() > c->d_files_cap) {
+        dfree(c->d_files);
+        cr_status st = dalloc(&c->d_files, files.size() * sizeof(cr_raster_file));
+        if (st != CR_OK) return st;
+        c->d_files_cap = (uint32_t)files.size();
+    }
+    // Stage through the pinned ring so the copy stays asynchronous and the
+    // host may overwrite the next slot while earlier copies are in flight.
+    const size_t nbytes = files.size() * sizeof(cr_raster_file);
+    if (!c->h_files_ring || nbytes > sizeof(cr_raster_file) * c->d_files_cap) {
+        CR_CUDA(cudaMemcpy(c->d_files, files.data(), nbytes, cudaMemcpyHostToDevice));
+        return CR_OK;
+    }
+    c->ring_slot = (c->ring_slot + 1) % cr_cloud::kFileRing;
+    const int s = c->ring_slot;
+    if (c->ring_used[s]) CR_CUDA(cudaEventSynchronize(c->ring_events[s]));
+    cr_raster_file *dst = c->h_files_ring + (size_t)s * c->d_files_cap;
+    std::memcpy(dst, files.data(), nbytes);
+    CR_CUDA(cudaMemcpyAsync(c->d_files, dst, nbytes, cudaMemcpyHostToDevice, c->ctx->stream));
+    CR_CUDA(cudaEventRecord(c->ring_events[s], c->ctx->stream));
+    c->ring_used[s] = true;
+    return CR_OK;
+}
+
+cr_status alloc_ring(cr_cloud *c) {
+    if (c->h_files_ring) {
+        for (int i = 0; i < cr_cloud::kFileRing; ++i)
+            if (c->ring_used[i]) cudaEventSynchronize(c->ring_events[i]);
+        cudaFreeHost(c->h_files_ring);
+        c->h_files_ring = nullptr;
+    }
+    CR_CUDA(cudaMallocHost((void **)&c->h_files_ring,
+                           sizeof(cr_raster_file) * c->d_files_cap * cr_cloud::kFileRing));
+    for (int i = 0; i < cr_cloud::kFileRing; ++i) {
+        if (!c->ring_events[i])
+            CR_CUDA(cudaEventCreateWithFlags(&c->ring_events[i], cudaEventDisableTiming));
+        c->ring_used[i] = false;
+    }
+    c->ring_slot = -1;
+    return CR_OK;
+}
+
+// allocateBuffers + rebuildFilesBuffer + rebuildCullBuffers
+// (ComputeRasteriserPointCloud.swift:532-589).
+cr_status allocate_cloud(cr_cloud *c, cr_capacity cap, const cr_raster_file *files, uint32_t nf) {
+    free_cloud_buffers(c);
+    c->cap = cap;
+    c->files.clear();
+    if (files && nf > 0)
+        c->files.assign(files, files + nf);
+    else
+        c->files.push_back(identity_file());
+    c->frame_files = c->files;
+    c->mirror.assign(cap.maxResidentBatches, cr_raster_batch{});
+    c->free_slots.clear();
+    for (int64_t s = (int64_t)cap.maxResidentBatches - 1; s >= 0; --s)
+        c->free_slots.push_back((int32_t)s);
+    c->resident = 0;
+    c->points = 0;
+    c->dirty_lo = INT64_MAX;
+    c->dirty_hi = -1;
+
+    const size_t pts = (size_t)cap.maxResidentBatches * cap.pointsPerBatch + kPointPad;
+    cr_status st;
+    if ((st = dalloc(&c->d_low, pts * 4)) || (st = dalloc(&c->d_med, pts * 4)) ||
+        (st = dalloc(&c->d_high, pts * 4)) || (st = dalloc(&c->d_colors, pts * 4)) ||
+        (st = dalloc(&c->d_levels, (pts + 15) & ~size_t(15))))
+        return st;
+    const size_t nb = std::max<size_t>(cap.maxResidentBatches, 1);
+    const size_t ctas = (nb + 255) / 256;
+    if ((st = dalloc(&c->d_batches, nb * sizeof(cr_raster_batch))) ||
+        (st = dalloc(&c->d_visible, nb * sizeof(cr_visible_batch))) ||
+        (st = dalloc(&c->d_cull_tmp, ctas * 256 * sizeof(cr_visible_batch))) ||
+        (st = dalloc(&c->d_cull_cta, ctas * sizeof(uint32_t))) ||
+        (st = dalloc(&c->d_counters, CNT_COUNT * sizeof(uint32_t))))
+        return st;
+    c->d_files_cap = (uint32_t)c->files.size();
+    if ((st = dalloc(&c->d_files, c->d_files_cap * sizeof(cr_raster_file)))) return st;
+    cudaStream_t s = c->ctx->stream;
+    CR_CUDA(cudaMemsetAsync(c->d_low, 0, pts * 4, s));
+    CR_CUDA(cudaMemsetAsync(c->d_med, 0, pts * 4, s));
+    CR_CUDA(cudaMemsetAsync(c->d_high, 0, pts * 4, s));
+    CR_CUDA(cudaMemsetAsync(c->d_colors, 0, pts * 4, s));
+    CR_CUDA(cudaMemsetAsync(c->d_levels, 0, (pts + 15) & ~size_t(15), s));
+    CR_CUDA(cudaMemsetAsync(c->d_batches, 0, nb * sizeof(cr_raster_batch), s));
+    CR_CUDA(cudaMemsetAsync(c->d_visible, 0, nb * sizeof(cr_visible_batch), s));
+    CR_CUDA(cudaMemsetAsync(c->d_counters, 0, CNT_COUNT * sizeof(uint32_t), s));
+    if ((st = alloc_ring(c))) return st;
+    if ((st = upload_files(c, c->files))) return st;
+    CR_CUDA(cudaStreamSynchronize(s));
+    return CR_OK;
+}
+
+bool config_unsupported(const cr_config *cfg, std::string &why) {
+    if (cfg->applyDisplacement) why = "applyDisplacement (user displacement kernels) is not supported";
+    else if (cfg->applyTint) why = "applyTint (user tint kernels) is not supported";
+    else if (cfg->tintAlphaIsCoverage) why = "tintAlphaIsCoverage (OIT coverage) is not supported";
+    else if (cfg->motionBlur > 0.0f) why = "motionBlur is not supported";
+    else return false;
+    return true;
+}
+
+CullUniforms make_cull_uniforms(const cr_config *cfg, const cr_camera *cam, int w, int h) {
+    CullUniforms u;
+    std::memcpy(u.view, cam->view, sizeof(u.view));
+    std::memcpy(u.proj, cam->projection, sizeof(u.proj));
+    u.width = w;
+    u.height = h;
+    u.enableFrustumCulling = cfg->enableFrustumCulling != 0;
+    u.lodBias = cfg->lodBias;
+    u.enableCLOD = cfg->enableCLOD != 0;
+    return u;
+}
+
+RasterUniforms make_raster_uniforms(const cr_config *cfg, const cr_camera *cam, int w, int h) {
+    RasterUniforms u;
+    std::memcpy(u.view, cam->view, sizeof(u.view));
+    std::memcpy(u.proj, cam->projection, sizeof(u.proj));
+    u.width = w;
+    u.height = h;
+    u.lodDither = cfg->enableLODDither != 0;
+    u.pointSizeMode = cfg->pointSizeMode;
+    u.minimumPointSize = cfg->minimumPointSize;
+    u.maximumPointSize = cfg->maximumPointSize;
+    u.pointSizeScale = cfg->pointSizeScale;
+    u.depthTolerance = cfg->depthTolerance;
+    u.colorizeChunks = cfg->colorizeChunks != 0;
+    u.colorizeOverdraw = cfg->colorizeOverdraw != 0;
+    return u;
+}
+
+cr_status validate_render(cr_context *ctx, cr_frame *frame, const cr_config *cfg,
+                          const cr_camera *cam) {
+    if (!ctx || !frame || !cfg || !cam) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    if (frame->ctx != ctx) return fail(CR_ERR_INVALID_ARGUMENT, "frame belongs to another context");
+    if (cfg->mode != CR_MODE_HIGH_QUALITY_AVERAGE && cfg->mode != CR_MODE_NEAREST_POINT)
+        return fail(CR_ERR_INVALID_ARGUMENT, "config.mode must be 0 (HQS) or 1 (nearest)");
+    if (cfg->pointSizeMode != 0 && cfg->pointSizeMode != 1)
+        return fail(CR_ERR_INVALID_ARGUMENT, "config.pointSizeMode must be 0 or 1");
+    std::string why;
+    if (config_unsupported(cfg, why)) return fail(CR_ERR_UNSUPPORTED, why);
+    return CR_OK;
+}
+
+// encodeNearestIndexPass (ComputeRasteriser.swift:505-522) into the frame's key plane.
+cr_status nearest_index_pass(cr_context *ctx, cr_frame *f, cr_cloud *cloud, const cr_config *cfg,
+                             const cr_camera *cam) {
+    cudaStream_t s = ctx->stream;
+    const size_t npix = (size_t)f->width * f->height;
+    CR_CUDA(cudaMemsetAsync(f->d_nearest, 0, npix * sizeof(unsigned long long), s));
+    cr_status st = launch_cull(cloud, make_cull_uniforms(cfg, cam, f->width, f->height), s);
+    if (st) return st;
+    RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
+    return launch_raster(cloud, PASS_NEAREST, make_raster_uniforms(cfg, cam, f->width, f->height),
+                         t, s);
+}
+
+int trunc_i(float x) {
+    if (std::isnan(x)) return 0;
+    if (x >= 2147483648.0f) return INT32_MAX;
+    if (x <= -2147483648.0f) return INT32_MIN;
+    return (int)x;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Exported API
+// ===========================================================================
+extern "C" {
+
+CR_API const char *cr_status_string(cr_status s) {
+    switch (s) {
+    case CR_OK: return "CR_OK";
+    case CR_ERR_INVALID_ARGUMENT: return "CR_ERR_INVALID_ARGUMENT";
+    case CR_ERR_OUT_OF_MEMORY: return "CR_ERR_OUT_OF_MEMORY";
+    case CR_ERR_CUDA: return "CR_ERR_CUDA";
+    case CR_ERR_UNSUPPORTED: return "CR_ERR_UNSUPPORTED";
+    case CR_ERR_CAPACITY: return "CR_ERR_CAPACITY";
+    case CR_ERR_TIMEOUT: return "CR_ERR_TIMEOUT";
+    case CR_ERR_NO_DEVICE: return "CR_ERR_NO_DEVICE";
+    case CR_ERR_INTERNAL: return "CR_ERR_INTERNAL";
+    }
+    return "CR_ERR_UNKNOWN";
+}
+
+CR_API const char *cr_last_error_detail(void) { return cri::g_detail.c_str(); }
+
+CR_API cr_status cr_layout_sizes(uint32_t sizes[5]) {
+    if (!sizes) return fail(CR_ERR_INVALID_ARGUMENT, "sizes is null");
+    sizes[0] = sizeof(cr_raster_batch);
+    sizes[1] = sizeof(cr_raster_file);
+    sizes[2] = sizeof(cr_raster_pixel);
+    sizes[3] = sizeof(cr_visible_batch);
+    sizes[4] = sizeof(cr_dispatch_args);
+    return CR_OK;
+}
+
+CR_API cr_status cr_config_default(cr_config *out) {
+    if (!out) return fail(CR_ERR_INVALID_ARGUMENT, "out is null");
+    std::memset(out, 0, sizeof(*out));
+    out->mode = CR_MODE_HIGH_QUALITY_AVERAGE;
+    out->depthTolerance = 0.01f;
+    out->enableFrustumCulling = 1;
+    out->lodBias = 0;
+    out->enableCLOD = 1;
+    out->enableLODDither = 1;
+    out->holeFillIterations = 0;
+    out->pointSizeMode = CR_POINT_SIZE_SCREEN_SPACE;
+    out->minimumPointSize = 1.0f;
+    out->maximumPointSize = 1.0f;
+    out->pointSizeScale = 1.0f;
+    out->writesSceneDepth = 1;
+    out->motionBlur = 0.0f;
+    out->motionBlurSamples = 8;
+    out->motionBlurMaxSpread = 64.0f;
+    return CR_OK;
+}
+
+// ---------------------------------------------------------------- context
+CR_API cr_status cr_context_create(int device, cr_context **out) {
+    if (!out) return fail(CR_ERR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(CR_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= n) return fail(CR_ERR_INVALID_ARGUMENT, "device out of range");
+    DeviceGuard g(device);
+    cudaDeviceProp prop;
+    CR_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return fail(CR_ERR_NO_DEVICE, "this library is built for sm_100a (B200) devices");
+    auto *ctx = new cr_context();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return cri::cuda_fail(e, "cudaStreamCreateWithFlags");
+    }
+    *out = ctx;
+    return CR_OK;
+}
+
+CR_API cr_status cr_context_destroy(cr_context *ctx) {
+    if (!ctx) return CR_OK;
+    DeviceGuard g(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return CR_OK;
+}
+
+CR_API cr_status cr_context_synchronize(cr_context *ctx) {
+    if (!ctx) return fail(CR_ERR_INVALID_ARGUMENT, "ctx is null");
+    DeviceGuard g(ctx->device);
+    CR_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CR_OK;
+}
+
+CR_API cr_status cr_context_stream(cr_context *ctx, void **stream_out) {
+    if (!ctx || !stream_out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    *stream_out = (void *)ctx->stream;
+    return CR_OK;
+}
+
+// ---------------------------------------------------------------- cloud
+CR_API cr_status cr_cloud_create(cr_context *ctx, cr_capacity cap, const cr_raster_file *files,
+                                 uint32_t nfiles, cr_cloud **out) {
+    if (!ctx || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    // ComputeRasteriserCapacity preconditions (ComputeRasteriserPointCloud.swift:31-36).
+    if (cap.maxResidentBatches == 0) return fail(CR_ERR_INVALID_ARGUMENT, "maxResidentBatches must be positive");
+    if (cap.pointsPerBatch == 0) return fail(CR_ERR_INVALID_ARGUMENT, "pointsPerBatch must be positive");
+    if ((uint64_t)cap.maxResidentBatches * cap.pointsPerBatch >= 0xffffffffull)
+        return fail(CR_ERR_CAPACITY, "pool exceeds 2^32-1 points (point indices are 32-bit)");
+    if (nfiles > 0 && !files) return fail(CR_ERR_INVALID_ARGUMENT, "files is null");
+    DeviceGuard g(ctx->device);
+    auto *c = new cr_cloud();
+    c->ctx = ctx;
+    cr_status st = allocate_cloud(c, cap, files, nfiles);
+    if (st != CR_OK) {
+        std::string d = cr_last_error_detail();
+        free_cloud_buffers(c);
+        delete c;
+        return fail(st, d);
+    }
+    *out = c;
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_destroy(cr_cloud *c) {
+    if (!c) return CR_OK;
+    DeviceGuard g(c->ctx->device);
+    cudaStreamSynchronize(c->ctx->stream);
+    free_cloud_buffers(c);
+    if (c->h_files_ring) cudaFreeHost(c->h_files_ring);
+    for (auto &e : c->ring_events)
+        if (e) cudaEventDestroy(e);
+    delete c;
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_reallocate(cr_cloud *c, cr_capacity cap, const cr_raster_file *files,
+                                     uint32_t nfiles) {
+    if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
+    if (cap.maxResidentBatches == 0 || cap.pointsPerBatch == 0)
+        return fail(CR_ERR_INVALID_ARGUMENT, "capacity must be positive");
+    if ((uint64_t)cap.maxResidentBatches * cap.pointsPerBatch >= 0xffffffffull)
+        return fail(CR_ERR_CAPACITY, "pool exceeds 2^32-1 points");
+    DeviceGuard g(c->ctx->device);
+    CR_CUDA(cudaStreamSynchronize(c->ctx->stream));
+    std::vector<cr_raster_file> keep;
+    if (files && nfiles) keep.assign(files, files + nfiles);
+    else keep = c->files;
+    return allocate_cloud(c, cap, keep.data(), (uint32_t)keep.size());
+}
+
+CR_API cr_status cr_cloud_set_files(cr_cloud *c, const cr_raster_file *files, uint32_t nfiles) {
+    if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
+    if (nfiles > 0 && !files) return fail(CR_ERR_INVALID_ARGUMENT, "files is null");
+    DeviceGuard g(c->ctx->device);
+    if (nfiles == 0) c->files.assign(1, identity_file());
+    else c->files.assign(files, files + nfiles);
+    c->frame_files = c->files;
+    if (c->files.size() > c->d_files_cap) {
+        CR_CUDA(cudaStreamSynchronize(c->ctx->stream));
+        dfree(c->d_files);
+        cr_status st = dalloc(&c->d_files, c->files.size() * sizeof(cr_raster_file));
+        if (st) return st;
+        c->d_files_cap = (uint32_t)c->files.size();
+        if ((st = alloc_ring(c))) return st;
+    }
+    return upload_files(c, c->files);
+}
+
+CR_API cr_status cr_cloud_add_batches(cr_cloud *c, const uint32_t *low, const uint32_t *med,
+                                      const uint32_t *high, const uint32_t *colors,
+                                      const uint8_t *levels, uint64_t points_len,
+                                      const cr_raster_batch *batches, uint32_t n, int commit,
+                                      int32_t *slots_out) {
+    if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
+    if (n > c->free_slots.size())
+        return fail(CR_ERR_CAPACITY, "addBatches: not enough free slots (have " +
+                                         std::to_string(c->free_slots.size()) + ", need " +
+                                         std::to_string(n) + ")");
+    if (n == 0) return CR_OK;
+    if (!batches || !low || !med || !high || !colors || !levels)
+        return fail(CR_ERR_INVALID_ARGUMENT, "null array");
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint64_t src = batches[i].firstPoint, cnt = batches[i].numPoints;
+        if (cnt > c->cap.pointsPerBatch)
+            return fail(CR_ERR_CAPACITY, "batch numPoints (" + std::to_string(cnt) +
+                                             ") exceeds slot capacity (" +
+                                             std::to_string(c->cap.pointsPerBatch) + ")");
+        if (src + cnt > points_len)
+            return fail(CR_ERR_INVALID_ARGUMENT, "addBatches: source data too small for batch");
+        if (batches[i].fileIndex >= c->files.size())
+            return fail(CR_ERR_INVALID_ARGUMENT, "batch fileIndex outside the file table");
+    }
+    DeviceGuard g(c->ctx->device);
+    cudaStream_t s = c->ctx->stream;
+    // Copies of consecutive batches into consecutive slots merge into one run.
+    uint64_t run_src = 0, run_dst = 0, run_n = 0;
+    auto flush_run = [&]() -> cr_status {
+        if (run_n == 0) return CR_OK;
+        CR_CUDA(cudaMemcpyAsync(c->d_low + run_dst, low + run_src, run_n * 4, cudaMemcpyHostToDevice, s));
+        CR_CUDA(cudaMemcpyAsync(c->d_med + run_dst, med + run_src, run_n * 4, cudaMemcpyHostToDevice, s));
+        CR_CUDA(cudaMemcpyAsync(c->d_high + run_dst, high + run_src, run_n * 4, cudaMemcpyHostToDevice, s));
+        CR_CUDA(cudaMemcpyAsync(c->d_colors + run_dst, colors + run_src, run_n * 4, cudaMemcpyHostToDevice, s));
+        CR_CUDA(cudaMemcpyAsync(c->d_levels + run_dst, levels + run_src, run_n, cudaMemcpyHostToDevice, s));
+        run_n = 0;
+        return CR_OK;
+    };
+    for (uint32_t i = 0; i < n; ++i) {
+        const int32_t slot = c->free_slots.back();
+        c->free_slots.pop_back();
+        if (slots_out) slots_out[i] = slot;
+        const uint64_t dst = (uint64_t)slot * c->cap.pointsPerBatch;
+        const uint64_t src = batches[i].firstPoint, cnt = batches[i].numPoints;
+        if (cnt > 0) {
+            if (run_n > 0 && run_src + run_n == src && run_dst + run_n == dst) {
+                run_n += cnt;
+            } else {
+                cr_status st = flush_run();
+                if (st) return st;
+                run_src = src;
+                run_dst = dst;
+                run_n = cnt;
+            }
+        }
+        cr_raster_batch b = batches[i];
+        b.firstPoint = (uint32_t)dst;
+        b.state = 1;
+        c->mirror[slot] = b;
+        mark_dirty(c, slot, slot);
+        c->resident += 1;
+        c->points += cnt;
+    }
+    cr_status st = flush_run();
+    if (st) return st;
+    if (commit) return flush_mirror(c);
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_remove_batches(cr_cloud *c, const int32_t *slots, uint32_t n, int commit) {
+    if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
+    if (n == 0) return CR_OK;
+    if (!slots) return fail(CR_ERR_INVALID_ARGUMENT, "slots is null");
+    for (uint32_t i = 0; i < n; ++i)
+        if (slots[i] < 0 || (uint32_t)slots[i] >= c->cap.maxResidentBatches)
+            return fail(CR_ERR_INVALID_ARGUMENT,
+                        "removeBatches: slot " + std::to_string(slots[i]) + " out of range");
+    for (uint32_t i = 0; i < n; ++i) {
+        cr_raster_batch &b = c->mirror[slots[i]];
+        if (b.state == 0) continue;
+        c->points -= b.numPoints;
+        c->resident -= 1;
+        b.state = 0;
+        b.numPoints = 0;
+        mark_dirty(c, slots[i], slots[i]);
+        c->free_slots.push_back(slots[i]);
+    }
+    if (commit) {
+        DeviceGuard g(c->ctx->device);
+        return flush_mirror(c);
+    }
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_commit(cr_cloud *c) {
+    if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
+    DeviceGuard g(c->ctx->device);
+    return flush_mirror(c);
+}
+
+CR_API cr_status cr_cloud_clear(cr_cloud *c) {
+    if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
+    for (auto &b : c->mirror) {
+        b.state = 0;
+        b.numPoints = 0;
+    }
+    c->free_slots.clear();
+    for (int64_t s = (int64_t)c->cap.maxResidentBatches - 1; s >= 0; --s)
+        c->free_slots.push_back((int32_t)s);
+    c->resident = 0;
+    c->points = 0;
+    mark_dirty(c, 0, (int64_t)c->mirror.size() - 1);
+    DeviceGuard g(c->ctx->device);
+    return flush_mirror(c);
+}
+
+CR_API cr_status cr_cloud_update_files(cr_cloud *c, const float vp[16], const float model[16],
+                                       const float *frustum, const float *prev_vp) {
+    if (!c || !vp || !model) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    DeviceGuard g(c->ctx->device);
+    std::vector<cr_raster_file> snap = c->files;
+    for (size_t i = 0; i < snap.size(); ++i) {
+        float world[16];
+        mat4mul(model, c->files[i].world, world);
+        mat4mul(vp, world, snap[i].transform);
+        mat4mul(frustum ? frustum : vp, world, snap[i].transformFrustum);
+        std::memcpy(snap[i].world, world, sizeof(world));
+        mat4mul(prev_vp ? prev_vp : vp, world, snap[i].prevTransform);
+    }
+    c->frame_files = snap;
+    return upload_files(c, snap);
+}
+
+CR_API cr_status cr_cloud_info_get(const cr_cloud *c, cr_cloud_info *out) {
+    if (!c || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    out->capacity = c->cap;
+    out->residentBatchCount = c->resident;
+    out->pointCount = c->points;
+    out->freeSlotCount = (uint32_t)c->free_slots.size();
+    out->fileCount = (uint32_t)c->files.size();
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_read_files(const cr_cloud *c, cr_raster_file *out, uint32_t n) {
+    if (!c || (!out && n)) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    if (n > c->frame_files.size()) return fail(CR_ERR_INVALID_ARGUMENT, "n exceeds file count");
+    std::memcpy(out, c->frame_files.data(), n * sizeof(cr_raster_file));
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_read_batches(cr_cloud *c, cr_raster_batch *out, uint32_t first, uint32_t n) {
+    if (!c || (!out && n)) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    if ((uint64_t)first + n > c->cap.maxResidentBatches)
+        return fail(CR_ERR_INVALID_ARGUMENT, "slot range out of bounds");
+    if (n == 0) return CR_OK;
+    DeviceGuard g(c->ctx->device);
+    CR_CUDA(cudaMemcpyAsync(out, c->d_batches + first, n * sizeof(cr_raster_batch),
+                            cudaMemcpyDeviceToHost, c->ctx->stream));
+    CR_CUDA(cudaStreamSynchronize(c->ctx->stream));
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_read_points(cr_cloud *c, uint64_t first, uint64_t n, uint32_t *low,
+                                      uint32_t *med, uint32_t *high, uint32_t *colors,
+                                      uint8_t *levels) {
+    if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
+    const uint64_t total = (uint64_t)c->cap.maxResidentBatches * c->cap.pointsPerBatch;
+    if (first + n > total) return fail(CR_ERR_INVALID_ARGUMENT, "point range out of bounds");
+    if (n == 0) return CR_OK;
+    DeviceGuard g(c->ctx->device);
+    cudaStream_t s = c->ctx->stream;
+    if (low) CR_CUDA(cudaMemcpyAsync(low, c->d_low + first, n * 4, cudaMemcpyDeviceToHost, s));
+    if (med) CR_CUDA(cudaMemcpyAsync(med, c->d_med + first, n * 4, cudaMemcpyDeviceToHost, s));
+    if (high) CR_CUDA(cudaMemcpyAsync(high, c->d_high + first, n * 4, cudaMemcpyDeviceToHost, s));
+    if (colors) CR_CUDA(cudaMemcpyAsync(colors, c->d_colors + first, n * 4, cudaMemcpyDeviceToHost, s));
+    if (levels) CR_CUDA(cudaMemcpyAsync(levels, c->d_levels + first, n, cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_read_visible(cr_cloud *c, cr_visible_batch *out, uint32_t cap,
+                                       uint32_t *count_out) {
+    if (!c || !count_out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    DeviceGuard g(c->ctx->device);
+    cudaStream_t s = c->ctx->stream;
+    uint32_t count = 0;
+    CR_CUDA(cudaMemcpyAsync(&count, c->d_counters + CNT_VISIBLE, 4, cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    *count_out = count;
+    const uint32_t k = std::min(count, cap);
+    if (k && out) {
+        CR_CUDA(cudaMemcpyAsync(out, c->d_visible, k * sizeof(cr_visible_batch),
+                                cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+    }
+    return CR_OK;
+}
+
+// ---------------------------------------------------------------- frame
+CR_API cr_status cr_frame_create(cr_context *ctx, int w, int h, cr_frame **out) {
+    if (!ctx || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (w <= 0 || h <= 0) return fail(CR_ERR_INVALID_ARGUMENT, "frame size must be positive");
+    if ((uint64_t)w * (uint64_t)h >= (1ull << 31))
+        return fail(CR_ERR_CAPACITY, "frame exceeds 2^31 pixels");
+    DeviceGuard g(ctx->device);
+    auto *f = new cr_frame();
+    f->ctx = ctx;
+    f->width = w;
+    f->height = h;
+    const size_t npix = (size_t)w * h;
+    cr_status st;
+    if ((st = dalloc(&f->d_depth, npix * 4)) || (st = dalloc(&f->d_accum, npix * 16)) ||
+        (st = dalloc(&f->d_nearest, npix * 8)) || (st = dalloc(&f->d_rgba[0], npix * 4)) ||
+        (st = dalloc(&f->d_rgba[1], npix * 4)) || (st = dalloc(&f->d_depthf, npix * 4))) {
+        std::string d = cr_last_error_detail();
+        cr_frame_destroy(f);
+        return fail(st, d);
+    }
+    cudaStream_t s = ctx->stream;
+    cudaMemsetAsync(f->d_depth, 0, npix * 4, s);
+    cudaMemsetAsync(f->d_accum, 0, npix * 16, s);
+    cudaMemsetAsync(f->d_nearest, 0, npix * 8, s);
+    cudaMemsetAsync(f->d_rgba[0], 0, npix * 4, s);
+    cudaMemsetAsync(f->d_rgba[1], 0, npix * 4, s);
+    cudaMemsetAsync(f->d_depthf, 0, npix * 4, s);
+    CR_CUDA(cudaStreamSynchronize(s));
+    *out = f;
+    return CR_OK;
+}
+
+CR_API cr_status cr_frame_destroy(cr_frame *f) {
+    if (!f) return CR_OK;
+    DeviceGuard g(f->ctx->device);
+    cudaStreamSynchronize(f->ctx->stream);
+    dfree(f->d_depth);
+    dfree(f->d_accum);
+    dfree(f->d_nearest);
+    dfree(f->d_rgba[0]);
+    dfree(f->d_rgba[1]);
+    dfree(f->d_depthf);
+    delete f;
+    return CR_OK;
+}
+
+CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds,
+                           uint32_t nclouds, const cr_config *cfg, const cr_camera *cam) {
+    cr_status st = validate_render(ctx, f, cfg, cam);
+    if (st) return st;
+    if (nclouds && !clouds) return fail(CR_ERR_INVALID_ARGUMENT, "clouds is null");
+    for (uint32_t i = 0; i < nclouds; ++i)
+        if (!clouds[i] || clouds[i]->ctx != ctx)
+            return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null or from another context");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int W = f->width, H = f->height;
+    const size_t npix = (size_t)W * H;
+    ResolveUniforms ru{W, H, {cfg->backgroundColor[0], cfg->backgroundColor[1],
+                              cfg->backgroundColor[2], cfg->backgroundColor[3]}};
+    if (cfg->mode == CR_MODE_HIGH_QUALITY_AVERAGE) {
+        // encodeHighQualityAverage (ComputeRasteriser.swift:322-456).
+        CR_CUDA(cudaMemsetAsync(f->d_depth, 0, npix * 4, s));
+        CR_CUDA(cudaMemsetAsync(f->d_accum, 0, npix * 16, s));
+        std::vector<cr_cloud *> resident;
+        for (uint32_t i = 0; i < nclouds; ++i)
+            if (clouds[i]->resident > 0) resident.push_back(clouds[i]);
+        const CullUniforms cu = make_cull_uniforms(cfg, cam, W, H);
+        const RasterUniforms rau = make_raster_uniforms(cfg, cam, W, H);
+        const RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
+        for (cr_cloud *c : resident)
+            if ((st = launch_cull(c, cu, s))) return st;
+        for (cr_cloud *c : resident)
+            if ((st = launch_raster(c, PASS_DEPTH, rau, t, s))) return st;
+        for (cr_cloud *c : resident)
+            if ((st = launch_raster(c, PASS_COLOR, rau, t, s))) return st;
+        if ((st = launch_resolve_hqs(f, ru, s))) return st;
+        f->last_mode = 0;
+    } else {
+        // encodeNearestPoint (ComputeRasteriser.swift:483-497): first resident cloud only.
+        cr_cloud *first = nullptr;
+        for (uint32_t i = 0; i < nclouds && !first; ++i)
+            if (clouds[i]->resident > 0) first = clouds[i];
+        if (first) {
+            if ((st = nearest_index_pass(ctx, f, first, cfg, cam))) return st;
+            if ((st = launch_resolve_nearest(f, first->d_colors, ru, s))) return st;
+            f->last_mode = 1;
+        }
+    }
+    // encodeHoleFill (ComputeRasteriser.swift:298-320) always starts from the
+    // resolve target.
+    f->final_rgba = 0;
+    return launch_hole_fill(f, std::max(0, cfg->holeFillIterations), s);
+}
+
+static cr_status read_plane(cr_frame *f, void *out, const void *src, size_t bytes) {
+    if (!f || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    DeviceGuard g(f->ctx->device);
+    CR_CUDA(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, f->ctx->stream));
+    CR_CUDA(cudaStreamSynchronize(f->ctx->stream));
+    return CR_OK;
+}
+
+CR_API cr_status cr_frame_read_rgba8(cr_frame *f, uint8_t *out) {
+    if (!f) return fail(CR_ERR_INVALID_ARGUMENT, "frame is null");
+    return read_plane(f, out, f->d_rgba[f->final_rgba], (size_t)f->width * f->height * 4);
+}
+
+CR_API cr_status cr_frame_read_depth_f32(cr_frame *f, float *out) {
+    if (!f) return fail(CR_ERR_INVALID_ARGUMENT, "frame is null");
+    return read_plane(f, out, f->d_depthf, (size_t)f->width * f->height * 4);
+}
+
+CR_API cr_status cr_frame_read_pixels(cr_frame *f, cr_raster_pixel *out) {
+    if (!f || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    const size_t npix = (size_t)f->width * f->height;
+    std::vector<uint32_t> depth(npix);
+    std::vector<uint4> acc(npix);
+    cr_status st = read_plane(f, depth.data(), f->d_depth, npix * 4);
+    if (st) return st;
+    if ((st = read_plane(f, acc.data(), f->d_accum, npix * 16))) return st;
+    for (size_t p = 0; p < npix; ++p) {
+        out[p].depth = depth[p];
+        out[p].red = acc[p].x;
+        out[p].green = acc[p].y;
+        out[p].blue = acc[p].z;
+        out[p].count = acc[p].w;
+        out[p].weight = 0;
+        out[p].padding[0] = out[p].padding[1] = 0;
+    }
+    return CR_OK;
+}
+
+static cr_status read_nearest(cr_frame *f, uint32_t *depth, uint32_t *index, int row0, int nrows) {
+    if (!f) return fail(CR_ERR_INVALID_ARGUMENT, "frame is null");
+    if (row0 < 0 || nrows < 0 || row0 + nrows > f->height)
+        return fail(CR_ERR_INVALID_ARGUMENT, "row range out of bounds");
+    const size_t n = (size_t)nrows * f->width;
+    if (n == 0) return CR_OK;
+    std::vector<unsigned long long> keys(n);
+    cr_status st = read_plane(f, keys.data(), f->d_nearest + (size_t)row0 * f->width, n * 8);
+    if (st) return st;
+    for (size_t p = 0; p < n; ++p) {
+        if (depth) depth[p] = (uint32_t)(keys[p] >> 32);
+        if (index) index[p] = ~(uint32_t)keys[p];
+    }
+    return CR_OK;
+}
+
+CR_API cr_status cr_frame_read_nearest_depth(cr_frame *f, uint32_t *out) {
+    if (!out) return fail(CR_ERR_INVALID_ARGUMENT, "out is null");
+    return read_nearest(f, out, nullptr, 0, f ? f->height : 0);
+}
+
+CR_API cr_status cr_frame_read_nearest_index(cr_frame *f, uint32_t *out) {
+    if (!out) return fail(CR_ERR_INVALID_ARGUMENT, "out is null");
+    return read_nearest(f, nullptr, out, 0, f ? f->height : 0);
+}
+
+CR_API cr_status cr_frame_read_nearest_index_rows(cr_frame *f, int row0, int nrows, uint32_t *out) {
+    if (!out) return fail(CR_ERR_INVALID_ARGUMENT, "out is null");
+    return read_nearest(f, nullptr, out, row0, nrows);
+}
+
+// pickPointIndex (ComputeRasteriser.swift:609-670).
+CR_API cr_status cr_pick(cr_context *ctx, cr_frame *f, cr_cloud *cloud, const float ndc[2],
+                         const cr_config *cfg, const cr_camera *cam, int search_radius,
+                         uint32_t *index_out, int *found_out) {
+    if (!ndc || !index_out || !found_out || !cloud)
+        return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    *found_out = 0;
+    cr_status st = validate_render(ctx, f, cfg, cam);
+    if (st) return st;
+    const int W = f->width, H = f->height;
+    if (cloud->resident == 0) return CR_OK;
+    DeviceGuard g(ctx->device);
+    // NDC (y up) -> buffer pixel; the nearest pass stores row 0 at the top.
+    const int px = std::min(std::max(trunc_i((ndc[0] * 0.5f + 0.5f) * (float)W), 0), W - 1);
+    const int pyb = trunc_i((ndc[1] * 0.5f + 0.5f) * (float)H);
+    const int py = std::min(std::max(H - 1 - pyb, 0), H - 1);
+    if ((st = nearest_index_pass(ctx, f, cloud, cfg, cam))) return st;
+    const int r = std::max(0, search_radius);
+    const int row0 = std::max(0, py - r), row1 = std::min(H - 1, py + r);
+    std::vector<uint32_t> band((size_t)(row1 - row0 + 1) * W);
+    if ((st = read_nearest(f, nullptr, band.data(), row0, row1 - row0 + 1))) return st;
+    long best_d = -1;
+    uint32_t best = 0;
+    const long r2 = (long)r * r;
+    for (int y = row0; y <= row1; ++y) {
+        const long dy = y - py;
+        for (int x = std::max(0, px - r); x <= std::min(W - 1, px + r); ++x) {
+            const long dx = x - px;
+            const long d = dx * dx + dy * dy;
+            if (d > r2 || (best_d >= 0 && d >= best_d)) continue;
+            const uint32_t v = band[(size_t)(y - row0) * W + x];
+            if (v != CR_INVALID_INDEX) {
+                best_d = d;
+                best = v;
+            }
+        }
+    }
+    if (best_d >= 0) {
+        *index_out = best;
+        *found_out = 1;
+    }
+    return CR_OK;
+}
+
+}  // extern "C"

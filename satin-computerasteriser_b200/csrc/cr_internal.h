@@ -1,0 +1,139 @@
+// cr_internal.h — library-internal objects and kernel launch interfaces.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "cr/cr.h"
+
+// ---------------------------------------------------------------------------
+// Error plumbing
+// ---------------------------------------------------------------------------
+namespace cri {
+void set_error(const std::string &detail);
+cr_status fail(cr_status st, const std::string &detail);
+cr_status cuda_fail(cudaError_t e, const char *what);
+}  // namespace cri
+
+#define CR_CUDA(call)                                                        \
+    do {                                                                     \
+        cudaError_t e_ = (call);                                             \
+        if (e_ != cudaSuccess) return cri::cuda_fail(e_, #call);             \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Per-cloud device counters (one cache line).
+// ---------------------------------------------------------------------------
+enum CounterSlot : int {
+    CNT_VISIBLE = 0,     // survivors of the last cull (VisibleBatch count)
+    CNT_WORK_DEPTH = 1,  // dynamic work cursor of the depth / nearest pass
+    CNT_WORK_COLOR = 2,  // dynamic work cursor of the colour pass
+    CNT_WORK_AUX = 3,    // spare cursor (gradient pass)
+    CNT_ARGS_X = 4,      // CRDispatchArgs mirror: {count, 1, 1}
+    CNT_ARGS_Y = 5,
+    CNT_ARGS_Z = 6,
+    CNT_ERROR = 7,       // first device-side error code (0 = none)
+    CNT_COUNT = 32
+};
+
+struct cr_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    int raster_blocks_per_sm = 0;  // occupancy of the persistent point passes
+};
+
+struct cr_cloud {
+    cr_context *ctx = nullptr;
+    cr_capacity cap{0, 0};
+    std::vector<cr_raster_file> files;        // file table (world matrices)
+    std::vector<cr_raster_file> frame_files;  // last updateFiles snapshot
+    std::vector<cr_raster_batch> mirror;      // host mirror of every slot
+    std::vector<int32_t> free_slots;          // LIFO, back() is handed out first
+    int64_t dirty_lo = INT64_MAX, dirty_hi = -1;
+    uint32_t resident = 0;
+    uint64_t points = 0;
+
+    // Device slot pool (structure of arrays, as the reference lays it out).
+    uint32_t *d_low = nullptr, *d_med = nullptr, *d_high = nullptr, *d_colors = nullptr;
+    uint8_t *d_levels = nullptr;
+    cr_raster_batch *d_batches = nullptr;
+    cr_raster_file *d_files = nullptr;
+    uint32_t d_files_cap = 0;
+
+    // Cull outputs and scratch.
+    cr_visible_batch *d_visible = nullptr;   // ordered survivors
+    cr_visible_batch *d_cull_tmp = nullptr;  // per-CTA compacted survivors
+    uint32_t *d_cull_cta = nullptr;          // per-CTA survivor counts
+    uint32_t *d_counters = nullptr;          // CounterSlot words
+
+    // Pinned staging ring for the per-frame file table upload.
+    static constexpr int kFileRing = 8;
+    cr_raster_file *h_files_ring = nullptr;
+    cudaEvent_t ring_events[kFileRing] = {};
+    bool ring_used[kFileRing] = {};
+    int ring_slot = -1;
+};
+
+struct cr_frame {
+    cr_context *ctx = nullptr;
+    int width = 0, height = 0;
+    uint32_t *d_depth = nullptr;            // HQS depth plane (RasterPixel.depth)
+    uint4 *d_accum = nullptr;               // HQS red, green, blue, count
+    unsigned long long *d_nearest = nullptr;  // (depth << 32) | ~pointIndex
+    uint32_t *d_rgba[2] = {nullptr, nullptr}; // RGBA8 ping-pong (resolve, hole fill)
+    float *d_depthf = nullptr;              // resolve R32F depth
+    int final_rgba = 0;                     // which d_rgba holds the final image
+    int last_mode = -1;                     // 0 HQS, 1 nearest, -1 none
+};
+
+// ---------------------------------------------------------------------------
+// Kernel launch interfaces
+// ---------------------------------------------------------------------------
+struct CullUniforms {
+    float view[16];
+    float proj[16];
+    int width, height;
+    int enableFrustumCulling, lodBias, enableCLOD;
+};
+
+cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s);
+
+enum RasterPass : int { PASS_DEPTH = 0, PASS_COLOR = 1, PASS_NEAREST = 2 };
+
+struct RasterUniforms {
+    float view[16];
+    float proj[16];
+    int width, height;
+    int lodDither;
+    int pointSizeMode;
+    float minimumPointSize, maximumPointSize, pointSizeScale;
+    float depthTolerance;
+    int colorizeChunks, colorizeOverdraw;
+};
+
+struct RasterTargets {
+    uint32_t *depth;              // HQS depth plane
+    uint4 *accum;                 // HQS accumulators
+    unsigned long long *nearest;  // nearest key plane
+};
+
+cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
+                        const RasterTargets &t, cudaStream_t s);
+
+struct ResolveUniforms {
+    int width, height;
+    float background[4];
+};
+
+cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t s);
+cr_status launch_resolve_nearest(cr_frame *f, const uint32_t *colors, const ResolveUniforms &u,
+                                 cudaStream_t s);
+cr_status launch_hole_fill(cr_frame *f, int iterations, cudaStream_t s);
+cr_status launch_split_nearest(const unsigned long long *keys, uint32_t *depth_out,
+                               uint32_t *index_out, size_t n, cudaStream_t s);
+
+int raster_blocks_per_sm(int pass);
