@@ -303,6 +303,126 @@ CR_API cr_status cr_pick(cr_context *ctx, cr_frame *frame, cr_cloud *cloud, cons
                          const cr_config *config, const cr_camera *camera, int search_radius,
                          uint32_t *index_out, int *found_out);
 
+/* ------------------------------------------------------------------------ */
+/* GPU packer (GPUPacker, GPUPacker.swift:27-392)                            */
+/* ------------------------------------------------------------------------ */
+typedef enum cr_color_format {
+    CR_COLOR_F32X4 = 0, /* RGBA float32 in [0,1] (the reference's float4 colour buffer) */
+    CR_COLOR_RGBA8 = 1  /* packed uint32 r | g<<8 | b<<16 | a<<24                        */
+} cr_color_format;
+
+/* One run of raw points.  positions: x, y, z float32 at each stride (12 for
+ * packed float3, 16 for the reference's 16-byte float3 or a 16-byte record);
+ * colors: one colour per stride in colorFormat.  A 16-byte record
+ * {float x, y, z; uint32 rgba8} is positions = rec, positionStrideBytes = 16,
+ * colors = (char*)rec + 12, colorStrideBytes = 16, colorFormat = CR_COLOR_RGBA8. */
+typedef struct cr_pack_input {
+    const void *positions;
+    uint32_t positionStrideBytes;
+    const void *colors;
+    uint32_t colorStrideBytes;
+    int32_t colorFormat; /* cr_color_format */
+} cr_pack_input;
+
+/* GPUPacker.init(context:lodLevels:coarseVoxelDivisions:) (GPUPacker.swift:75-99). */
+typedef struct cr_pack_params {
+    int32_t lodLevels;            /* default 4, clamped to 1..8              */
+    int32_t coarseVoxelDivisions; /* default 64, at least 1                  */
+    int32_t mortonBits;           /* 10 = 30-bit keys (default), 21 = 63-bit */
+} cr_pack_params;
+
+CR_API cr_status cr_pack_params_default(cr_pack_params *out);
+
+/* GPUPacker.pack(positions:colors:count:into:commandBuffer:) followed by the
+ * completion-handler bounds adoption (GPUPacker.swift:140-160, replacePackedPointCloud
+ * :507-519): the pool grows to ceil(count/pointsPerBatch) slots if needed,
+ * slots [0, nb) are filled in Morton order with per-batch AABBs, LOD levels
+ * and split-precision words, and every other slot is emptied.  inputs_on_device
+ * = 1 when the pointers are device memory.  source_indices (optional, host,
+ * count entries) receives the input index of every packed point (the
+ * PackedPointCloud.sourceIndices permutation).  Synchronous. */
+CR_API cr_status cr_pack(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *input,
+                         uint64_t count, const cr_pack_params *params, int inputs_on_device,
+                         uint32_t *source_indices);
+
+/* addRawChunksGPU(packer:queue:chunks:maxConcurrent:) (GPUPacker.swift:545-577):
+ * each chunk with count > 0 takes the first run of ceil(count/pointsPerBatch)
+ * contiguous free slots and is packed there, leaving every other slot
+ * untouched; chunks without a free run are skipped.  first_slots (nchunks
+ * entries) receives the first slot of each placed chunk in input order and
+ * placed_out their number.  Synchronous. */
+CR_API cr_status cr_pack_chunks(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *chunks,
+                                const uint64_t *counts, uint32_t nchunks,
+                                const cr_pack_params *params, int inputs_on_device,
+                                int32_t *first_slots, uint32_t *placed_out);
+
+/* ------------------------------------------------------------------------ */
+/* Device buffers and pinned host memory (for callers without a CUDA runtime) */
+/* ------------------------------------------------------------------------ */
+CR_API cr_status cr_buffer_create(cr_context *ctx, uint64_t bytes, void **device_ptr);
+CR_API cr_status cr_buffer_destroy(cr_context *ctx, void *device_ptr);
+/* Stream-ordered copies on the context stream, synchronised before return. */
+CR_API cr_status cr_buffer_upload(cr_context *ctx, void *dst_device, const void *src_host,
+                                  uint64_t bytes);
+CR_API cr_status cr_buffer_download(cr_context *ctx, void *dst_host, const void *src_device,
+                                    uint64_t bytes);
+CR_API cr_status cr_host_alloc(uint64_t bytes, void **host_ptr);
+CR_API cr_status cr_host_free(void *host_ptr);
+
+/* ------------------------------------------------------------------------ */
+/* Per-pass timing (the reference's labelled encoders, ComputeRasteriser.swift:379-428) */
+/* ------------------------------------------------------------------------ */
+typedef enum cr_pass_id {
+    CR_PASS_CLEAR = 0,
+    CR_PASS_CULL = 1,
+    CR_PASS_DEPTH = 2,   /* HQS depth, or the fused nearest depth/index pass */
+    CR_PASS_COLOR = 3,
+    CR_PASS_RESOLVE = 4,
+    CR_PASS_HOLE_FILL = 5,
+    CR_PASS_COUNT = 6
+} cr_pass_id;
+
+/* When enabled, every cr_render brackets each pass (over all clouds) with
+ * CUDA events on the context stream, in a ring of the last 256 frames.
+ * Enabling or disabling synchronises the stream and empties the ring. */
+CR_API cr_status cr_context_set_profiling(cr_context *ctx, int enable);
+/* Device milliseconds per pass of the last min(nframes, recorded, 256)
+ * profiled frames, oldest first: ms[k*CR_PASS_COUNT + pass] (0 for passes
+ * that did not run).  frames_out receives the number of frames written.
+ * Synchronises on the events it reads. */
+CR_API cr_status cr_context_pass_times(cr_context *ctx, int32_t nframes, float *ms,
+                                       int32_t *frames_out);
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic workloads (seeded; a pure function of seed and point index)     */
+/* ------------------------------------------------------------------------ */
+/* Fractal heightfield: 2-D gradient noise summed over `octaves` with
+ * `lacunarity` and `gain`, times `amplitude`; x, y uniform in [0, extent];
+ * `outlierFraction` of the points uniform in z over the height range widened
+ * by `outlierMargin`; colour = height ramp + N(0, colorNoiseSigma) per channel. */
+typedef struct cr_synth_terrain {
+    uint64_t seed;
+    float extent;          /* 4000 m  */
+    float amplitude;       /* 200 m   */
+    float baseWavelength;  /* 1500 m  */
+    int32_t octaves;       /* 6       */
+    float lacunarity;      /* 2       */
+    float gain;            /* 0.5     */
+    float outlierFraction; /* 0.05    */
+    float outlierMargin;   /* 50 m    */
+    float colorNoiseSigma; /* 10      */
+} cr_synth_terrain;
+
+CR_API cr_status cr_synth_terrain_default(cr_synth_terrain *t);
+/* Height of the noise surface at (x, y), evaluated on the host. */
+CR_API float cr_synth_terrain_height(const cr_synth_terrain *t, float x, float y);
+/* Points [first, first+count) as 16-byte records {x, y, z, rgba8} in device memory. */
+CR_API cr_status cr_synth_terrain_points(cr_context *ctx, const cr_synth_terrain *t, uint64_t first,
+                                         uint64_t count, void *device_records);
+/* n_axis^3 lattice over [lo, hi]^3 with uniform jitter, uniform RGB8, alpha 255. */
+CR_API cr_status cr_synth_lattice_points(cr_context *ctx, uint64_t seed, uint32_t n_axis, float lo,
+                                         float hi, float jitter, void *device_records);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

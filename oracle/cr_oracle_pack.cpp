@@ -52,6 +52,19 @@ inline uint64_t spread21(uint64_t v) {
 
 struct f3 { float x, y, z; };
 
+// Bounds reductions order floats by their sign-flipped bit patterns (a total
+// order with -0 below +0), so a serial loop and a parallel tree agree on the
+// sign of a zero bound.
+inline uint32_t flip(float f) {
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+    return b ^ ((b >> 31) ? 0xffffffffu : 0x80000000u);
+}
+inline float bmin_(float a, float b) { return flip(b) < flip(a) ? b : a; }
+inline float bmax_(float a, float b) { return flip(b) > flip(a) ? b : a; }
+inline f3 min3(f3 a, f3 b) { return f3{bmin_(a.x, b.x), bmin_(a.y, b.y), bmin_(a.z, b.z)}; }
+inline f3 max3(f3 a, f3 b) { return f3{bmax_(a.x, b.x), bmax_(a.y, b.y), bmax_(a.z, b.z)}; }
+
 // mortonOrder (PackedPointCloudFixtures.swift:218-239): key per point, then a
 // stable sort of the indices by key (equal keys keep input order).
 std::vector<uint32_t> morton_order(const std::vector<f3> &pos, f3 bmin, f3 bmax, int bits) {
@@ -149,8 +162,8 @@ extern "C" int orc_pack(const float *positions, const float *colors_f32,
     f3 bmin{3.4028235e38f, 3.4028235e38f, 3.4028235e38f};
     f3 bmax{-3.4028235e38f, -3.4028235e38f, -3.4028235e38f};
     for (const f3 &p : pos) {
-        bmin = f3{std::min(bmin.x, p.x), std::min(bmin.y, p.y), std::min(bmin.z, p.z)};
-        bmax = f3{std::max(bmax.x, p.x), std::max(bmax.y, p.y), std::max(bmax.z, p.z)};
+        bmin = min3(bmin, p);
+        bmax = max3(bmax, p);
     }
 
     std::vector<uint32_t> order = morton_order(pos, bmin, bmax, morton_bits);
@@ -191,9 +204,8 @@ extern "C" int orc_pack(const float *positions, const float *colors_f32,
         f3 mn{3.4028235e38f, 3.4028235e38f, 3.4028235e38f};
         f3 mx{-3.4028235e38f, -3.4028235e38f, -3.4028235e38f};
         for (uint64_t i = first; i < end; ++i) {
-            const f3 &p = sorted[i];
-            mn = f3{std::min(mn.x, p.x), std::min(mn.y, p.y), std::min(mn.z, p.z)};
-            mx = f3{std::max(mx.x, p.x), std::max(mx.y, p.y), std::max(mx.z, p.z)};
+            mn = min3(mn, sorted[i]);
+            mx = max3(mx, sorted[i]);
         }
         const f3 size{fmax_(mx.x - mn.x, 0.000001f), fmax_(mx.y - mn.y, 0.000001f),
                       fmax_(mx.z - mn.z, 0.000001f)};

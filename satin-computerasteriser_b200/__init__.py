@@ -28,7 +28,11 @@ __all__ = ["Context", "ComputeRasteriserConfiguration", "ComputeRasteriserCapaci
            "ComputeRasteriserPointCloud", "ComputeRasteriser", "PackedPointCloud",
            "PerspectiveCamera", "CRError", "BATCH_DTYPE", "FILE_DTYPE", "PIXEL_DTYPE",
            "VISIBLE_DTYPE", "computeRasteriserThreadsPerGroup", "MODE_HQS", "MODE_NEAREST",
-           "identity_files", "matrix_multiply"]
+           "identity_files", "matrix_multiply", "GPUPacker", "PackInput", "DeviceBuffer",
+           "HostBuffer", "TerrainParams", "synth_terrain", "synth_lattice", "terrain_height",
+           "PASS_NAMES"]
+
+PASS_NAMES = ("clear", "cull", "depth", "color", "resolve", "hole_fill")
 
 computeRasteriserThreadsPerGroup = 128
 MODE_HQS = 0      # ComputeRasteriserMode.highQualityAverage
@@ -91,6 +95,17 @@ class Context:
         N.check(N.lib().cr_context_stream(self._h, C.byref(s)))
         return s.value or 0
 
+    def set_profiling(self, enable: bool):
+        """Bracket every pass of every cr_render with CUDA events (ring of 256 frames)."""
+        N.check(N.lib().cr_context_set_profiling(self._h, int(enable)))
+
+    def pass_times(self, nframes: int = 256) -> np.ndarray:
+        """(frames, 6) device milliseconds per pass (PASS_NAMES order), oldest first."""
+        out = np.zeros((max(nframes, 1), len(PASS_NAMES)), np.float32)
+        got = C.c_int32()
+        N.check(N.lib().cr_context_pass_times(self._h, nframes, N.ptr(out), C.byref(got)))
+        return out[:got.value].copy()
+
     def close(self):
         if self._h:
             N.lib().cr_context_destroy(self._h)
@@ -101,6 +116,117 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+class DeviceBuffer:
+    """Device memory owned through the C ABI (cr_buffer_*); exposes
+    __cuda_array_interface__ so it can be handed to the packer or to torch."""
+
+    def __init__(self, context: Context, nbytes: int, shape=None, dtype=np.uint8):
+        self.context = context
+        self.nbytes = int(nbytes)
+        self.dtype = np.dtype(dtype)
+        self.shape = tuple(shape) if shape is not None else (self.nbytes // self.dtype.itemsize,)
+        p = C.c_void_p()
+        N.check(N.lib().cr_buffer_create(context.handle, self.nbytes, C.byref(p)))
+        self.ptr = p.value
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": self.shape, "typestr": self.dtype.str, "data": (self.ptr, False),
+                "version": 3, "strides": None}
+
+    def upload(self, host: np.ndarray):
+        h = np.ascontiguousarray(host)
+        N.check(N.lib().cr_buffer_upload(self.context.handle, C.c_void_p(self.ptr), N.ptr(h),
+                                         min(h.nbytes, self.nbytes)))
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.shape, self.dtype)
+        N.check(N.lib().cr_buffer_download(self.context.handle, N.ptr(out), C.c_void_p(self.ptr),
+                                           out.nbytes))
+        return out
+
+    def close(self):
+        if self.ptr:
+            N.lib().cr_buffer_destroy(self.context.handle, C.c_void_p(self.ptr))
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HostBuffer:
+    """Pinned (page-locked) host memory as a numpy array (cr_host_alloc)."""
+
+    def __init__(self, shape, dtype=np.uint8):
+        dt = np.dtype(dtype)
+        n = int(np.prod(shape)) * dt.itemsize
+        p = C.c_void_p()
+        N.check(N.lib().cr_host_alloc(n, C.byref(p)))
+        self._p = p
+        buf = (C.c_uint8 * max(n, 1)).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
+
+    def close(self):
+        if self._p:
+            self.array = None
+            N.lib().cr_host_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class TerrainParams:
+    """cr_synth_terrain: the 4 km x 4 km fractal heightfield workload."""
+    seed: int = 0xC0FFEE02
+    extent: float = 4000.0
+    amplitude: float = 200.0
+    baseWavelength: float = 1500.0
+    octaves: int = 6
+    lacunarity: float = 2.0
+    gain: float = 0.5
+    outlierFraction: float = 0.05
+    outlierMargin: float = 50.0
+    colorNoiseSigma: float = 10.0
+
+    def to_c(self) -> N.cr_synth_terrain:
+        return N.cr_synth_terrain(self.seed, self.extent, self.amplitude, self.baseWavelength,
+                                  self.octaves, self.lacunarity, self.gain, self.outlierFraction,
+                                  self.outlierMargin, self.colorNoiseSigma)
+
+
+def terrain_height(params: TerrainParams, x: float, y: float) -> float:
+    t = params.to_c()
+    return float(N.lib().cr_synth_terrain_height(C.byref(t), float(x), float(y)))
+
+
+def synth_terrain(context: Context, params: TerrainParams, count: int,
+                  out: DeviceBuffer | None = None, first: int = 0) -> DeviceBuffer:
+    """count 16-byte records {x, y, z, rgba8} of the heightfield in device memory."""
+    buf = out or DeviceBuffer(context, count * 16, (count, 4), np.float32)
+    t = params.to_c()
+    N.check(N.lib().cr_synth_terrain_points(context.handle, C.byref(t), first, count,
+                                            C.c_void_p(buf.ptr)))
+    return buf
+
+
+def synth_lattice(context: Context, n_axis: int, seed: int = 0xC0FFEE01, lo: float = -1.0,
+                  hi: float = 1.0, jitter: float = 0.002) -> DeviceBuffer:
+    """n_axis^3 jittered lattice records {x, y, z, rgba8} in device memory."""
+    count = n_axis ** 3
+    buf = DeviceBuffer(context, count * 16, (count, 4), np.float32)
+    N.check(N.lib().cr_synth_lattice_points(context.handle, seed, n_axis, lo, hi, jitter,
+                                            C.c_void_p(buf.ptr)))
+    return buf
 
 
 @dataclass
@@ -298,6 +424,21 @@ class ComputeRasteriserPointCloud:
         if packed.batchCount > 0:
             self._upload_packed(packed)
 
+    def replacePackedPointCloudGPU(self, packer: "GPUPacker", positions=None, colors=None,
+                                   count=None, records=None):
+        """replacePackedPointCloud(packer:queue:positions:colors:count:) (GPUPacker.swift:507-519)."""
+        return packer.pack(positions, colors, count, into=self, records=records)
+
+    def addRawChunksGPU(self, packer: "GPUPacker", chunks, maxConcurrent: int = 1) -> list[int]:
+        """addRawChunksGPU(packer:queue:chunks:maxConcurrent:) (GPUPacker.swift:545-577):
+        chunks are (positions, colors) pairs or PackInput objects."""
+        return packer.addRawChunks(self, chunks)
+
+    def _sync_capacity(self):
+        info = self._info()
+        self._capacity = ComputeRasteriserCapacity(info.capacity.maxResidentBatches,
+                                                   info.capacity.pointsPerBatch)
+
     def _upload_packed(self, packed: PackedPointCloud):
         self.addBatches(packed.xyzLow, packed.xyzMed, packed.xyzHigh, packed.colors,
                         packed.levels, packed.batches)
@@ -348,6 +489,110 @@ class ComputeRasteriserPointCloud:
             self.close()
         except Exception:
             pass
+
+
+class PackInput:
+    """Raw points for the GPU packer: one of
+      * positions (n, 3) float32 (12-byte stride) or (n, 4) float32 (the
+        reference's 16-byte float3 slots), with colours (n, 4) float32 RGBA
+        in [0, 1] or (n,) uint32 packed RGBA8;
+      * records: (n, 4) of 16-byte records {float x, y, z; uint32 rgba8}
+        given as a float32 or uint32 view.
+    Arrays may live on the host (numpy) or on the device (any object with
+    __cuda_array_interface__, e.g. a CUDA torch tensor)."""
+
+    def __init__(self, positions=None, colors=None, records=None):
+        self._keep = []
+        if records is not None:
+            base, dev, n, row = self._view(records)
+            if row != 16:
+                raise CRError(1, "records must be 16 bytes each")
+            self.on_device, self.count = dev, n
+            self.c = N.cr_pack_input(base, 16, base + 12, 16, 1)
+            return
+        pb, pdev, n, prow = self._view(positions)
+        cb, cdev, nc, crow = self._view(colors)
+        if pdev != cdev:
+            raise CRError(1, "positions and colors must both be host or both device arrays")
+        if n != nc:
+            raise CRError(1, "positions and colors must have the same count")
+        if prow not in (12, 16):
+            raise CRError(1, "positions must be (n, 3) or (n, 4) float32")
+        fmt = 1 if crow == 4 else 0
+        if crow not in (4, 16):
+            raise CRError(1, "colors must be (n, 4) float32 or (n,) uint32 RGBA8")
+        self.on_device, self.count = pdev, n
+        self.c = N.cr_pack_input(pb, prow, cb, crow, fmt)
+
+    def _view(self, a):
+        if hasattr(a, "__cuda_array_interface__"):
+            ai = a.__cuda_array_interface__
+            shape = ai["shape"]
+            itemsize = np.dtype(ai["typestr"]).itemsize
+            if ai.get("strides") not in (None,) and ai["strides"] is not None:
+                exp = [itemsize]
+                for d in reversed(shape[1:]):
+                    exp.insert(0, exp[0] * d)
+                if tuple(ai["strides"]) != tuple(exp):
+                    raise CRError(1, "device arrays must be C-contiguous")
+            row = itemsize * (int(np.prod(shape[1:])) if len(shape) > 1 else 1)
+            self._keep.append(a)
+            return int(ai["data"][0]), True, int(shape[0]) if shape else 0, row
+        arr = np.ascontiguousarray(a)
+        if arr.dtype == np.float64:
+            arr = arr.astype(np.float32)
+        self._keep.append(arr)
+        row = arr.dtype.itemsize * (int(np.prod(arr.shape[1:])) if arr.ndim > 1 else 1)
+        return int(arr.ctypes.data), False, int(arr.shape[0]) if arr.ndim else 0, row
+
+
+class GPUPacker:
+    """GPUPacker (GPUPacker.swift:27-392): packs raw points on the GPU straight
+    into a cloud's slot pool, decode-identical to the CPU pack.
+
+    mortonBits = 10 reproduces the reference's 30-bit Morton order;
+    mortonBits = 21 sorts 63-bit keys (21 bits per axis)."""
+
+    def __init__(self, context: Context, lodLevels: int = 4, coarseVoxelDivisions: int = 64,
+                 mortonBits: int = 10):
+        self.context = context
+        self.lodLevels = max(1, min(int(lodLevels), 8))
+        self.coarseVoxelDivisions = max(1, int(coarseVoxelDivisions))
+        self.mortonBits = int(mortonBits)
+
+    def _params(self) -> N.cr_pack_params:
+        return N.cr_pack_params(self.lodLevels, self.coarseVoxelDivisions, self.mortonBits)
+
+    def pack(self, positions=None, colors=None, count=None, into=None, records=None,
+             sourceIndices: bool = False):
+        """pack(positions:colors:count:into:commandBuffer:) (GPUPacker.swift:140-160),
+        synchronous.  Returns the source-index permutation when asked."""
+        if into is None:
+            raise CRError(1, "into (a ComputeRasteriserPointCloud) is required")
+        inp = PackInput(positions, colors, records)
+        n = inp.count if count is None else int(count)
+        if n > inp.count:
+            raise CRError(1, "count exceeds the input length")
+        src = np.zeros(max(n, 1), np.uint32) if sourceIndices else None
+        N.check(N.lib().cr_pack(self.context.handle, into.handle, C.byref(inp.c), n,
+                                C.byref(self._params()), int(inp.on_device), N.ptr(src)))
+        into._sync_capacity()
+        return src[:n] if sourceIndices else None
+
+    def addRawChunks(self, cloud, chunks) -> list[int]:
+        """The packing half of addRawChunksGPU (GPUPacker.swift:545-577)."""
+        inputs = [c if isinstance(c, PackInput) else PackInput(*c) for c in chunks]
+        if len({i.on_device for i in inputs}) > 1:
+            raise CRError(1, "chunks must all be host or all be device arrays")
+        arr = (N.cr_pack_input * max(len(inputs), 1))(*[i.c for i in inputs])
+        counts = np.array([i.count for i in inputs] or [0], np.uint64)
+        firsts = np.zeros(max(len(inputs), 1), np.int32)
+        placed = C.c_uint32()
+        on_dev = int(inputs[0].on_device) if inputs else 0
+        N.check(N.lib().cr_pack_chunks(self.context.handle, cloud.handle, arr, N.ptr(counts),
+                                       len(inputs), C.byref(self._params()), on_dev,
+                                       N.ptr(firsts), C.byref(placed)))
+        return firsts[:placed.value].tolist()
 
 
 class _Frame:
@@ -506,9 +751,13 @@ class ComputeRasteriser:
                                   C.byref(cfg), C.byref(cam)))
 
     # --- outputs (row 0 = top of the viewport) ---
-    def outputRGBA8(self) -> np.ndarray:
+    def outputRGBA8(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The final RGBA8 image (row 0 at the top); `out` may be a pinned HostBuffer array."""
         f = self._require_frame()
-        out = np.zeros((f.height, f.width, 4), np.uint8)
+        if out is None:
+            out = np.zeros((f.height, f.width, 4), np.uint8)
+        elif out.nbytes < f.width * f.height * 4 or not out.flags.c_contiguous:
+            raise CRError(1, "out is too small or not contiguous")
         N.check(N.lib().cr_frame_read_rgba8(f.handle, N.ptr(out)))
         return out
 

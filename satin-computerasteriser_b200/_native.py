@@ -53,6 +53,24 @@ class cr_capacity(C.Structure):
     _fields_ = [("maxResidentBatches", C.c_uint32), ("pointsPerBatch", C.c_uint32)]
 
 
+class cr_pack_input(C.Structure):
+    _fields_ = [("positions", C.c_void_p), ("positionStrideBytes", C.c_uint32),
+                ("colors", C.c_void_p), ("colorStrideBytes", C.c_uint32),
+                ("colorFormat", C.c_int32)]
+
+
+class cr_pack_params(C.Structure):
+    _fields_ = [("lodLevels", C.c_int32), ("coarseVoxelDivisions", C.c_int32),
+                ("mortonBits", C.c_int32)]
+
+
+class cr_synth_terrain(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("extent", C.c_float), ("amplitude", C.c_float),
+                ("baseWavelength", C.c_float), ("octaves", C.c_int32),
+                ("lacunarity", C.c_float), ("gain", C.c_float), ("outlierFraction", C.c_float),
+                ("outlierMargin", C.c_float), ("colorNoiseSigma", C.c_float)]
+
+
 class cr_cloud_info(C.Structure):
     _fields_ = [("capacity", cr_capacity), ("residentBatchCount", C.c_uint32),
                 ("pointCount", C.c_uint64), ("freeSlotCount", C.c_uint32),
@@ -100,6 +118,23 @@ PROTOTYPES = {
     "cr_frame_read_nearest_index_rows": (C.c_int, [P, C.c_int, C.c_int, P]),
     "cr_pick": (C.c_int, [P, P, P, P, C.POINTER(cr_config), C.POINTER(cr_camera), C.c_int,
                           C.POINTER(u32), C.POINTER(C.c_int)]),
+    "cr_pack_params_default": (C.c_int, [C.POINTER(cr_pack_params)]),
+    "cr_buffer_create": (C.c_int, [P, u64, VP]),
+    "cr_buffer_destroy": (C.c_int, [P, P]),
+    "cr_buffer_upload": (C.c_int, [P, P, P, u64]),
+    "cr_buffer_download": (C.c_int, [P, P, P, u64]),
+    "cr_host_alloc": (C.c_int, [u64, VP]),
+    "cr_host_free": (C.c_int, [P]),
+    "cr_context_set_profiling": (C.c_int, [P, C.c_int]),
+    "cr_context_pass_times": (C.c_int, [P, i32, P, C.POINTER(i32)]),
+    "cr_synth_terrain_default": (C.c_int, [C.POINTER(cr_synth_terrain)]),
+    "cr_synth_terrain_height": (C.c_float, [C.POINTER(cr_synth_terrain), C.c_float, C.c_float]),
+    "cr_synth_terrain_points": (C.c_int, [P, C.POINTER(cr_synth_terrain), u64, u64, P]),
+    "cr_synth_lattice_points": (C.c_int, [P, u64, u32, C.c_float, C.c_float, C.c_float, P]),
+    "cr_pack": (C.c_int, [P, P, C.POINTER(cr_pack_input), u64, C.POINTER(cr_pack_params),
+                          C.c_int, P]),
+    "cr_pack_chunks": (C.c_int, [P, P, P, P, u32, C.POINTER(cr_pack_params), C.c_int, P,
+                                 C.POINTER(u32)]),
 }
 
 _lib = None

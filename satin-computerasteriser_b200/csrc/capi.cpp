@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "cr_internal.h"
+#include "cr_pack.h"
 
 // ---------------------------------------------------------------------------
 // Errors
@@ -363,10 +364,12 @@ CR_API cr_status cr_context_create(int device, cr_context **out) {
     if (prop.major < 10)
         return fail(CR_ERR_NO_DEVICE, "this library is built for sm_100a (B200) devices");
     auto *ctx = new cr_context();
+    ctx->pack = new PackScratch();
     ctx->device = device;
     ctx->sm_count = prop.multiProcessorCount;
     e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
+        delete ctx->pack;
         delete ctx;
         return cri::cuda_fail(e, "cudaStreamCreateWithFlags");
     }
@@ -378,6 +381,14 @@ CR_API cr_status cr_context_destroy(cr_context *ctx) {
     if (!ctx) return CR_OK;
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    for (auto &fr : ctx->pass_ev)
+        for (auto &pe : fr)
+            for (auto &e : pe)
+                if (e) cudaEventDestroy(e);
+    if (ctx->pack) {
+        pack_scratch_free(*ctx->pack);
+        delete ctx->pack;
+    }
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CR_OK;
@@ -725,23 +736,43 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
     const size_t npix = (size_t)W * H;
     ResolveUniforms ru{W, H, {cfg->backgroundColor[0], cfg->backgroundColor[1],
                               cfg->backgroundColor[2], cfg->backgroundColor[3]}};
+    if (ctx->profiling) {
+        ctx->prof_frame = (ctx->prof_frame + 1) % cr_context::kProfRing;
+        ctx->prof_count += 1;
+        for (int p = 0; p < CR_PASS_COUNT; ++p) ctx->pass_recorded[ctx->prof_frame][p] = false;
+    }
     if (cfg->mode == CR_MODE_HIGH_QUALITY_AVERAGE) {
         // encodeHighQualityAverage (ComputeRasteriser.swift:322-456).
-        CR_CUDA(cudaMemsetAsync(f->d_depth, 0, npix * 4, s));
-        CR_CUDA(cudaMemsetAsync(f->d_accum, 0, npix * 16, s));
+        {
+            PassTimer pt(ctx, CR_PASS_CLEAR);
+            CR_CUDA(cudaMemsetAsync(f->d_depth, 0, npix * 4, s));
+            CR_CUDA(cudaMemsetAsync(f->d_accum, 0, npix * 16, s));
+        }
         std::vector<cr_cloud *> resident;
         for (uint32_t i = 0; i < nclouds; ++i)
             if (clouds[i]->resident > 0) resident.push_back(clouds[i]);
         const CullUniforms cu = make_cull_uniforms(cfg, cam, W, H);
         const RasterUniforms rau = make_raster_uniforms(cfg, cam, W, H);
         const RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
-        for (cr_cloud *c : resident)
-            if ((st = launch_cull(c, cu, s))) return st;
-        for (cr_cloud *c : resident)
-            if ((st = launch_raster(c, PASS_DEPTH, rau, t, s))) return st;
-        for (cr_cloud *c : resident)
-            if ((st = launch_raster(c, PASS_COLOR, rau, t, s))) return st;
-        if ((st = launch_resolve_hqs(f, ru, s))) return st;
+        {
+            PassTimer pt(ctx, CR_PASS_CULL);
+            for (cr_cloud *c : resident)
+                if ((st = launch_cull(c, cu, s))) return st;
+        }
+        {
+            PassTimer pt(ctx, CR_PASS_DEPTH);
+            for (cr_cloud *c : resident)
+                if ((st = launch_raster(c, PASS_DEPTH, rau, t, s))) return st;
+        }
+        {
+            PassTimer pt(ctx, CR_PASS_COLOR);
+            for (cr_cloud *c : resident)
+                if ((st = launch_raster(c, PASS_COLOR, rau, t, s))) return st;
+        }
+        {
+            PassTimer pt(ctx, CR_PASS_RESOLVE);
+            if ((st = launch_resolve_hqs(f, ru, s))) return st;
+        }
         f->last_mode = 0;
     } else {
         // encodeNearestPoint (ComputeRasteriser.swift:483-497): first resident cloud only.
@@ -749,15 +780,36 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
         for (uint32_t i = 0; i < nclouds && !first; ++i)
             if (clouds[i]->resident > 0) first = clouds[i];
         if (first) {
-            if ((st = nearest_index_pass(ctx, f, first, cfg, cam))) return st;
-            if ((st = launch_resolve_nearest(f, first->d_colors, ru, s))) return st;
+            {
+                PassTimer pt(ctx, CR_PASS_CLEAR);
+                CR_CUDA(cudaMemsetAsync(f->d_nearest, 0, npix * sizeof(unsigned long long), s));
+            }
+            {
+                PassTimer pt(ctx, CR_PASS_CULL);
+                if ((st = launch_cull(first, make_cull_uniforms(cfg, cam, W, H), s))) return st;
+            }
+            {
+                PassTimer pt(ctx, CR_PASS_DEPTH);
+                const RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
+                if ((st = launch_raster(first, PASS_NEAREST, make_raster_uniforms(cfg, cam, W, H),
+                                        t, s)))
+                    return st;
+            }
+            {
+                PassTimer pt(ctx, CR_PASS_RESOLVE);
+                if ((st = launch_resolve_nearest(f, first->d_colors, ru, s))) return st;
+            }
             f->last_mode = 1;
         }
     }
     // encodeHoleFill (ComputeRasteriser.swift:298-320) always starts from the
     // resolve target.
     f->final_rgba = 0;
-    return launch_hole_fill(f, std::max(0, cfg->holeFillIterations), s);
+    if (cfg->holeFillIterations > 0) {
+        PassTimer pt(ctx, CR_PASS_HOLE_FILL);
+        return launch_hole_fill(f, cfg->holeFillIterations, s);
+    }
+    return CR_OK;
 }
 
 static cr_status read_plane(cr_frame *f, void *out, const void *src, size_t bytes) {
@@ -871,6 +923,247 @@ CR_API cr_status cr_pick(cr_context *ctx, cr_frame *f, cr_cloud *cloud, const fl
         *found_out = 1;
     }
     return CR_OK;
+}
+
+// ---------------------------------------------------------------- buffers
+CR_API cr_status cr_buffer_create(cr_context *ctx, uint64_t bytes, void **out) {
+    if (!ctx || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    DeviceGuard g(ctx->device);
+    return dalloc(reinterpret_cast<uint8_t **>(out), bytes);
+}
+
+CR_API cr_status cr_buffer_destroy(cr_context *ctx, void *p) {
+    if (!ctx) return fail(CR_ERR_INVALID_ARGUMENT, "ctx is null");
+    if (!p) return CR_OK;
+    DeviceGuard g(ctx->device);
+    CR_CUDA(cudaStreamSynchronize(ctx->stream));
+    CR_CUDA(cudaFree(p));
+    return CR_OK;
+}
+
+CR_API cr_status cr_buffer_upload(cr_context *ctx, void *dst, const void *src, uint64_t bytes) {
+    if (!ctx || (bytes && (!dst || !src))) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    if (!bytes) return CR_OK;
+    DeviceGuard g(ctx->device);
+    CR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    CR_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CR_OK;
+}
+
+CR_API cr_status cr_buffer_download(cr_context *ctx, void *dst, const void *src, uint64_t bytes) {
+    if (!ctx || (bytes && (!dst || !src))) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    if (!bytes) return CR_OK;
+    DeviceGuard g(ctx->device);
+    CR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CR_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CR_OK;
+}
+
+CR_API cr_status cr_host_alloc(uint64_t bytes, void **out) {
+    if (!out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    CR_CUDA(cudaMallocHost(out, bytes ? bytes : 16));
+    return CR_OK;
+}
+
+CR_API cr_status cr_host_free(void *p) {
+    if (p) CR_CUDA(cudaFreeHost(p));
+    return CR_OK;
+}
+
+// ---------------------------------------------------------------- profiling
+CR_API cr_status cr_context_set_profiling(cr_context *ctx, int enable) {
+    if (!ctx) return fail(CR_ERR_INVALID_ARGUMENT, "ctx is null");
+    DeviceGuard g(ctx->device);
+    if (enable && !ctx->pass_ev[0][0][0])
+        for (auto &fr : ctx->pass_ev)
+            for (auto &pe : fr)
+                for (auto &e : pe) CR_CUDA(cudaEventCreate(&e));
+    CR_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->profiling = enable != 0;
+    ctx->prof_frame = -1;
+    ctx->prof_count = 0;
+    for (auto &fr : ctx->pass_recorded)
+        for (bool &r : fr) r = false;
+    return CR_OK;
+}
+
+CR_API cr_status cr_context_pass_times(cr_context *ctx, int32_t nframes, float *ms,
+                                       int32_t *frames_out) {
+    if (!ctx || !frames_out || (nframes > 0 && !ms))
+        return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    DeviceGuard g(ctx->device);
+    const int64_t avail = std::min<int64_t>(ctx->prof_count, cr_context::kProfRing);
+    const int n = (int)std::min<int64_t>(std::max(nframes, 0), avail);
+    *frames_out = n;
+    for (int k = 0; k < n; ++k) {
+        // k = 0 is the oldest of the last n frames.
+        const int slot = (ctx->prof_frame - (n - 1 - k) + cr_context::kProfRing) % cr_context::kProfRing;
+        for (int p = 0; p < CR_PASS_COUNT; ++p) {
+            float &out = ms[(size_t)k * CR_PASS_COUNT + p];
+            out = 0.0f;
+            if (!ctx->pass_recorded[slot][p]) continue;
+            CR_CUDA(cudaEventSynchronize(ctx->pass_ev[slot][p][1]));
+            CR_CUDA(cudaEventElapsedTime(&out, ctx->pass_ev[slot][p][0], ctx->pass_ev[slot][p][1]));
+        }
+    }
+    return CR_OK;
+}
+
+// ---------------------------------------------------------------- packer
+CR_API cr_status cr_pack_params_default(cr_pack_params *out) {
+    if (!out) return fail(CR_ERR_INVALID_ARGUMENT, "out is null");
+    out->lodLevels = 4;             // PackedPointCloudFixtures.defaultLODLevels
+    out->coarseVoxelDivisions = 64; // PackedPointCloudFixtures.defaultCoarseVoxelDivisions
+    out->mortonBits = 10;
+    return CR_OK;
+}
+
+static cr_status validate_pack(cr_context *ctx, cr_cloud *cloud, const cr_pack_params *prm) {
+    if (!ctx || !cloud || !prm) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    if (cloud->ctx != ctx) return fail(CR_ERR_INVALID_ARGUMENT, "cloud belongs to another context");
+    if (prm->mortonBits != 10 && prm->mortonBits != 21)
+        return fail(CR_ERR_INVALID_ARGUMENT, "mortonBits must be 10 or 21");
+    // GPUPacker.swift:215: uint16 cumulative LOD counts.
+    if (cloud->cap.pointsPerBatch > 65535)
+        return fail(CR_ERR_INVALID_ARGUMENT, "pointsPerBatch must fit the uint16 LOD prefix counts");
+    return CR_OK;
+}
+
+static cr_status validate_input(const cr_pack_input *in) {
+    if (!in || !in->positions || !in->colors) return fail(CR_ERR_INVALID_ARGUMENT, "null input");
+    if (in->positionStrideBytes < 12 || (in->positionStrideBytes & 3))
+        return fail(CR_ERR_INVALID_ARGUMENT, "positionStrideBytes must be >= 12 and a multiple of 4");
+    if (in->colorFormat != CR_COLOR_F32X4 && in->colorFormat != CR_COLOR_RGBA8)
+        return fail(CR_ERR_INVALID_ARGUMENT, "unknown colorFormat");
+    const uint32_t cs = in->colorFormat == CR_COLOR_RGBA8 ? 4u : 16u;
+    if (in->colorStrideBytes < cs || (in->colorStrideBytes & 3))
+        return fail(CR_ERR_INVALID_ARGUMENT, "colorStrideBytes too small or unaligned");
+    if (((uintptr_t)in->positions & 3) || ((uintptr_t)in->colors & 3))
+        return fail(CR_ERR_INVALID_ARGUMENT, "input pointers must be 4-byte aligned");
+    return CR_OK;
+}
+
+// Adopt GPU-written batches into the host mirror (adoptGPUBatchBounds /
+// finalizeGPUChunk, ComputeRasteriserPointCloud.swift:313-363).
+static cr_status adopt_batches(cr_cloud *c, uint32_t first, uint32_t n) {
+    if (n == 0) return CR_OK;
+    CR_CUDA(cudaMemcpyAsync(c->mirror.data() + first, c->d_batches + first,
+                            (size_t)n * sizeof(cr_raster_batch), cudaMemcpyDeviceToHost,
+                            c->ctx->stream));
+    CR_CUDA(cudaStreamSynchronize(c->ctx->stream));
+    return CR_OK;
+}
+
+CR_API cr_status cr_pack(cr_context *ctx, cr_cloud *c, const cr_pack_input *in, uint64_t count,
+                         const cr_pack_params *prm, int on_device, uint32_t *src_idx) {
+    cr_status st = validate_pack(ctx, c, prm);
+    if (st) return st;
+    DeviceGuard g(ctx->device);
+    // GPUPacker.pack: an empty input clears the cloud (GPUPacker.swift:147-150).
+    if (count == 0) return cr_cloud_clear(c);
+    if ((st = validate_input(in))) return st;
+    if (count >= 0xffffffffull) return fail(CR_ERR_CAPACITY, "count must be below 2^32-1");
+    // prepareForGPUPack (ComputeRasteriserPointCloud.swift:278-307).
+    const uint32_t ppb = c->cap.pointsPerBatch;
+    const uint64_t nb64 = std::max<uint64_t>(1, (count + ppb - 1) / ppb);
+    if (nb64 > c->cap.maxResidentBatches) {
+        if ((uint64_t)nb64 * ppb >= 0xffffffffull)
+            return fail(CR_ERR_CAPACITY, "pool would exceed 2^32-1 points");
+        CR_CUDA(cudaStreamSynchronize(ctx->stream));
+        std::vector<cr_raster_file> keep = c->files;
+        if ((st = allocate_cloud(c, cr_capacity{(uint32_t)nb64, ppb}, keep.data(),
+                                 (uint32_t)keep.size())))
+            return st;
+    }
+    const uint32_t nb = (uint32_t)nb64;
+    for (uint32_t slot = 0; slot < c->cap.maxResidentBatches; ++slot) {
+        cr_raster_batch &b = c->mirror[slot];
+        if (slot < nb) {
+            b = cr_raster_batch{};
+            b.state = 1;
+            b.firstPoint = slot * ppb;
+            b.numPoints = (uint32_t)std::min<uint64_t>(ppb, count - (uint64_t)slot * ppb);
+        } else {
+            b.state = 0;
+            b.numPoints = 0;
+        }
+    }
+    c->free_slots.clear();
+    for (int64_t s2 = (int64_t)c->cap.maxResidentBatches - 1; s2 >= (int64_t)nb; --s2)
+        c->free_slots.push_back((int32_t)s2);
+    c->resident = nb;
+    c->points = count;
+    mark_dirty(c, 0, (int64_t)c->mirror.size() - 1);
+    if ((st = flush_mirror(c))) return st;
+    if ((st = pack_run(ctx, c, in, count, prm, on_device, 0, src_idx))) return st;
+    return adopt_batches(c, 0, nb);
+}
+
+// reserveContiguousSlots (ComputeRasteriserPointCloud.swift:330-346): first-fit run of
+// empty slots; the slots leave the free list and are marked resident provisionally.
+static int64_t reserve_contiguous(cr_cloud *c, uint32_t n) {
+    const uint32_t cap = c->cap.maxResidentBatches;
+    if (n == 0 || n > cap) return -1;
+    uint32_t s = 0;
+    while ((uint64_t)s + n <= cap) {
+        uint32_t k = 0;
+        while (k < n && c->mirror[s + k].state == 0) ++k;
+        if (k == n) {
+            std::vector<int32_t> keep;
+            keep.reserve(c->free_slots.size());
+            for (int32_t f : c->free_slots)
+                if (!((uint32_t)f >= s && (uint32_t)f < s + n)) keep.push_back(f);
+            c->free_slots.swap(keep);
+            for (uint32_t q = s; q < s + n; ++q) c->mirror[q].state = 1;
+            mark_dirty(c, s, (int64_t)s + n - 1);
+            return s;
+        }
+        s += k + 1;
+    }
+    return -1;
+}
+
+CR_API cr_status cr_pack_chunks(cr_context *ctx, cr_cloud *c, const cr_pack_input *chunks,
+                                const uint64_t *counts, uint32_t nchunks,
+                                const cr_pack_params *prm, int on_device, int32_t *first_slots,
+                                uint32_t *placed_out) {
+    cr_status st = validate_pack(ctx, c, prm);
+    if (st) return st;
+    if (!placed_out || (nchunks && (!chunks || !counts)))
+        return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    *placed_out = 0;
+    const uint32_t ppb = c->cap.pointsPerBatch;
+    for (uint32_t i = 0; i < nchunks; ++i) {
+        if (counts[i] == 0) continue;
+        if ((st = validate_input(&chunks[i]))) return st;
+        if (counts[i] >= 0xffffffffull) return fail(CR_ERR_CAPACITY, "chunk count too large");
+    }
+    DeviceGuard g(ctx->device);
+    struct Placed {
+        uint32_t first, nb, index;
+    };
+    std::vector<Placed> placed;
+    for (uint32_t i = 0; i < nchunks; ++i) {
+        if (counts[i] == 0) continue;
+        const uint64_t nb = std::max<uint64_t>(1, (counts[i] + ppb - 1) / ppb);
+        const int64_t first = reserve_contiguous(c, (uint32_t)std::min<uint64_t>(nb, UINT32_MAX));
+        if (first < 0) continue;
+        placed.push_back(Placed{(uint32_t)first, (uint32_t)nb, i});
+    }
+    for (const Placed &p : placed)
+        if ((st = pack_run(ctx, c, &chunks[p.index], counts[p.index], prm, on_device, p.first,
+                           nullptr)))
+            return st;
+    for (size_t k = 0; k < placed.size(); ++k) {
+        const Placed &p = placed[k];
+        if ((st = adopt_batches(c, p.first, p.nb))) return st;
+        c->resident += p.nb;
+        c->points += counts[p.index];
+        if (first_slots) first_slots[k] = (int32_t)p.first;
+    }
+    *placed_out = (uint32_t)placed.size();
+    return flush_mirror(c);
 }
 
 }  // extern "C"

@@ -39,11 +39,37 @@ enum CounterSlot : int {
     CNT_COUNT = 32
 };
 
+struct PackScratch;
+
 struct cr_context {
+    PackScratch *pack = nullptr;  // grow-only packer scratch
     int device = 0;
     cudaStream_t stream = nullptr;
     int sm_count = 0;
     int raster_blocks_per_sm = 0;  // occupancy of the persistent point passes
+    // Profiling: a ring of frames, each with a start/stop event per pass.
+    static constexpr int kProfRing = 256;
+    bool profiling = false;
+    int prof_frame = -1;      // ring index of the frame being recorded
+    int64_t prof_count = 0;   // frames recorded since profiling was enabled
+    cudaEvent_t pass_ev[kProfRing][CR_PASS_COUNT][2] = {};
+    bool pass_recorded[kProfRing][CR_PASS_COUNT] = {};
+};
+
+// Brackets one pass with profiling events when profiling is on.
+struct PassTimer {
+    cr_context *ctx;
+    int pass;
+    PassTimer(cr_context *c, int p) : ctx(c), pass(p) {
+        if (ctx->profiling)
+            cudaEventRecord(ctx->pass_ev[ctx->prof_frame][pass][0], ctx->stream);
+    }
+    ~PassTimer() {
+        if (ctx->profiling) {
+            cudaEventRecord(ctx->pass_ev[ctx->prof_frame][pass][1], ctx->stream);
+            ctx->pass_recorded[ctx->prof_frame][pass] = true;
+        }
+    }
 };
 
 struct cr_cloud {
@@ -137,3 +163,7 @@ cr_status launch_split_nearest(const unsigned long long *keys, uint32_t *depth_o
                                uint32_t *index_out, size_t n, cudaStream_t s);
 
 int raster_blocks_per_sm(int pass);
+
+cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, uint64_t count,
+                   const cr_pack_params *prm, int on_device, uint32_t first_slot,
+                   uint32_t *src_idx_host);

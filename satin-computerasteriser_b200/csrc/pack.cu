@@ -1,0 +1,540 @@
+// pack.cu — the GPU packer: raw points -> Morton-ordered, LOD-bucketed,
+// split-precision batches written straight into a cloud's slot pool.
+//
+// Restates GPUPacker.encodePack (GPUPacker.swift:204-392) and its kernels
+// (Pipelines/GPUPacker/Shaders.metal:41-414), which in turn mirror the CPU
+// PackedPointCloudFixtures.pack (PackedPointCloudFixtures.swift:30-344):
+//   1 bounds        global AABB (order-preserving flipped-bit min/max)
+//   2 morton        10 bits/axis (30-bit key) or 21 bits/axis (63-bit key)
+//   3 sort          stable LSD radix of (key, input index)      [radix.cu]
+//   4 gather        positions in Morton order, levels = maxLevel
+//   5 LOD           per level, coarsest first: dense voxel grid, atomicMin
+//                   of the Morton position claims a voxel for the first
+//                   eligible point in sorted order (the CPU's "first point
+//                   to occupy an empty voxel")
+//   6 batches       one CTA per batch: AABB, level histogram, stable
+//                   level-ascending scatter (warp ballots), RasterBatch with
+//                   the cumulative LOD counts
+//   7 emit          gather in final order, 30-bit quantisation into three
+//                   10-bit/axis words, colours, levels, source indices.
+// Host-side float math (scale, voxel sizes, grid dims) is compiled without
+// contraction and uses the same operation order as the CPU oracle.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cr_device.cuh"
+#include "cr_internal.h"
+#include "cr_pack.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint64_t kLodCellCap = 1ull << 28;  // 1 GiB of uint32 voxels
+
+__host__ __device__ __forceinline__ uint32_t flip(float f) {
+#ifdef __CUDA_ARCH__
+    const uint32_t b = __float_as_uint(f);
+#else
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+#endif
+    return b ^ ((b >> 31) ? 0xffffffffu : 0x80000000u);
+}
+__host__ __device__ __forceinline__ float unflip(uint32_t u) {
+    const uint32_t b = u ^ ((u >> 31) ? 0x80000000u : 0xffffffffu);
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(b);
+#else
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+#endif
+}
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+    uint32_t x = v & 0x3ffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+__device__ __forceinline__ unsigned long long spread21(unsigned long long v) {
+    unsigned long long x = v & 0x1fffffull;
+    x = (x | (x << 32)) & 0x1f00000000ffffull;
+    x = (x | (x << 16)) & 0x1f0000ff0000ffull;
+    x = (x | (x << 8)) & 0x100f00f00f00f00full;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+struct LoadArgs {
+    const uint8_t *pos;
+    uint32_t pos_stride;
+    const uint8_t *col;
+    uint32_t col_stride;
+    int col_format;
+};
+
+// Stage 0: raw input -> float4 positions + packed RGBA8 (GPUPacker/Shaders.metal:219-235
+// colour rule: uint(clamp(c, 0, 1) * 255), truncating).
+__global__ void __launch_bounds__(kThreads)
+    pack_load(LoadArgs a, uint64_t n, float4 *__restrict__ pos, uint32_t *__restrict__ col) {
+    const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const float *p = reinterpret_cast<const float *>(a.pos + i * a.pos_stride);
+    pos[i] = make_float4(p[0], p[1], p[2], 0.0f);
+    if (a.col_format == 1) {
+        col[i] = *reinterpret_cast<const uint32_t *>(a.col + i * a.col_stride);
+    } else {
+        const float *c = reinterpret_cast<const float *>(a.col + i * a.col_stride);
+        const uint32_t r = (uint32_t)(fminf(fmaxf(c[0], 0.0f), 1.0f) * 255.0f);
+        const uint32_t g = (uint32_t)(fminf(fmaxf(c[1], 0.0f), 1.0f) * 255.0f);
+        const uint32_t b = (uint32_t)(fminf(fmaxf(c[2], 0.0f), 1.0f) * 255.0f);
+        const uint32_t al = (uint32_t)(fminf(fmaxf(c[3], 0.0f), 1.0f) * 255.0f);
+        col[i] = r | (g << 8) | (b << 16) | (al << 24);
+    }
+}
+
+// Stage 1: global bounds (packBounds, GPUPacker/Shaders.metal:71-105).
+__global__ void __launch_bounds__(kThreads)
+    pack_bounds(const float4 *__restrict__ pos, uint64_t n, uint32_t *__restrict__ bounds) {
+    uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
+    for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * kThreads) {
+        const float4 p = pos[i];
+        const uint32_t f[3] = {flip(p.x), flip(p.y), flip(p.z)};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = min(mn[k], f[k]);
+            mx[k] = max(mx[k], f[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const uint32_t a = __reduce_min_sync(0xffffffffu, mn[k]);
+        const uint32_t b = __reduce_max_sync(0xffffffffu, mx[k]);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&bounds[k], a);
+            atomicMax(&bounds[3 + k], b);
+        }
+    }
+}
+
+struct MortonArgs {
+    float bmin[3];
+    float scale[3];
+    float top;
+};
+
+// Stage 2: Morton key + identity index (packMorton, GPUPacker/Shaders.metal:109-126).
+template <typename K>
+__global__ void __launch_bounds__(kThreads)
+    pack_morton(const float4 *__restrict__ pos, uint64_t n, MortonArgs m, K *__restrict__ keys,
+                uint32_t *__restrict__ idx) {
+    const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos[i];
+    const uint32_t qx = (uint32_t)fminf(fmaxf((p.x - m.bmin[0]) * m.scale[0], 0.0f), m.top);
+    const uint32_t qy = (uint32_t)fminf(fmaxf((p.y - m.bmin[1]) * m.scale[1], 0.0f), m.top);
+    const uint32_t qz = (uint32_t)fminf(fmaxf((p.z - m.bmin[2]) * m.scale[2], 0.0f), m.top);
+    if (sizeof(K) == 8)
+        keys[i] = (K)((spread21(qx) << 2) | (spread21(qy) << 1) | spread21(qz));
+    else
+        keys[i] = (K)((spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz));
+    idx[i] = (uint32_t)i;
+}
+
+// Stage 4: gather into Morton order, all levels at maxLevel (packLODInit).
+__global__ void __launch_bounds__(kThreads)
+    pack_gather(const float4 *__restrict__ pos, const uint32_t *__restrict__ idx, uint64_t n,
+                float4 *__restrict__ sorted, uint8_t *__restrict__ lv, uint8_t max_level) {
+    const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    sorted[i] = pos[idx[i]];
+    lv[i] = max_level;
+}
+
+struct LodArgs {
+    float bmin[3];
+    float inv;
+    uint32_t dims[3];
+    uint8_t max_level;
+    uint8_t level;
+};
+
+__device__ __forceinline__ uint64_t lod_cell(const float4 &p, const LodArgs &a) {
+    const float lx = (p.x - a.bmin[0]) * a.inv;
+    const float ly = (p.y - a.bmin[1]) * a.inv;
+    const float lz = (p.z - a.bmin[2]) * a.inv;
+    const uint32_t cx = min((uint32_t)max(0, (int)floorf(lx)), a.dims[0] - 1u);
+    const uint32_t cy = min((uint32_t)max(0, (int)floorf(ly)), a.dims[1] - 1u);
+    const uint32_t cz = min((uint32_t)max(0, (int)floorf(lz)), a.dims[2] - 1u);
+    return (uint64_t)cx + (uint64_t)a.dims[0] * ((uint64_t)cy + (uint64_t)a.dims[1] * cz);
+}
+
+// Stage 5 (packLODClaim / packLODAssign, GPUPacker/Shaders.metal:337-371).
+__global__ void __launch_bounds__(kThreads)
+    pack_lod_claim(const float4 *__restrict__ sorted, const uint8_t *__restrict__ lv, uint64_t n,
+                   LodArgs a, uint32_t *__restrict__ grid) {
+    const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n || lv[i] != a.max_level) return;
+    atomicMin(&grid[lod_cell(sorted[i], a)], (uint32_t)i);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    pack_lod_assign(const float4 *__restrict__ sorted, uint8_t *__restrict__ lv, uint64_t n,
+                    LodArgs a, const uint32_t *__restrict__ grid) {
+    const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n || lv[i] != a.max_level) return;
+    if (grid[lod_cell(sorted[i], a)] == (uint32_t)i) lv[i] = a.level;
+}
+
+// Stage 6: per batch AABB + stable level bucketing + RasterBatch
+// (packBatchAABB + packBucketLOD, GPUPacker/Shaders.metal:243-284, 383-414).
+__global__ void __launch_bounds__(kThreads)
+    pack_batches(const float4 *__restrict__ sorted, const uint8_t *__restrict__ lv, uint64_t n,
+                 uint32_t ppb, uint32_t first_slot, cr_raster_batch *__restrict__ batches,
+                 uint32_t *__restrict__ perm, uint8_t *__restrict__ lv_out) {
+    __shared__ uint32_t red[6][kThreads / 32];
+    __shared__ uint32_t cnt[8];
+    __shared__ uint32_t running[8];
+    __shared__ uint32_t wl[kThreads / 32][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t start = (uint64_t)blockIdx.x * ppb;
+    const uint64_t end = (start + ppb < n) ? start + ppb : n;
+    if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
+    for (uint64_t i = start + threadIdx.x; i < end; i += kThreads) {
+        const float4 p = sorted[i];
+        const uint32_t f[3] = {flip(p.x), flip(p.y), flip(p.z)};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = min(mn[k], f[k]);
+            mx[k] = max(mx[k], f[k]);
+        }
+        atomicAdd(&cnt[lv[i] & 7u], 1u);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const uint32_t a = __reduce_min_sync(0xffffffffu, mn[k]);
+        const uint32_t b = __reduce_max_sync(0xffffffffu, mx[k]);
+        if (lane == 0) {
+            red[k][warp] = a;
+            red[3 + k][warp] = b;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t m[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+        for (int w = 0; w < kThreads / 32; ++w)
+            for (int k = 0; k < 3; ++k) {
+                m[k] = min(m[k], red[k][w]);
+                m[3 + k] = max(m[3 + k], red[3 + k][w]);
+            }
+        uint32_t cum[8], acc = 0;
+        for (int l = 0; l < 8; ++l) {
+            running[l] = acc;
+            acc += cnt[l];
+            cum[l] = acc;
+        }
+        cr_raster_batch rb;
+        rb.state = 1;
+        rb.minX = unflip(m[0]);
+        rb.minY = unflip(m[1]);
+        rb.minZ = unflip(m[2]);
+        rb.maxX = unflip(m[3]);
+        rb.maxY = unflip(m[4]);
+        rb.maxZ = unflip(m[5]);
+        rb.numPoints = (uint32_t)(end - start);
+        rb.firstPoint = (first_slot + blockIdx.x) * ppb;
+        rb.fileIndex = 0;
+        rb.lodCum01 = cum[0] | (cum[1] << 16);
+        rb.lodCum23 = cum[2] | (cum[3] << 16);
+        rb.lodCum45 = cum[4] | (cum[5] << 16);
+        rb.lodCum67 = cum[6] | (cum[7] << 16);
+        rb.padding7 = 0;
+        rb.padding8 = 0;
+        batches[blockIdx.x] = rb;
+    }
+    __syncthreads();
+    const uint32_t lt = (1u << lane) - 1u;
+    for (uint64_t r0 = start; r0 < end; r0 += kThreads) {
+        const uint64_t i = r0 + threadIdx.x;
+        const bool v = i < end;
+        const uint32_t l = v ? (lv[i] & 7u) : 8u;
+        uint32_t my_rank = 0;
+#pragma unroll
+        for (uint32_t L = 0; L < 8; ++L) {
+            const uint32_t b = __ballot_sync(0xffffffffu, l == L);
+            if (lane == 0) wl[warp][L] = __popc(b);
+            if (l == L) my_rank = __popc(b & lt);
+        }
+        __syncthreads();
+        if (v) {
+            uint32_t before = running[l];
+            for (int w = 0; w < warp; ++w) before += wl[w][l];
+            const uint64_t dst = start + before + my_rank;
+            if (dst < end) {  // always true: the ranks come from the same levels
+                perm[dst] = (uint32_t)i;
+                lv_out[dst] = lv[i];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 8) {
+            uint32_t s = 0;
+            for (int w = 0; w < kThreads / 32; ++w) s += wl[w][threadIdx.x];
+            running[threadIdx.x] += s;
+        }
+        __syncthreads();
+    }
+}
+
+// Stage 7: final order, quantisation (packQuantize, GPUPacker/Shaders.metal:288-309).
+__global__ void __launch_bounds__(kThreads)
+    pack_emit(uint64_t n, uint32_t ppb, const uint32_t *__restrict__ perm,
+              const uint32_t *__restrict__ idx_sorted, const float4 *__restrict__ pos,
+              const uint32_t *__restrict__ col, const uint8_t *__restrict__ lv_out,
+              const cr_raster_batch *__restrict__ batches, uint32_t *__restrict__ low,
+              uint32_t *__restrict__ med, uint32_t *__restrict__ high,
+              uint32_t *__restrict__ colors, uint8_t *__restrict__ levels,
+              uint32_t *__restrict__ src_out) {
+    const uint64_t j = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t pj = perm[j];
+    if (pj >= n) return;  // unreachable for a complete permutation
+    const uint32_t orig = idx_sorted[pj];
+    if (orig >= n) return;
+    const float4 p = pos[orig];
+    const cr_raster_batch &b = batches[j / ppb];
+    const float sx = fmaxf(b.maxX - b.minX, 0.000001f);
+    const float sy = fmaxf(b.maxY - b.minY, 0.000001f);
+    const float sz = fmaxf(b.maxZ - b.minZ, 0.000001f);
+    const float nx = fminf(fmaxf((p.x - b.minX) / sx, 0.0f), 0.99999994f);
+    const float ny = fminf(fmaxf((p.y - b.minY) / sy, 0.0f), 0.99999994f);
+    const float nz = fminf(fmaxf((p.z - b.minZ) / sz, 0.0f), 0.99999994f);
+    // Float(2^30 - 1) rounds to 2^30 in f32.
+    const uint32_t qx = (uint32_t)(nx * 1073741824.0f);
+    const uint32_t qy = (uint32_t)(ny * 1073741824.0f);
+    const uint32_t qz = (uint32_t)(nz * 1073741824.0f);
+    low[j] = ((qx >> 20) & 1023u) | (((qy >> 20) & 1023u) << 10) | (((qz >> 20) & 1023u) << 20);
+    med[j] = ((qx >> 10) & 1023u) | (((qy >> 10) & 1023u) << 10) | (((qz >> 10) & 1023u) << 20);
+    high[j] = (qx & 1023u) | ((qy & 1023u) << 10) | ((qz & 1023u) << 20);
+    colors[j] = col[orig];
+    levels[j] = lv_out[j];
+    if (src_out) src_out[j] = orig;
+}
+
+unsigned grid_for(uint64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+template <typename T>
+cr_status grow(T **p, uint64_t &cap, uint64_t want_elems) {
+    if (*p && cap >= want_elems) return CR_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    cudaError_t e = cudaMalloc((void **)p, std::max<uint64_t>(want_elems, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cap = 0;
+        return cri::cuda_fail(e, "cudaMalloc (pack scratch)");
+    }
+    cap = want_elems;
+    return CR_OK;
+}
+
+// Keys are sized for 64-bit words so either key width fits.
+cr_status ensure_points(PackScratch &s, uint64_t n) {
+    if (s.cap_points >= n && s.keys[0]) return CR_OK;
+    pack_scratch_free(s);
+    const uint64_t m = std::max<uint64_t>(n, 1) + 64;
+    cudaError_t e;
+#define ALLOC(ptr, bytes)                                                   \
+    do {                                                                    \
+        e = cudaMalloc((void **)&(ptr), (bytes));                           \
+        if (e != cudaSuccess) {                                             \
+            pack_scratch_free(s);                                           \
+            return cri::cuda_fail(e, "cudaMalloc (pack scratch)");          \
+        }                                                                   \
+    } while (0)
+    ALLOC(s.pos, m * sizeof(float4));
+    ALLOC(s.col, m * 4);
+    ALLOC(s.keys[0], m * 8);
+    ALLOC(s.keys[1], m * 8);
+    ALLOC(s.idx[0], m * 4);
+    ALLOC(s.idx[1], m * 4);
+    ALLOC(s.sorted, m * sizeof(float4));
+    ALLOC(s.lv_morton, (m + 15) & ~15ull);
+    ALLOC(s.lv_out, (m + 15) & ~15ull);
+    ALLOC(s.perm, m * 4);
+    ALLOC(s.src_idx, m * 4);
+    ALLOC(s.digit_total, 256 * 4);
+    ALLOC(s.bounds, 8 * 4);
+#undef ALLOC
+    s.cap_points = n;
+    return CR_OK;
+}
+
+}  // namespace
+
+void pack_scratch_free(PackScratch &s) {
+    void *ptrs[] = {s.raw, s.pos, s.col, s.keys[0], s.keys[1], s.idx[0], s.idx[1], s.sorted,
+                    s.lv_morton, s.lv_out, s.perm, s.grid, s.hist, s.digit_total, s.bounds,
+                    s.src_idx};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    s = PackScratch{};
+}
+
+// Packs `count` points into slots [first_slot, first_slot + ceil(count/ppb)) of
+// the cloud's pool.  Enqueues on the context stream; one synchronisation reads
+// the global bounds back to size the Morton scale and the LOD grid.
+cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, uint64_t count,
+                   const cr_pack_params *prm, int on_device, uint32_t first_slot,
+                   uint32_t *src_idx_host) {
+    cudaStream_t s = ctx->stream;
+    PackScratch &sc = *ctx->pack;
+    const bool wide = prm->mortonBits == 21;
+    cr_status st = ensure_points(sc, count);
+    if (st) return st;
+    const uint32_t ppb = cloud->cap.pointsPerBatch;
+    const uint32_t nb = (uint32_t)((count + ppb - 1) / ppb);
+
+    // Stage 0: stage host input (one copy when the colour sits inside the position record).
+    LoadArgs la;
+    la.pos_stride = in->positionStrideBytes;
+    la.col_stride = in->colorStrideBytes;
+    la.col_format = in->colorFormat;
+    const uint64_t csize = in->colorFormat == CR_COLOR_RGBA8 ? 4 : 16;
+    if (on_device) {
+        la.pos = static_cast<const uint8_t *>(in->positions);
+        la.col = static_cast<const uint8_t *>(in->colors);
+    } else {
+        const uint8_t *hp = static_cast<const uint8_t *>(in->positions);
+        const uint8_t *hc = static_cast<const uint8_t *>(in->colors);
+        const uint64_t pbytes = (count - 1) * in->positionStrideBytes + 12;
+        const uint64_t cbytes = (count - 1) * in->colorStrideBytes + csize;
+        const bool inside = hc >= hp && in->colorStrideBytes == in->positionStrideBytes &&
+                            (uint64_t)(hc - hp) + csize <= in->positionStrideBytes;
+        const uint64_t need = inside ? std::max(pbytes, (uint64_t)(hc - hp) + cbytes)
+                                     : ((pbytes + 255) & ~255ull) + cbytes;
+        if ((st = grow(reinterpret_cast<uint8_t **>(&sc.raw), sc.cap_raw_bytes, need))) return st;
+        uint8_t *raw = static_cast<uint8_t *>(sc.raw);
+        if (inside) {
+            CR_CUDA(cudaMemcpyAsync(raw, hp, need, cudaMemcpyHostToDevice, s));
+            la.pos = raw;
+            la.col = raw + (hc - hp);
+        } else {
+            const uint64_t coff = (pbytes + 255) & ~255ull;
+            CR_CUDA(cudaMemcpyAsync(raw, hp, pbytes, cudaMemcpyHostToDevice, s));
+            CR_CUDA(cudaMemcpyAsync(raw + coff, hc, cbytes, cudaMemcpyHostToDevice, s));
+            la.pos = raw;
+            la.col = raw + coff;
+        }
+    }
+    pack_load<<<grid_for(count), kThreads, 0, s>>>(la, count, sc.pos, sc.col);
+    CR_CUDA(cudaGetLastError());
+
+    // Stage 1: bounds, read back once.
+    const uint32_t binit[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    CR_CUDA(cudaMemcpyAsync(sc.bounds, binit, sizeof(binit), cudaMemcpyHostToDevice, s));
+    pack_bounds<<<std::min<unsigned>(grid_for(count), (unsigned)ctx->sm_count * 8), kThreads, 0,
+                  s>>>(sc.pos, count, sc.bounds);
+    CR_CUDA(cudaGetLastError());
+    uint32_t bflip[6];
+    CR_CUDA(cudaMemcpyAsync(bflip, sc.bounds, sizeof(bflip), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    float bmin[3], bmax[3], ext[3];
+    for (int k = 0; k < 3; ++k) {
+        bmin[k] = unflip(bflip[k]);
+        bmax[k] = unflip(bflip[3 + k]);
+        ext[k] = std::fmax(bmax[k] - bmin[k], 0.000001f);
+    }
+
+    // Stage 2-3: Morton keys, stable sort.
+    MortonArgs ma;
+    ma.top = wide ? 2097151.0f : 1023.0f;
+    for (int k = 0; k < 3; ++k) {
+        ma.bmin[k] = bmin[k];
+        ma.scale[k] = ma.top / ext[k];
+    }
+    if ((st = grow(&sc.hist, sc.cap_hist, radix_hist_words(count)))) return st;
+    bool in_alt = false;
+    if (wide) {
+        auto *k0 = static_cast<unsigned long long *>(sc.keys[0]);
+        auto *k1 = static_cast<unsigned long long *>(sc.keys[1]);
+        pack_morton<unsigned long long><<<grid_for(count), kThreads, 0, s>>>(sc.pos, count, ma, k0,
+                                                                             sc.idx[0]);
+        CR_CUDA(cudaGetLastError());
+        st = radix_sort_pairs<unsigned long long>(k0, sc.idx[0], k1, sc.idx[1], count, 63, sc.hist,
+                                                  sc.digit_total, s, &in_alt);
+    } else {
+        auto *k0 = static_cast<uint32_t *>(sc.keys[0]);
+        auto *k1 = static_cast<uint32_t *>(sc.keys[1]);
+        pack_morton<uint32_t><<<grid_for(count), kThreads, 0, s>>>(sc.pos, count, ma, k0, sc.idx[0]);
+        CR_CUDA(cudaGetLastError());
+        st = radix_sort_pairs<uint32_t>(k0, sc.idx[0], k1, sc.idx[1], count, 30, sc.hist,
+                                        sc.digit_total, s, &in_alt);
+    }
+    if (st) return st;
+    const uint32_t *idx_sorted = sc.idx[in_alt ? 1 : 0];
+
+    // Stage 4-5: gather, LOD levels.
+    const int L = std::max(1, std::min(prm->lodLevels, 8));
+    const int divs = std::max(1, prm->coarseVoxelDivisions);
+    const uint8_t max_level = (uint8_t)(L - 1);
+    pack_gather<<<grid_for(count), kThreads, 0, s>>>(sc.pos, idx_sorted, count, sc.sorted,
+                                                     sc.lv_morton, max_level);
+    CR_CUDA(cudaGetLastError());
+    if (L > 1) {
+        const float longest = std::fmax(ext[0], std::fmax(ext[1], ext[2]));
+        const float base_voxel = longest / (float)divs;
+        for (int level = 0; level < L - 1; ++level) {
+            LodArgs a;
+            const float voxel = base_voxel * std::pow(0.5f, (float)level);
+            a.inv = 1.0f / std::fmax(voxel, 0.000001f);
+            uint64_t cells = 1;
+            for (int k = 0; k < 3; ++k) {
+                a.bmin[k] = bmin[k];
+                const float d = std::floor(ext[k] * a.inv);
+                if (!(d < 2097151.0f))
+                    return cri::fail(CR_ERR_CAPACITY, "LOD grid exceeds 2^21 cells per axis");
+                a.dims[k] = (uint32_t)d + 1u;
+                cells *= a.dims[k];
+            }
+            if (cells > kLodCellCap)
+                return cri::fail(CR_ERR_CAPACITY,
+                                 "LOD grid of " + std::to_string(cells) + " cells exceeds the cap");
+            a.max_level = max_level;
+            a.level = (uint8_t)level;
+            if ((st = grow(&sc.grid, sc.cap_grid, cells))) return st;
+            CR_CUDA(cudaMemsetAsync(sc.grid, 0xff, cells * 4, s));
+            pack_lod_claim<<<grid_for(count), kThreads, 0, s>>>(sc.sorted, sc.lv_morton, count, a,
+                                                                sc.grid);
+            CR_CUDA(cudaGetLastError());
+            pack_lod_assign<<<grid_for(count), kThreads, 0, s>>>(sc.sorted, sc.lv_morton, count,
+                                                                 a, sc.grid);
+            CR_CUDA(cudaGetLastError());
+        }
+    }
+
+    // Stage 6-7: batches, final order, quantisation into the pool.
+    cr_raster_batch *dst_batches = cloud->d_batches + first_slot;
+    pack_batches<<<nb, kThreads, 0, s>>>(sc.sorted, sc.lv_morton, count, ppb, first_slot,
+                                         dst_batches, sc.perm, sc.lv_out);
+    CR_CUDA(cudaGetLastError());
+    const uint64_t p0 = (uint64_t)first_slot * ppb;
+    pack_emit<<<grid_for(count), kThreads, 0, s>>>(
+        count, ppb, sc.perm, idx_sorted, sc.pos, sc.col, sc.lv_out, dst_batches, cloud->d_low + p0,
+        cloud->d_med + p0, cloud->d_high + p0, cloud->d_colors + p0, cloud->d_levels + p0,
+        sc.src_idx);
+    CR_CUDA(cudaGetLastError());
+    if (src_idx_host)
+        CR_CUDA(cudaMemcpyAsync(src_idx_host, sc.src_idx, count * 4, cudaMemcpyDeviceToHost, s));
+    return CR_OK;
+}
