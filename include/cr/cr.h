@@ -394,6 +394,20 @@ CR_API cr_status cr_context_pass_times(cr_context *ctx, int32_t nframes, float *
                                        int32_t *frames_out);
 
 /* ------------------------------------------------------------------------ */
+/* Launch tuning of the point passes                                         */
+/* ------------------------------------------------------------------------ */
+/* chunkPoints: survivor points per work record of the depth / colour /
+ * nearest passes (>= 256); useTiles: accumulate compact batches in
+ * shared-memory screen tiles.  Results do not depend on either value. */
+typedef struct cr_tuning {
+    int32_t chunkPoints; /* default 2048 */
+    int32_t useTiles;    /* default 1    */
+} cr_tuning;
+
+CR_API cr_status cr_context_get_tuning(cr_context *ctx, cr_tuning *out);
+CR_API cr_status cr_context_set_tuning(cr_context *ctx, const cr_tuning *tuning);
+
+/* ------------------------------------------------------------------------ */
 /* Synthetic workloads (seeded; a pure function of seed and point index)     */
 /* ------------------------------------------------------------------------ */
 /* Fractal heightfield: 2-D gradient noise summed over `octaves` with

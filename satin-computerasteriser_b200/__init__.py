@@ -95,6 +95,18 @@ class Context:
         N.check(N.lib().cr_context_stream(self._h, C.byref(s)))
         return s.value or 0
 
+    def tuning(self) -> dict:
+        t = N.cr_tuning()
+        N.check(N.lib().cr_context_get_tuning(self._h, C.byref(t)))
+        return {"chunkPoints": t.chunkPoints, "useTiles": bool(t.useTiles)}
+
+    def set_tuning(self, chunkPoints: int | None = None, useTiles: bool | None = None):
+        """Launch tuning of the point passes (results do not depend on it)."""
+        cur = self.tuning()
+        t = N.cr_tuning(int(cur["chunkPoints"] if chunkPoints is None else chunkPoints),
+                        int(cur["useTiles"] if useTiles is None else useTiles))
+        N.check(N.lib().cr_context_set_tuning(self._h, C.byref(t)))
+
     def set_profiling(self, enable: bool):
         """Bracket every pass of every cr_render with CUDA events (ring of 256 frames)."""
         N.check(N.lib().cr_context_set_profiling(self._h, int(enable)))

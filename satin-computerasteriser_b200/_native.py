@@ -71,6 +71,10 @@ class cr_synth_terrain(C.Structure):
                 ("outlierMargin", C.c_float), ("colorNoiseSigma", C.c_float)]
 
 
+class cr_tuning(C.Structure):
+    _fields_ = [("chunkPoints", C.c_int32), ("useTiles", C.c_int32)]
+
+
 class cr_cloud_info(C.Structure):
     _fields_ = [("capacity", cr_capacity), ("residentBatchCount", C.c_uint32),
                 ("pointCount", C.c_uint64), ("freeSlotCount", C.c_uint32),
@@ -126,6 +130,8 @@ PROTOTYPES = {
     "cr_host_alloc": (C.c_int, [u64, VP]),
     "cr_host_free": (C.c_int, [P]),
     "cr_context_set_profiling": (C.c_int, [P, C.c_int]),
+    "cr_context_get_tuning": (C.c_int, [P, C.POINTER(cr_tuning)]),
+    "cr_context_set_tuning": (C.c_int, [P, C.POINTER(cr_tuning)]),
     "cr_context_pass_times": (C.c_int, [P, i32, P, C.POINTER(i32)]),
     "cr_synth_terrain_default": (C.c_int, [C.POINTER(cr_synth_terrain)]),
     "cr_synth_terrain_height": (C.c_float, [C.POINTER(cr_synth_terrain), C.c_float, C.c_float]),

@@ -106,6 +106,8 @@ void free_cloud_buffers(cr_cloud *c) {
     dfree(c->d_visible);
     dfree(c->d_cull_tmp);
     dfree(c->d_cull_cta);
+    dfree(c->d_chunks);
+    c->chunk_cap = 0;
     dfree(c->d_counters);
 }
 
@@ -202,10 +204,12 @@ cr_status allocate_cloud(cr_cloud *c, cr_capacity cap, const cr_raster_file *fil
     const size_t ctas = (nb + 255) / 256;
     if ((st = dalloc(&c->d_batches, nb * sizeof(cr_raster_batch))) ||
         (st = dalloc(&c->d_visible, nb * sizeof(cr_visible_batch))) ||
-        (st = dalloc(&c->d_cull_tmp, ctas * 256 * sizeof(cr_visible_batch))) ||
-        (st = dalloc(&c->d_cull_cta, ctas * sizeof(uint32_t))) ||
+        (st = dalloc(&c->d_cull_tmp, ctas * 256 * sizeof(CullRec))) ||
+        (st = dalloc(&c->d_cull_cta, ctas * 2 * sizeof(uint32_t))) ||
         (st = dalloc(&c->d_counters, CNT_COUNT * sizeof(uint32_t))))
         return st;
+    c->chunk_cap = chunk_capacity(cap, kMinChunkPoints);
+    if ((st = dalloc(&c->d_chunks, c->chunk_cap * sizeof(ChunkRec)))) return st;
     c->d_files_cap = (uint32_t)c->files.size();
     if ((st = dalloc(&c->d_files, c->d_files_cap * sizeof(cr_raster_file)))) return st;
     cudaStream_t s = c->ctx->stream;
@@ -968,6 +972,23 @@ CR_API cr_status cr_host_alloc(uint64_t bytes, void **out) {
 
 CR_API cr_status cr_host_free(void *p) {
     if (p) CR_CUDA(cudaFreeHost(p));
+    return CR_OK;
+}
+
+// ---------------------------------------------------------------- tuning
+CR_API cr_status cr_context_get_tuning(cr_context *ctx, cr_tuning *out) {
+    if (!ctx || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    out->chunkPoints = ctx->chunk_points;
+    out->useTiles = ctx->use_tiles ? 1 : 0;
+    return CR_OK;
+}
+
+CR_API cr_status cr_context_set_tuning(cr_context *ctx, const cr_tuning *t) {
+    if (!ctx || !t) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    if (t->chunkPoints < kMinChunkPoints || t->chunkPoints > 65536)
+        return fail(CR_ERR_INVALID_ARGUMENT, "chunkPoints must be in [256, 65536]");
+    ctx->chunk_points = t->chunkPoints;
+    ctx->use_tiles = t->useTiles != 0;
     return CR_OK;
 }
 

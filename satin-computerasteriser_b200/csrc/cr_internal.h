@@ -31,7 +31,7 @@ enum CounterSlot : int {
     CNT_VISIBLE = 0,     // survivors of the last cull (VisibleBatch count)
     CNT_WORK_DEPTH = 1,  // dynamic work cursor of the depth / nearest pass
     CNT_WORK_COLOR = 2,  // dynamic work cursor of the colour pass
-    CNT_WORK_AUX = 3,    // spare cursor (gradient pass)
+    CNT_CHUNKS = 3,      // chunk work records written by the last cull
     CNT_ARGS_X = 4,      // CRDispatchArgs mirror: {count, 1, 1}
     CNT_ARGS_Y = 5,
     CNT_ARGS_Z = 6,
@@ -41,12 +41,43 @@ enum CounterSlot : int {
 
 struct PackScratch;
 
+// One survivor of the cull with the per-batch values the point passes need
+// (cull_classify output, 64 bytes).
+struct CullRec {
+    cr_visible_batch vb;
+    float minX, minY, minZ;  // batch min
+    float qx, qy, qz;        // batchSize / steps of the survivor's precision level
+    uint32_t first;          // batch firstPoint
+    uint32_t file;           // batch fileIndex
+    int32_t x0, y0, tw, th;  // screen rectangle (buffer rows), tw <= 0 when unknown
+};
+
+// One unit of point-pass work: up to `chunkPoints` consecutive survivor points
+// of one batch (64 bytes, written by cull_compact in survivor order).
+struct ChunkRec {
+    uint32_t first;  // absolute index of the chunk's first point
+    uint32_t count;
+    int32_t level;
+    float thr;
+    uint32_t batchIndex;
+    uint32_t file;
+    float minX, minY, minZ;
+    float qx, qy, qz;
+    int32_t x0, y0, tw, th;
+};
+static_assert(sizeof(CullRec) == 64, "CullRec is 64 bytes");
+static_assert(sizeof(ChunkRec) == 64, "ChunkRec is 64 bytes");
+
+constexpr int kMinChunkPoints = 256;
+
 struct cr_context {
     PackScratch *pack = nullptr;  // grow-only packer scratch
     int device = 0;
     cudaStream_t stream = nullptr;
     int sm_count = 0;
-    int raster_blocks_per_sm = 0;  // occupancy of the persistent point passes
+    int blocks_per_sm[3] = {0, 0, 0};  // occupancy of the persistent point passes
+    int chunk_points = 2048;           // points per chunk work record
+    bool use_tiles = true;             // shared-memory screen tiles
     // Profiling: a ring of frames, each with a start/stop event per pass.
     static constexpr int kProfRing = 256;
     bool profiling = false;
@@ -92,8 +123,10 @@ struct cr_cloud {
 
     // Cull outputs and scratch.
     cr_visible_batch *d_visible = nullptr;   // ordered survivors
-    cr_visible_batch *d_cull_tmp = nullptr;  // per-CTA compacted survivors
-    uint32_t *d_cull_cta = nullptr;          // per-CTA survivor counts
+    CullRec *d_cull_tmp = nullptr;           // per-CTA compacted survivors
+    uint32_t *d_cull_cta = nullptr;          // per-CTA survivor and chunk counts
+    ChunkRec *d_chunks = nullptr;            // chunk work records
+    uint64_t chunk_cap = 0;                  // capacity of d_chunks
     uint32_t *d_counters = nullptr;          // CounterSlot words
 
     // Pinned staging ring for the per-frame file table upload.
@@ -127,6 +160,8 @@ struct CullUniforms {
 };
 
 cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s);
+// Chunk records a cloud may need at the given chunk size.
+uint64_t chunk_capacity(const cr_capacity &cap, int chunk_points);
 
 enum RasterPass : int { PASS_DEPTH = 0, PASS_COLOR = 1, PASS_NEAREST = 2 };
 

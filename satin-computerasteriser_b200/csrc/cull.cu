@@ -1,5 +1,5 @@
 // cull.cu — batch frustum cull + CLOD survivor prefix, compacted into an
-// ordered work list.
+// ordered work list, plus the chunk work records of the point passes.
 //
 // Restates cullUpdate (Pipelines/Cull/Shaders.metal:19-83) and
 // cullFinalizeUpdate (Pipelines/CullFinalize/Shaders.metal:3-14).  The
@@ -7,11 +7,15 @@
 // unspecified; here the list is in ascending slot order (deterministic and
 // comparable to the CPU oracle):
 //   1. cull_classify: one thread per slot; each 256-slot CTA compacts its
-//      survivors in order with warp ballots and writes its count.
+//      survivors in order with warp ballots, adds the per-batch values the
+//      point passes need (decode steps, screen rectangle), and writes its
+//      survivor and chunk counts.
 //   2. cull_compact: each CTA sums the counts of the CTAs before it, copies
-//      its survivors to that offset; the last CTA publishes the total as the
-//      "indirect argument" the persistent point passes read, and resets
-//      their work cursors.
+//      its survivors to that offset and writes one chunk record per
+//      `chunkPoints` survivor points; the last CTA publishes the totals (the
+//      CUDA counterpart of the indirect argument buffer).
+#include <algorithm>
+
 #include "cr_device.cuh"
 #include "cr_internal.h"
 
@@ -24,13 +28,46 @@ struct CullArgs {
     uint32_t nbatches;
     const cr_raster_file *files;
     uint32_t nfiles;
-    cr_visible_batch *tmp;
+    CullRec *tmp;
     uint32_t *cta_counts;
+    uint32_t chunk_points;
     CullUniforms u;
 };
 
+// Screen rectangle (buffer rows, widened by two pixels, clamped) covering the
+// projection of the batch AABB's eight corners; tw = 0 when a corner lies
+// behind the camera.  Every point of the box then projects inside the hull
+// of the corners; the point passes treat the rectangle as a cache only.
+__device__ __forceinline__ void screen_rect(const cr_raster_batch &b, const float *T, int W,
+                                            int H, CullRec &r) {
+    float xmin = 3.0e38f, xmax = -3.0e38f, ymin = 3.0e38f, ymax = -3.0e38f;
+    bool front = true;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const crd::f4 clip = crd::mulp(T, (c & 1) ? b.maxX : b.minX, (c & 2) ? b.maxY : b.minY,
+                                       (c & 4) ? b.maxZ : b.minZ);
+        if (!(clip.w > 0.000001f) || !isfinite(clip.x) || !isfinite(clip.y)) front = false;
+        const float fx = (clip.x / clip.w * 0.5f + 0.5f) * (float)W;
+        const float fy = (clip.y / clip.w * 0.5f + 0.5f) * (float)H;
+        xmin = fminf(xmin, fx);
+        xmax = fmaxf(xmax, fx);
+        ymin = fminf(ymin, fy);
+        ymax = fmaxf(ymax, fy);
+    }
+    r.x0 = r.y0 = r.tw = r.th = 0;
+    if (!front || !(xmax - xmin < 1.0e6f) || !(ymax - ymin < 1.0e6f)) return;
+    const int x0 = max((int)floorf(xmin) - 2, 0), x1 = min((int)ceilf(xmax) + 2, W - 1);
+    const int yl = (int)floorf(ymin) - 2, yh = (int)ceilf(ymax) + 2;
+    const int y0 = max(H - 1 - yh, 0), y1 = min(H - 1 - yl, H - 1);
+    if (x1 < x0 || y1 < y0) return;
+    r.x0 = x0;
+    r.y0 = y0;
+    r.tw = x1 - x0 + 1;
+    r.th = y1 - y0 + 1;
+}
+
 // One slot of cullUpdate (Cull/Shaders.metal:28-82).
-__device__ __forceinline__ bool cull_slot(const CullArgs &a, uint32_t gid, cr_visible_batch &out) {
+__device__ __forceinline__ bool cull_slot(const CullArgs &a, uint32_t gid, CullRec &out) {
     const cr_raster_batch b = a.batches[gid];
     if (b.state == 0) return false;  // residency gate (:33-36)
     // A fileIndex past the file table is rejected here (the reference would
@@ -63,62 +100,139 @@ __device__ __forceinline__ bool cull_slot(const CullArgs &a, uint32_t gid, cr_vi
         active = min(active, b.numPoints);
     }
     if (active == 0u) return false;
-    out.batchIndex = gid;
-    out.level = level;
-    out.lodThreshold = thr;
-    out.activePoints = active;
+    out.vb.batchIndex = gid;
+    out.vb.level = level;
+    out.vb.lodThreshold = thr;
+    out.vb.activePoints = active;
+    // batchSize (Common.metal:81-83) over the steps of the precision level.
+    const float steps = level == 0 ? 1073741824.0f : level == 1 ? 1048576.0f : 1024.0f;
+    out.minX = b.minX;
+    out.minY = b.minY;
+    out.minZ = b.minZ;
+    out.qx = fmaxf(b.maxX - b.minX, 0.000001f) / steps;
+    out.qy = fmaxf(b.maxY - b.minY, 0.000001f) / steps;
+    out.qz = fmaxf(b.maxZ - b.minZ, 0.000001f) / steps;
+    out.first = b.firstPoint;
+    out.file = b.fileIndex;
+    screen_rect(b, file->transform, a.u.width, a.u.height, out);
     return true;
+}
+
+__device__ __forceinline__ uint32_t nchunks(uint32_t active, uint32_t c) {
+    return (active + c - 1u) / c;
 }
 
 __global__ void __launch_bounds__(kCullThreads) cull_classify(CullArgs a) {
     __shared__ uint32_t warp_counts[kCullThreads / 32];
+    __shared__ uint32_t warp_chunks[kCullThreads / 32];
     const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    cr_visible_batch rec;
+    CullRec rec;
     bool keep = false;
     if (gid < a.nbatches) keep = cull_slot(a, gid, rec);
     const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
-    if (lane == 0) warp_counts[warp] = __popc(ballot);
+    const uint32_t ch = __reduce_add_sync(
+        0xffffffffu, keep ? nchunks(rec.vb.activePoints, a.chunk_points) : 0u);
+    if (lane == 0) {
+        warp_counts[warp] = __popc(ballot);
+        warp_chunks[warp] = ch;
+    }
     __syncthreads();
-    uint32_t before = 0, total = 0;
+    uint32_t before = 0, total = 0, total_chunks = 0;
 #pragma unroll
     for (int w = 0; w < kCullThreads / 32; ++w) {
         if (w < warp) before += warp_counts[w];
         total += warp_counts[w];
+        total_chunks += warp_chunks[w];
     }
     if (keep) {
         const uint32_t pos = before + __popc(ballot & ((1u << lane) - 1u));
         a.tmp[blockIdx.x * kCullThreads + pos] = rec;
     }
-    if (threadIdx.x == 0) a.cta_counts[blockIdx.x] = total;
+    if (threadIdx.x == 0) {
+        a.cta_counts[2 * blockIdx.x] = total;
+        a.cta_counts[2 * blockIdx.x + 1] = total_chunks;
+    }
 }
 
 __global__ void __launch_bounds__(kCullThreads)
-    cull_compact(const cr_visible_batch *tmp, const uint32_t *cta_counts, cr_visible_batch *out,
-                 uint32_t *counters) {
-    __shared__ uint32_t partial[kCullThreads / 32];
-    // Exclusive prefix of the CTA counts before this CTA.
-    uint32_t s = 0;
-    for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kCullThreads) s += cta_counts[i];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) partial[threadIdx.x >> 5] = s;
+    cull_compact(const CullRec *tmp, const uint32_t *cta_counts, cr_visible_batch *out,
+                 ChunkRec *chunks, uint32_t chunk_points, uint32_t *counters) {
+    __shared__ uint32_t part_v[kCullThreads / 32], part_c[kCullThreads / 32];
+    __shared__ uint32_t scan_w[kCullThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // Exclusive prefix of the survivor and chunk counts of the CTAs before this one.
+    uint32_t sv = 0, sc = 0;
+    for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kCullThreads) {
+        sv += cta_counts[2 * i];
+        sc += cta_counts[2 * i + 1];
+    }
+    sv = __reduce_add_sync(0xffffffffu, sv);
+    sc = __reduce_add_sync(0xffffffffu, sc);
+    if (lane == 0) {
+        part_v[warp] = sv;
+        part_c[warp] = sc;
+    }
     __syncthreads();
-    uint32_t offset = 0;
+    uint32_t off_v = 0, off_c = 0;
 #pragma unroll
-    for (int w = 0; w < kCullThreads / 32; ++w) offset += partial[w];
-    const uint32_t mine = cta_counts[blockIdx.x];
-    for (uint32_t i = threadIdx.x; i < mine; i += kCullThreads)
-        out[offset + i] = tmp[blockIdx.x * kCullThreads + i];
+    for (int w = 0; w < kCullThreads / 32; ++w) {
+        off_v += part_v[w];
+        off_c += part_c[w];
+    }
+    const uint32_t mine = cta_counts[2 * blockIdx.x];
+    const uint32_t mine_chunks = cta_counts[2 * blockIdx.x + 1];
+    // One survivor per thread (a CTA holds at most 256): ordered copy and an
+    // exclusive scan of the chunk counts for the chunk record offsets.
+    CullRec r;
+    uint32_t c = 0;
+    if (threadIdx.x < mine) {
+        r = tmp[blockIdx.x * kCullThreads + threadIdx.x];
+        out[off_v + threadIdx.x] = r.vb;
+        c = nchunks(r.vb.activePoints, chunk_points);
+    }
+    uint32_t x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) scan_w[warp] = x;
+    __syncthreads();
+    uint32_t wbase = 0;
+#pragma unroll
+    for (int w = 0; w < kCullThreads / 32; ++w)
+        if (w < warp) wbase += scan_w[w];
+    const uint32_t base = off_c + wbase + (x - c);
+    for (uint32_t j = 0; j < c; ++j) {
+        ChunkRec k;
+        k.first = r.first + j * chunk_points;
+        k.count = min(chunk_points, r.vb.activePoints - j * chunk_points);
+        k.level = r.vb.level;
+        k.thr = r.vb.lodThreshold;
+        k.batchIndex = r.vb.batchIndex;
+        k.file = r.file;
+        k.minX = r.minX;
+        k.minY = r.minY;
+        k.minZ = r.minZ;
+        k.qx = r.qx;
+        k.qy = r.qy;
+        k.qz = r.qz;
+        k.x0 = r.x0;
+        k.y0 = r.y0;
+        k.tw = r.tw;
+        k.th = r.th;
+        chunks[base + j] = k;
+    }
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
         // cullFinalizeUpdate (CullFinalize/Shaders.metal:3-14): {count, 1, 1}.
-        counters[CNT_VISIBLE] = offset + mine;
-        counters[CNT_ARGS_X] = offset + mine;
+        counters[CNT_VISIBLE] = off_v + mine;
+        counters[CNT_ARGS_X] = off_v + mine;
         counters[CNT_ARGS_Y] = 1u;
         counters[CNT_ARGS_Z] = 1u;
         counters[CNT_WORK_DEPTH] = 0u;
         counters[CNT_WORK_COLOR] = 0u;
-        counters[CNT_WORK_AUX] = 0u;
+        counters[CNT_CHUNKS] = off_c + mine_chunks;
     }
 }
 
@@ -129,10 +243,15 @@ __global__ void cull_empty(uint32_t *counters) {
     counters[CNT_ARGS_Z] = 1u;
     counters[CNT_WORK_DEPTH] = 0u;
     counters[CNT_WORK_COLOR] = 0u;
-    counters[CNT_WORK_AUX] = 0u;
+    counters[CNT_CHUNKS] = 0u;
 }
 
 }  // namespace
+
+uint64_t chunk_capacity(const cr_capacity &cap, int chunk_points) {
+    const uint64_t per = ((uint64_t)cap.pointsPerBatch + chunk_points - 1) / chunk_points;
+    return std::max<uint64_t>(1, (uint64_t)cap.maxResidentBatches * per);
+}
 
 cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s) {
     const uint32_t n = cloud->cap.maxResidentBatches;
@@ -141,13 +260,15 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s) {
         CR_CUDA(cudaGetLastError());
         return CR_OK;
     }
+    const uint32_t cp = (uint32_t)std::max(cloud->ctx->chunk_points, kMinChunkPoints);
     const uint32_t ctas = (n + kCullThreads - 1) / kCullThreads;
-    CullArgs a{cloud->d_batches, n, cloud->d_files, (uint32_t)cloud->files.size(), cloud->d_cull_tmp,
-               cloud->d_cull_cta, u};
+    CullArgs a{cloud->d_batches, n, cloud->d_files, (uint32_t)cloud->files.size(),
+               cloud->d_cull_tmp, cloud->d_cull_cta, cp, u};
     cull_classify<<<ctas, kCullThreads, 0, s>>>(a);
     CR_CUDA(cudaGetLastError());
     cull_compact<<<ctas, kCullThreads, 0, s>>>(cloud->d_cull_tmp, cloud->d_cull_cta,
-                                               cloud->d_visible, cloud->d_counters);
+                                               cloud->d_visible, cloud->d_chunks, cp,
+                                               cloud->d_counters);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

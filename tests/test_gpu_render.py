@@ -266,3 +266,25 @@ def test_render_is_deterministic(cr, orc, ctx):
         outs.append((ras.outputRGBA8(), ras.pixels()))
     for o in outs[1:]:
         assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("chunk,tiles", [(256, True), (777, False), (2048, True), (65536, True),
+                                         (2048, False)])
+def test_tuning_does_not_change_results(cr, orc, ctx, mode, chunk, tiles):
+    """Chunk size and shared-memory tiles are launch choices only: every setting
+    renders the oracle's frame bit for bit (dense far-field cloud: many points
+    per pixel, so the tiles are exercised)."""
+    pos, rgba = blob_cloud(120000, 31, scale=1.0)
+    cloud, _ = make_cloud(cr, orc, ctx, pos, rgba, ppb=4096)
+    ctx.set_tuning(chunkPoints=chunk, useTiles=tiles)
+    try:
+        cfg = cr.ComputeRasteriserConfiguration(mode=mode, enableCLOD=False,
+                                                enableLODDither=False)
+        cam = camera(cr, (0.0, 0.0, 6.0), w=320, h=200, fov=40.0)
+        ras, gpu, ref = render_both(cr, orc, ctx, [cloud], cfg, cam, 320, 200)
+        assert_same(cr, cfg, gpu, ref)
+        if mode == 0:
+            assert ref.accum[..., 3].max() > 10  # many points per pixel
+    finally:
+        ctx.set_tuning(chunkPoints=2048, useTiles=True)
