@@ -63,6 +63,10 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--chunk-points", type=int, default=None,
+                    help="points per work record of the point passes (launch tuning)")
+    ap.add_argument("--tiles", type=int, default=None, choices=[0, 1],
+                    help="shared-memory screen tiles on/off (launch tuning)")
     return ap.parse_args()
 
 
@@ -226,6 +230,7 @@ def build_cloud(cr, ctx, args, params):
     ctx.synchronize()
     pack_s = time.perf_counter() - t0
     recs.close()
+    ctx.trim()
     return cloud, pack_s
 
 
@@ -262,6 +267,8 @@ def run_ours(args, dist):
     cr = importlib.import_module("satin-computerasteriser_b200")
     import torch
     ctx = cr.Context(dist.local)
+    ctx.set_tuning(chunkPoints=args.chunk_points, useTiles=None if args.tiles is None
+                   else bool(args.tiles))
     params = cr.TerrainParams(seed=args.seed)
     cloud, pack_s = build_cloud(cr, ctx, args, params)
     W, H = args.width, args.height
@@ -353,6 +360,7 @@ def run_ours(args, dist):
            "gpu_launches": int(args.steps * (5 if args.mode == "hqs" else 4)),
            "pass_ms": {n: round(float(v), 4) for n, v in zip(PASS_NAMES, avg)},
            "survivor_points_per_frame": int(active.mean()),
+           "tuning": ctx.tuning(),
            "pack_s": round(pack_s, 3)}
 
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:

@@ -209,6 +209,8 @@ CR_API cr_status cr_context_destroy(cr_context *ctx);
 CR_API cr_status cr_context_synchronize(cr_context *ctx);
 /* The context's cudaStream_t, as an opaque pointer. */
 CR_API cr_status cr_context_stream(cr_context *ctx, void **stream_out);
+/* Release the packer's grow-only scratch (it is re-allocated by the next pack). */
+CR_API cr_status cr_context_trim(cr_context *ctx);
 
 /* ------------------------------------------------------------------------ */
 /* Point cloud slot pool (ComputeRasteriserPointCloud)                       */

@@ -95,6 +95,10 @@ class Context:
         N.check(N.lib().cr_context_stream(self._h, C.byref(s)))
         return s.value or 0
 
+    def trim(self):
+        """Release the packer's scratch memory."""
+        N.check(N.lib().cr_context_trim(self._h))
+
     def tuning(self) -> dict:
         t = N.cr_tuning()
         N.check(N.lib().cr_context_get_tuning(self._h, C.byref(t)))

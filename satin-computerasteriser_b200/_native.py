@@ -97,6 +97,7 @@ PROTOTYPES = {
     "cr_context_destroy": (C.c_int, [P]),
     "cr_context_synchronize": (C.c_int, [P]),
     "cr_context_stream": (C.c_int, [P, VP]),
+    "cr_context_trim": (C.c_int, [P]),
     "cr_cloud_create": (C.c_int, [P, cr_capacity, P, u32, VP]),
     "cr_cloud_destroy": (C.c_int, [P]),
     "cr_cloud_reallocate": (C.c_int, [P, cr_capacity, P, u32]),

@@ -411,6 +411,14 @@ CR_API cr_status cr_context_stream(cr_context *ctx, void **stream_out) {
     return CR_OK;
 }
 
+CR_API cr_status cr_context_trim(cr_context *ctx) {
+    if (!ctx) return fail(CR_ERR_INVALID_ARGUMENT, "ctx is null");
+    DeviceGuard g(ctx->device);
+    CR_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->pack) pack_scratch_free(*ctx->pack);
+    return CR_OK;
+}
+
 // ---------------------------------------------------------------- cloud
 CR_API cr_status cr_cloud_create(cr_context *ctx, cr_capacity cap, const cr_raster_file *files,
                                  uint32_t nfiles, cr_cloud **out) {

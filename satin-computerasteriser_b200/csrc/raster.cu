@@ -29,13 +29,14 @@
 // screen rectangle (the projection of its AABB's eight corners, widened by
 // two pixels, computed by the cull).  When that rectangle has few pixels per
 // point, the CTA
-// accumulates in shared memory — depth max, or R|G and B|count packed in two
-// 64-bit adds (a batch's per-pixel sums stay below 2^32), or the nearest key
-// — and then flushes one global atomic per touched pixel.  The colour pass
+// accumulates in shared memory — depth max, or R | count << 20, G and B (a
+// chunk of fewer than 4096 points keeps every field below its width), or
+// the nearest key — and then flushes one global atomic per touched pixel.  The colour pass
 // also stages the rectangle's settled depths in shared memory.  Points that
 // round outside the rectangle use global atomics directly, so the tile is a
-// cache and never changes a result.  Other batches use global atomics with
-// a warp-level pre-merge of same-pixel lanes (__match_any_sync + redux).
+// cache and never changes a result.  Other batches, large on screen with
+// few points per pixel, use one global atomic per point.  Atomics are
+// predicated single instructions rather than branches around code.
 // Integer max and sum are associative and commutative: the planes are
 // bit-identical to a per-point atomic order either way.
 #include "cr_device.cuh"
@@ -56,7 +57,7 @@ struct TileCfg<PASS_DEPTH> {
 template <>
 struct TileCfg<PASS_COLOR> {
     static constexpr int kPx = 2048;
-    static constexpr int kBytes = kPx * 16 + kPx * 4;  // 2 x u64 accumulators + depth
+    static constexpr int kBytes = kPx * 16;  // R|count, G, B accumulators + settled depth
 };
 template <>
 struct TileCfg<PASS_NEAREST> {
@@ -107,20 +108,17 @@ template <int PASS>
 __device__ __forceinline__ void project_point(const RasterArgs &a, const BatchShared &sb,
                                               const ChunkRec &c, uint32_t lo, uint32_t me,
                                               uint32_t hi, PointOut &o) {
-    uint32_t x, y, z;
-    if (c.level == 0) {
-        x = ((lo & 1023u) << 20) | ((me & 1023u) << 10) | (hi & 1023u);
-        y = (((lo >> 10) & 1023u) << 20) | (((me >> 10) & 1023u) << 10) | ((hi >> 10) & 1023u);
-        z = (((lo >> 20) & 1023u) << 20) | (((me >> 20) & 1023u) << 10) | ((hi >> 20) & 1023u);
-    } else if (c.level == 1) {
-        x = ((lo & 1023u) << 10) | (me & 1023u);
-        y = (((lo >> 10) & 1023u) << 10) | ((me >> 10) & 1023u);
-        z = (((lo >> 20) & 1023u) << 10) | ((me >> 20) & 1023u);
-    } else {
-        x = lo & 1023u;
-        y = (lo >> 10) & 1023u;
-        z = (lo >> 20) & 1023u;
-    }
+    // Branch-free split-precision decode: a word the chunk's level does not
+    // use was never loaded and is zero; the shifts place the coarse (low),
+    // medium and fine (high) 10-bit chunks for level 0 (30 bits), level 1
+    // (20 bits) or level >= 2 (10 bits).
+    const uint32_t sl = c.level == 0 ? 20u : (c.level == 1 ? 10u : 0u);
+    const uint32_t sm = c.level == 0 ? 10u : 0u;
+    const uint32_t x = ((lo & 1023u) << sl) | ((me & 1023u) << sm) | (hi & 1023u);
+    const uint32_t y = (((lo >> 10) & 1023u) << sl) | (((me >> 10) & 1023u) << sm) |
+                       ((hi >> 10) & 1023u);
+    const uint32_t z = (((lo >> 20) & 1023u) << sl) | (((me >> 20) & 1023u) << sm) |
+                       ((hi >> 20) & 1023u);
     o.px = (float)x * c.qx + c.minX;
     o.py = (float)y * c.qy + c.minY;
     o.pz = (float)z * c.qz + c.minZ;
@@ -159,78 +157,58 @@ __device__ __forceinline__ void color_global(const RasterArgs &a, uint32_t pix, 
     atomicAdd(acc + 3, n);
 }
 
-// Direct path, radius 0: warp pre-merge of same-pixel lanes, then one global
-// atomic per distinct pixel.  Every lane of the warp calls this.
+// Direct path, radius 0: one global atomic per point (batches large on
+// screen, where points rarely share a pixel).
 template <int PASS>
 __device__ __forceinline__ void emit_direct(const RasterArgs &a, const PointOut &o) {
-    const int lane = threadIdx.x & 31;
     const uint32_t pix = (uint32_t)(o.iy * a.u.width + o.ix);
     if (PASS == PASS_DEPTH) {
-        const uint32_t peers = __match_any_sync(kFull, o.ok ? pix : kFull);
-        if (o.ok) {
-            const uint32_t m = __reduce_max_sync(peers, o.depth);
-            if (lane == __ffs(peers) - 1) atomicMax(&a.t.depth[pix], m);
-        }
+        if (o.ok) atomicMax(&a.t.depth[pix], o.depth);
     } else if (PASS == PASS_COLOR) {
-        bool vis = false;
-        if (o.ok) {
-            const uint32_t closest = a.t.depth[pix];
-            vis = closest != 0u && o.nz >= crd::uint_to_depth(closest) * a.keep_scale;
-        }
-        const uint32_t peers = __match_any_sync(kFull, vis ? pix : kFull);
-        if (vis) {
-            const uint32_t r = __reduce_add_sync(peers, o.color & 0xffu);
-            const uint32_t g = __reduce_add_sync(peers, (o.color >> 8) & 0xffu);
-            const uint32_t b = __reduce_add_sync(peers, (o.color >> 16) & 0xffu);
-            if (lane == __ffs(peers) - 1) color_global(a, pix, r, g, b, (uint32_t)__popc(peers));
-        }
+        const uint32_t closest = o.ok ? a.t.depth[pix] : 0u;
+        const bool vis = closest != 0u && o.nz >= crd::uint_to_depth(closest) * a.keep_scale;
+        if (vis)
+            color_global(a, pix, o.color & 0xffu, (o.color >> 8) & 0xffu, (o.color >> 16) & 0xffu,
+                         1u);
     } else {
-        const uint32_t peers = __match_any_sync(kFull, o.ok ? pix : kFull);
-        if (o.ok) {
-            const uint32_t m = __reduce_max_sync(peers, o.depth);
-            const uint32_t tied = __ballot_sync(peers, o.depth == m);
-            if (o.depth == m) {
-                const uint32_t mi = __reduce_min_sync(tied, o.pointIndex);
-                if (lane == __ffs(tied) - 1) atomicMax(&a.t.nearest[pix], nearest_key(m, mi));
-            }
-        }
+        if (o.ok) atomicMax(&a.t.nearest[pix], nearest_key(o.depth, o.pointIndex));
     }
 }
 
-// Tile path, radius 0: shared-memory accumulation (global fallback outside).
+// Tile path, radius 0: shared-memory accumulation, global atomics for points
+// that round outside the rectangle.  Colour tiles hold R | count << 20, G and
+// B per pixel in 32-bit words (exact while a chunk has at most 4095 points).
 template <int PASS>
 __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ChunkRec &c,
                                           unsigned char *smem, const PointOut &o) {
-    if (!o.ok) return;
     const int lx = o.ix - c.x0, ly = o.iy - c.y0;
     const bool inside = (unsigned)lx < (unsigned)c.tw && (unsigned)ly < (unsigned)c.th;
+    const bool in_tile = o.ok && inside, outside = o.ok && !inside;
     const uint32_t pix = (uint32_t)(o.iy * a.u.width + o.ix);
-    const int l = ly * c.tw + lx;
+    const int l = inside ? ly * c.tw + lx : 0;
     if (PASS == PASS_DEPTH) {
-        if (inside)
-            atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
-        else
-            atomicMax(&a.t.depth[pix], o.depth);
+        if (in_tile) atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
+        if (outside) atomicMax(&a.t.depth[pix], o.depth);
     } else if (PASS == PASS_COLOR) {
-        const uint32_t *sdep =
-            reinterpret_cast<const uint32_t *>(smem + TileCfg<PASS_COLOR>::kPx * 16);
-        const uint32_t closest = inside ? sdep[l] : a.t.depth[pix];
-        if (closest == 0u || !(o.nz >= crd::uint_to_depth(closest) * a.keep_scale)) return;
+        constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
+        uint32_t *acc = reinterpret_cast<uint32_t *>(smem);
+        const uint32_t *sdep = acc + 3 * kPx;
+        uint32_t closest = sdep[l];
+        if (outside) closest = a.t.depth[pix];
+        const bool vis = o.ok && closest != 0u &&
+                         o.nz >= crd::uint_to_depth(closest) * a.keep_scale;
         const uint32_t r = o.color & 0xffu, g = (o.color >> 8) & 0xffu,
                        b = (o.color >> 16) & 0xffu;
-        if (inside) {
-            unsigned long long *acc = reinterpret_cast<unsigned long long *>(smem) + 2 * l;
-            atomicAdd(acc, (unsigned long long)r | ((unsigned long long)g << 32));
-            atomicAdd(acc + 1, (unsigned long long)b | (1ull << 32));
-        } else {
-            color_global(a, pix, r, g, b, 1u);
+        if (vis && inside) {
+            atomicAdd(acc + l, r | (1u << 20));
+            atomicAdd(acc + kPx + l, g);
+            atomicAdd(acc + 2 * kPx + l, b);
         }
+        if (vis && !inside) color_global(a, pix, r, g, b, 1u);
     } else {
         const unsigned long long k = nearest_key(o.depth, o.pointIndex);
-        if (inside)
-            atomicMax(reinterpret_cast<unsigned long long *>(smem) + l, k);
-        else
-            atomicMax(&a.t.nearest[pix], k);
+        if (in_tile) atomicMax(reinterpret_cast<unsigned long long *>(smem) + l, k);
+        if (outside) atomicMax(&a.t.nearest[pix], k);
     }
 }
 
@@ -294,12 +272,13 @@ __device__ __forceinline__ void tile_init(const RasterArgs &a, const ChunkRec &c
         if (PASS == PASS_DEPTH) {
             reinterpret_cast<uint32_t *>(smem)[l] = 0u;
         } else if (PASS == PASS_COLOR) {
-            unsigned long long *acc = reinterpret_cast<unsigned long long *>(smem);
-            acc[2 * l] = 0ull;
-            acc[2 * l + 1] = 0ull;
+            constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
+            uint32_t *acc = reinterpret_cast<uint32_t *>(smem);
+            acc[l] = 0u;
+            acc[kPx + l] = 0u;
+            acc[2 * kPx + l] = 0u;
             const int gx = c.x0 + l % c.tw, gy = c.y0 + l / c.tw;
-            reinterpret_cast<uint32_t *>(smem + TileCfg<PASS_COLOR>::kPx * 16)[l] =
-                a.t.depth[gy * a.u.width + gx];
+            acc[3 * kPx + l] = a.t.depth[gy * a.u.width + gx];
         } else {
             reinterpret_cast<unsigned long long *>(smem)[l] = 0ull;
         }
@@ -316,10 +295,11 @@ __device__ __forceinline__ void tile_flush(const RasterArgs &a, const ChunkRec &
             const uint32_t v = reinterpret_cast<const uint32_t *>(smem)[l];
             if (v) atomicMax(&a.t.depth[pix], v);
         } else if (PASS == PASS_COLOR) {
-            const unsigned long long *acc = reinterpret_cast<const unsigned long long *>(smem);
-            const unsigned long long rg = acc[2 * l], bc = acc[2 * l + 1];
-            const uint32_t cnt = (uint32_t)(bc >> 32);
-            if (cnt) color_global(a, pix, (uint32_t)rg, (uint32_t)(rg >> 32), (uint32_t)bc, cnt);
+            constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
+            const uint32_t *acc = reinterpret_cast<const uint32_t *>(smem);
+            const uint32_t rc = acc[l];
+            const uint32_t cnt = rc >> 20;
+            if (cnt) color_global(a, pix, rc & 0xfffffu, acc[kPx + l], acc[2 * kPx + l], cnt);
         } else {
             const unsigned long long k = reinterpret_cast<const unsigned long long *>(smem)[l];
             if (k) atomicMax(&a.t.nearest[pix], k);
@@ -367,7 +347,8 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
         cp_async_commit();
         const bool new_file = c.file != sb.file;
         const bool tiled = a.use_tiles && a.radius_zero && c.tw > 0 &&
-                           c.tw * c.th <= TileCfg<PASS>::kPx && c.tw * c.th <= (int)(2 * c.count);
+                           c.tw * c.th <= TileCfg<PASS>::kPx && c.tw * c.th <= (int)(2 * c.count) &&
+                           (PASS != PASS_COLOR || c.count < 4096u);
         if (new_file || tiled) {
             __syncthreads();  // everyone has read sb.file
             if (new_file) {
