@@ -108,6 +108,10 @@ void free_cloud_buffers(cr_cloud *c) {
     dfree(c->d_cull_cta);
     dfree(c->d_chunks);
     c->chunk_cap = 0;
+    dfree(c->d_frag_xy);
+    dfree(c->d_frag_z);
+    dfree(c->d_frag_col);
+    dfree(c->d_frag_count);
     dfree(c->d_counters);
 }
 
@@ -209,7 +213,11 @@ cr_status allocate_cloud(cr_cloud *c, cr_capacity cap, const cr_raster_file *fil
         (st = dalloc(&c->d_counters, CNT_COUNT * sizeof(uint32_t))))
         return st;
     c->chunk_cap = chunk_capacity(cap, kMinChunkPoints);
-    if ((st = dalloc(&c->d_chunks, c->chunk_cap * sizeof(ChunkRec)))) return st;
+    if ((st = dalloc(&c->d_chunks, c->chunk_cap * sizeof(ChunkRec))) ||
+        (st = dalloc(&c->d_frag_count, c->chunk_cap * sizeof(uint32_t))) ||
+        (st = dalloc(&c->d_frag_xy, pts * 4)) || (st = dalloc(&c->d_frag_z, pts * 4)) ||
+        (st = dalloc(&c->d_frag_col, pts * 4)))
+        return st;
     c->d_files_cap = (uint32_t)c->files.size();
     if ((st = dalloc(&c->d_files, c->d_files_cap * sizeof(cr_raster_file)))) return st;
     cudaStream_t s = c->ctx->stream;
@@ -694,6 +702,8 @@ CR_API cr_status cr_frame_create(cr_context *ctx, int w, int h, cr_frame **out) 
     if (w <= 0 || h <= 0) return fail(CR_ERR_INVALID_ARGUMENT, "frame size must be positive");
     if ((uint64_t)w * (uint64_t)h >= (1ull << 31))
         return fail(CR_ERR_CAPACITY, "frame exceeds 2^31 pixels");
+    if (w > 65535 || h > 65535)
+        return fail(CR_ERR_CAPACITY, "frame width and height must be at most 65535");
     DeviceGuard g(ctx->device);
     auto *f = new cr_frame();
     f->ctx = ctx;
@@ -771,15 +781,21 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
             for (cr_cloud *c : resident)
                 if ((st = launch_cull(c, cu, s))) return st;
         }
+        // With single-pixel footprints the depth pass keeps every point that
+        // reaches the screen as a fragment and the colour pass reads those
+        // instead of decoding and projecting the points again.
+        const bool frags = std::fmax(cfg->minimumPointSize, cfg->maximumPointSize) <= 1.0f;
         {
             PassTimer pt(ctx, CR_PASS_DEPTH);
             for (cr_cloud *c : resident)
-                if ((st = launch_raster(c, PASS_DEPTH, rau, t, s))) return st;
+                if ((st = launch_raster(c, frags ? PASS_DEPTH_FRAG : PASS_DEPTH, rau, t, s)))
+                    return st;
         }
         {
             PassTimer pt(ctx, CR_PASS_COLOR);
             for (cr_cloud *c : resident)
-                if ((st = launch_raster(c, PASS_COLOR, rau, t, s))) return st;
+                if ((st = launch_raster(c, frags ? PASS_COLOR_FRAG : PASS_COLOR, rau, t, s)))
+                    return st;
         }
         {
             PassTimer pt(ctx, CR_PASS_RESOLVE);

@@ -75,7 +75,7 @@ struct cr_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     int sm_count = 0;
-    int blocks_per_sm[3] = {0, 0, 0};  // occupancy of the persistent point passes
+    int blocks_per_sm[5] = {0, 0, 0, 0, 0};  // occupancy of the persistent point passes
     int chunk_points = 2048;           // points per chunk work record
     bool use_tiles = true;             // shared-memory screen tiles
     // Profiling: a ring of frames, each with a start/stop event per pass.
@@ -127,6 +127,13 @@ struct cr_cloud {
     uint32_t *d_cull_cta = nullptr;          // per-CTA survivor and chunk counts
     ChunkRec *d_chunks = nullptr;            // chunk work records
     uint64_t chunk_cap = 0;                  // capacity of d_chunks
+
+    // Fragments of the last depth pass, in pool point index space: a chunk
+    // starting at point p keeps its n kept points compacted at [p, p + n).
+    uint32_t *d_frag_xy = nullptr;     // pixel x | row << 16
+    float *d_frag_z = nullptr;         // NDC z
+    uint32_t *d_frag_col = nullptr;    // RGBA8 (after the colorize options)
+    uint32_t *d_frag_count = nullptr;  // kept points per chunk record
     uint32_t *d_counters = nullptr;          // CounterSlot words
 
     // Pinned staging ring for the per-frame file table upload.
@@ -163,7 +170,16 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s);
 // Chunk records a cloud may need at the given chunk size.
 uint64_t chunk_capacity(const cr_capacity &cap, int chunk_points);
 
-enum RasterPass : int { PASS_DEPTH = 0, PASS_COLOR = 1, PASS_NEAREST = 2 };
+// PASS_DEPTH_FRAG is the depth pass that also writes each kept point as a
+// fragment; PASS_COLOR_FRAG is the colour pass over those fragments.
+enum RasterPass : int {
+    PASS_DEPTH = 0,
+    PASS_COLOR = 1,
+    PASS_NEAREST = 2,
+    PASS_DEPTH_FRAG = 3,
+    PASS_COLOR_FRAG = 4
+};
+constexpr int kRasterPassCount = 5;
 
 struct RasterUniforms {
     float view[16];

@@ -65,6 +65,14 @@ struct TileCfg<PASS_NEAREST> {
     static constexpr int kBytes = kPx * 8;
 };
 
+template <>
+struct TileCfg<PASS_DEPTH_FRAG> : TileCfg<PASS_DEPTH> {};
+template <>
+struct TileCfg<PASS_COLOR_FRAG> : TileCfg<PASS_COLOR> {};
+
+__host__ __device__ constexpr bool is_depth(int p) { return p == PASS_DEPTH || p == PASS_DEPTH_FRAG; }
+__host__ __device__ constexpr bool is_color(int p) { return p == PASS_COLOR || p == PASS_COLOR_FRAG; }
+
 struct RasterArgs {
     const ChunkRec *chunks;
     const cr_raster_file *files;
@@ -76,6 +84,10 @@ struct RasterArgs {
     float keep_scale;  // 1 - depthTolerance
     int radius_zero;   // every footprint is a single pixel
     int use_tiles;
+    uint32_t *frag_xy;
+    float *frag_z;
+    uint32_t *frag_col;
+    uint32_t *frag_count;
 };
 
 struct BatchShared {
@@ -136,7 +148,7 @@ __device__ __forceinline__ void project_point(const RasterArgs &a, const BatchSh
     o.depth = crd::depth_to_uint(nz);
     o.nz = nz;
     o.ok = ok;
-    if (PASS == PASS_COLOR) {  // ColorPass/Shaders.metal:95-100
+    if (PASS == PASS_COLOR || PASS == PASS_DEPTH_FRAG) {  // ColorPass/Shaders.metal:95-100
         if (a.u.colorizeChunks)
             o.color = c.batchIndex * 1234567u;
         else if (a.u.colorizeOverdraw)
@@ -162,9 +174,9 @@ __device__ __forceinline__ void color_global(const RasterArgs &a, uint32_t pix, 
 template <int PASS>
 __device__ __forceinline__ void emit_direct(const RasterArgs &a, const PointOut &o) {
     const uint32_t pix = (uint32_t)(o.iy * a.u.width + o.ix);
-    if (PASS == PASS_DEPTH) {
+    if (is_depth(PASS)) {
         if (o.ok) atomicMax(&a.t.depth[pix], o.depth);
-    } else if (PASS == PASS_COLOR) {
+    } else if (is_color(PASS)) {
         const uint32_t closest = o.ok ? a.t.depth[pix] : 0u;
         const bool vis = closest != 0u && o.nz >= crd::uint_to_depth(closest) * a.keep_scale;
         if (vis)
@@ -186,10 +198,10 @@ __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ChunkRec &c
     const bool in_tile = o.ok && inside, outside = o.ok && !inside;
     const uint32_t pix = (uint32_t)(o.iy * a.u.width + o.ix);
     const int l = inside ? ly * c.tw + lx : 0;
-    if (PASS == PASS_DEPTH) {
+    if (is_depth(PASS)) {
         if (in_tile) atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
         if (outside) atomicMax(&a.t.depth[pix], o.depth);
-    } else if (PASS == PASS_COLOR) {
+    } else if (is_color(PASS)) {
         constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
         uint32_t *acc = reinterpret_cast<uint32_t *>(smem);
         const uint32_t *sdep = acc + 3 * kPx;
@@ -228,9 +240,9 @@ __device__ __forceinline__ void emit_footprint(const RasterArgs &a, const BatchS
             const int tx = o.ix + ox, ty = o.iy + oy;
             if (tx < 0 || tx >= W || ty < 0 || ty >= H) continue;
             const uint32_t pix = (uint32_t)(ty * W + tx);
-            if (PASS == PASS_DEPTH) {
+            if (is_depth(PASS)) {
                 atomicMax(&a.t.depth[pix], o.depth);
-            } else if (PASS == PASS_COLOR) {
+            } else if (is_color(PASS)) {
                 const uint32_t closest = a.t.depth[pix];
                 if (closest == 0u) continue;
                 if (!(o.nz >= crd::uint_to_depth(closest) * a.keep_scale)) continue;
@@ -240,6 +252,26 @@ __device__ __forceinline__ void emit_footprint(const RasterArgs &a, const BatchS
                 atomicMax(&a.t.nearest[pix], nearest_key(o.depth, o.pointIndex));
             }
         }
+    }
+}
+
+// Shared count of the fragments the current chunk has kept.
+__shared__ uint32_t s_frag_count;
+
+// Appends the warp's kept points to the chunk's fragment range [first, first+n):
+// one shared-memory atomic per warp, lanes placed by ballot rank.
+__device__ __forceinline__ void emit_fragment(const RasterArgs &a, const ChunkRec &c,
+                                              const PointOut &o) {
+    const uint32_t ballot = __ballot_sync(kFull, o.ok);
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&s_frag_count, __popc(ballot));
+    base = __shfl_sync(kFull, base, 0);
+    if (o.ok) {
+        const uint32_t i = c.first + base + __popc(ballot & ((1u << lane) - 1u));
+        a.frag_xy[i] = (uint32_t)o.ix | ((uint32_t)o.iy << 16);
+        a.frag_z[i] = o.nz;
+        a.frag_col[i] = o.color;
     }
 }
 
@@ -262,6 +294,23 @@ __device__ __forceinline__ void do_point(const RasterArgs &a, const BatchShared 
         emit_tile<PASS>(a, c, smem, o);
     else
         emit_direct<PASS>(a, o);
+    if (PASS == PASS_DEPTH_FRAG) emit_fragment(a, c, o);
+}
+
+// One fragment of the colour pass (PASS_COLOR_FRAG); every lane calls this.
+__device__ __forceinline__ void do_fragment(const RasterArgs &a, unsigned char *smem,
+                                            const ChunkRec &c, bool tiled, bool valid,
+                                            uint32_t xy, float nz, uint32_t color) {
+    PointOut o;
+    o.ok = valid;
+    o.ix = (int)(xy & 0xffffu);
+    o.iy = (int)(xy >> 16);
+    o.nz = nz;
+    o.color = color;
+    if (tiled)
+        emit_tile<PASS_COLOR_FRAG>(a, c, smem, o);
+    else
+        emit_direct<PASS_COLOR_FRAG>(a, o);
 }
 
 template <int PASS>
@@ -269,9 +318,9 @@ __device__ __forceinline__ void tile_init(const RasterArgs &a, const ChunkRec &c
                                           unsigned char *smem) {
     const int n = c.tw * c.th;
     for (int l = threadIdx.x; l < n; l += kThreads) {
-        if (PASS == PASS_DEPTH) {
+        if (is_depth(PASS)) {
             reinterpret_cast<uint32_t *>(smem)[l] = 0u;
-        } else if (PASS == PASS_COLOR) {
+        } else if (is_color(PASS)) {
             constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
             uint32_t *acc = reinterpret_cast<uint32_t *>(smem);
             acc[l] = 0u;
@@ -291,10 +340,10 @@ __device__ __forceinline__ void tile_flush(const RasterArgs &a, const ChunkRec &
     const int n = c.tw * c.th;
     for (int l = threadIdx.x; l < n; l += kThreads) {
         const uint32_t pix = (uint32_t)((c.y0 + l / c.tw) * a.u.width + c.x0 + l % c.tw);
-        if (PASS == PASS_DEPTH) {
+        if (is_depth(PASS)) {
             const uint32_t v = reinterpret_cast<const uint32_t *>(smem)[l];
             if (v) atomicMax(&a.t.depth[pix], v);
-        } else if (PASS == PASS_COLOR) {
+        } else if (is_color(PASS)) {
             constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
             const uint32_t *acc = reinterpret_cast<const uint32_t *>(smem);
             const uint32_t rc = acc[l];
@@ -313,6 +362,11 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src)
                  : "memory");
 }
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem_src)
+                 : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() {
     asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
@@ -328,27 +382,35 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ BatchShared sb;
     __shared__ __align__(16) ChunkRec rec[2];
+    __shared__ __align__(16) uint32_t rec_frags[2][4];
     const uint32_t nchunks = a.counters[CNT_CHUNKS];
     uint32_t k = blockIdx.x;
     if (k >= nchunks) return;
     if (threadIdx.x < 4) cp_async16(reinterpret_cast<uint4 *>(&rec[0]) + threadIdx.x,
                                     reinterpret_cast<const uint4 *>(a.chunks + k) + threadIdx.x);
+    if (PASS == PASS_COLOR_FRAG && threadIdx.x == 4) cp_async4(&rec_frags[0][0], a.frag_count + k);
     cp_async_commit();
-    if (threadIdx.x == 0) sb.file = 0xffffffffu;
+    if (threadIdx.x == 0) {
+        sb.file = 0xffffffffu;
+        s_frag_count = 0u;
+    }
     int buf = 0;
     for (; k < nchunks; k += gridDim.x, buf ^= 1) {
         cp_async_wait_all();
         __syncthreads();  // rec[buf] complete; the previous chunk is fully done
         const ChunkRec c = rec[buf];
+        const uint32_t nfrag = PASS == PASS_COLOR_FRAG ? rec_frags[buf][0] : 0u;
         const uint32_t kn = k + gridDim.x;
         if (kn < nchunks && threadIdx.x < 4)
             cp_async16(reinterpret_cast<uint4 *>(&rec[buf ^ 1]) + threadIdx.x,
                        reinterpret_cast<const uint4 *>(a.chunks + kn) + threadIdx.x);
+        if (PASS == PASS_COLOR_FRAG && kn < nchunks && threadIdx.x == 4)
+            cp_async4(&rec_frags[buf ^ 1][0], a.frag_count + kn);
         cp_async_commit();
         const bool new_file = c.file != sb.file;
         const bool tiled = a.use_tiles && a.radius_zero && c.tw > 0 &&
                            c.tw * c.th <= TileCfg<PASS>::kPx && c.tw * c.th <= (int)(2 * c.count) &&
-                           (PASS != PASS_COLOR || c.count < 4096u);
+                           (!is_color(PASS) || c.count < 4096u);
         if (new_file || tiled) {
             __syncthreads();  // everyone has read sb.file
             if (new_file) {
@@ -363,7 +425,37 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
             __syncthreads();
         }
         const bool need_med = c.level <= 1, need_high = c.level == 0;
-        if ((c.first & 3u) == 0u) {
+        constexpr bool kNeedColor = PASS == PASS_COLOR || PASS == PASS_DEPTH_FRAG;
+        if (PASS == PASS_COLOR_FRAG) {
+            // The chunk's fragments, four per thread when 16-byte aligned.
+            if ((c.first & 3u) == 0u) {
+                const uint32_t nquads = (nfrag + 3u) >> 2;
+                for (uint32_t q0 = 0; q0 < nquads; q0 += kThreads) {
+                    const uint32_t q = q0 + threadIdx.x;
+                    const uint32_t base = c.first + 4u * q;
+                    uint4 xy4 = make_uint4(0, 0, 0, 0), co4 = xy4;
+                    float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (q < nquads) {
+                        xy4 = __ldcs(reinterpret_cast<const uint4 *>(a.frag_xy + base));
+                        z4 = __ldcs(reinterpret_cast<const float4 *>(a.frag_z + base));
+                        co4 = __ldcs(reinterpret_cast<const uint4 *>(a.frag_col + base));
+                    }
+                    const uint32_t l0 = 4u * q;
+                    do_fragment(a, smem, c, tiled, l0 + 0 < nfrag, xy4.x, z4.x, co4.x);
+                    do_fragment(a, smem, c, tiled, l0 + 1 < nfrag, xy4.y, z4.y, co4.y);
+                    do_fragment(a, smem, c, tiled, l0 + 2 < nfrag, xy4.z, z4.z, co4.z);
+                    do_fragment(a, smem, c, tiled, l0 + 3 < nfrag, xy4.w, z4.w, co4.w);
+                }
+            } else {
+                for (uint32_t l0 = 0; l0 < nfrag; l0 += kThreads) {
+                    const uint32_t l = l0 + threadIdx.x;
+                    const bool v = l < nfrag;
+                    const uint32_t i = c.first + (v ? l : 0u);
+                    do_fragment(a, smem, c, tiled, v, v ? a.frag_xy[i] : 0u, v ? a.frag_z[i] : 0.f,
+                                v ? a.frag_col[i] : 0u);
+                }
+            }
+        } else if ((c.first & 3u) == 0u) {
             // Four points per thread, 16-byte loads.
             const uint32_t nquads = (c.count + 3u) >> 2;
             for (uint32_t q0 = 0; q0 < nquads; q0 += kThreads) {
@@ -377,7 +469,7 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
                     lo4 = __ldg(reinterpret_cast<const uint4 *>(a.low + base));
                     if (need_med) me4 = __ldg(reinterpret_cast<const uint4 *>(a.med + base));
                     if (need_high) hi4 = __ldg(reinterpret_cast<const uint4 *>(a.high + base));
-                    if (PASS == PASS_COLOR)
+                    if (kNeedColor)
                         co4 = __ldg(reinterpret_cast<const uint4 *>(a.colors + base));
                 }
                 const uint32_t l0 = 4u * q;
@@ -400,13 +492,17 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
                 const uint32_t lo = v ? a.low[i] : 0u;
                 const uint32_t me = (v && need_med) ? a.med[i] : 0u;
                 const uint32_t hi = (v && need_high) ? a.high[i] : 0u;
-                const uint32_t co = (v && PASS == PASS_COLOR) ? a.colors[i] : 0u;
+                const uint32_t co = (v && kNeedColor) ? a.colors[i] : 0u;
                 do_point<PASS>(a, sb, smem, c, tiled, v, local, lv, lo, me, hi, co);
             }
         }
-        if (tiled) {
+        if (tiled || PASS == PASS_DEPTH_FRAG) {
             __syncthreads();
-            tile_flush<PASS>(a, c, smem);
+            if (tiled) tile_flush<PASS>(a, c, smem);
+            if (PASS == PASS_DEPTH_FRAG && threadIdx.x == 0) {
+                a.frag_count[k] = s_frag_count;
+                s_frag_count = 0u;
+            }
         }
     }
     cp_async_wait_all();
@@ -429,6 +525,8 @@ int raster_blocks_per_sm(int pass) {
     switch (pass) {
     case PASS_DEPTH: return blocks_per_sm_for<PASS_DEPTH>();
     case PASS_COLOR: return blocks_per_sm_for<PASS_COLOR>();
+    case PASS_DEPTH_FRAG: return blocks_per_sm_for<PASS_DEPTH_FRAG>();
+    case PASS_COLOR_FRAG: return blocks_per_sm_for<PASS_COLOR_FRAG>();
     default: return blocks_per_sm_for<PASS_NEAREST>();
     }
 }
@@ -451,6 +549,10 @@ cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &
     // upper bound is 1 every radius is 0 whatever the distance.
     a.radius_zero = fmaxf(u.minimumPointSize, u.maximumPointSize) <= 1.0f ? 1 : 0;
     a.use_tiles = cloud->ctx->use_tiles ? 1 : 0;
+    a.frag_xy = cloud->d_frag_xy;
+    a.frag_z = cloud->d_frag_z;
+    a.frag_col = cloud->d_frag_col;
+    a.frag_count = cloud->d_frag_count;
     cr_context *ctx = cloud->ctx;
     if (ctx->blocks_per_sm[pass] == 0) ctx->blocks_per_sm[pass] = raster_blocks_per_sm(pass);
     const int grid = ctx->sm_count * ctx->blocks_per_sm[pass];
@@ -460,6 +562,12 @@ cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &
         break;
     case PASS_COLOR:
         raster_kernel<PASS_COLOR><<<grid, kThreads, TileCfg<PASS_COLOR>::kBytes, s>>>(a);
+        break;
+    case PASS_DEPTH_FRAG:
+        raster_kernel<PASS_DEPTH_FRAG><<<grid, kThreads, TileCfg<PASS_DEPTH>::kBytes, s>>>(a);
+        break;
+    case PASS_COLOR_FRAG:
+        raster_kernel<PASS_COLOR_FRAG><<<grid, kThreads, TileCfg<PASS_COLOR>::kBytes, s>>>(a);
         break;
     default:
         raster_kernel<PASS_NEAREST><<<grid, kThreads, TileCfg<PASS_NEAREST>::kBytes, s>>>(a);
