@@ -439,6 +439,30 @@ CR_API cr_status cr_synth_terrain_points(cr_context *ctx, const cr_synth_terrain
 CR_API cr_status cr_synth_lattice_points(cr_context *ctx, uint64_t seed, uint32_t n_axis, float lo,
                                          float hi, float jitter, void *device_records);
 
+/* ------------------------------------------------------------------------ */
+/* Allocation-free cull                                                      */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory — plug-ins whose host application owns every device allocation,
+ * real-time loops that cannot take cudaMalloc's device-wide synchronisation
+ * mid-frame — this runs the same ordered cull as cr_render on arrays the
+ * caller owns: `batches` (nbatches slots), `files` (nfiles) and the outputs
+ * `visible` (room for nbatches records) and `count` (one uint32) are device
+ * pointers; config and camera are host structs; `stream` is a cudaStream_t
+ * (NULL = the legacy default stream) the work is queued on.  It allocates
+ * nothing: its scratch (one count per 256 slots) is a fixed array in the
+ * library's device image, held by every GPU that loads the library until the
+ * process exits, so at most 1,048,576 slots are accepted (CR_ERR_CAPACITY
+ * above that).  The first call on a device looks up that array's address on
+ * the current device; make it before any stream capture.  All calls share the
+ * array: calls whose work overlaps on the GPU race.  Asynchronous: the
+ * results are valid once the stream has reached them. */
+CR_API cr_status cr_cull_noalloc(const cr_raster_batch *batches, uint32_t nbatches,
+                                 const cr_raster_file *files, uint32_t nfiles,
+                                 const cr_config *config, const cr_camera *camera, int width,
+                                 int height, cr_visible_batch *visible, uint32_t *count,
+                                 void *stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -138,6 +138,8 @@ PROTOTYPES = {
     "cr_synth_terrain_height": (C.c_float, [C.POINTER(cr_synth_terrain), C.c_float, C.c_float]),
     "cr_synth_terrain_points": (C.c_int, [P, C.POINTER(cr_synth_terrain), u64, u64, P]),
     "cr_synth_lattice_points": (C.c_int, [P, u64, u32, C.c_float, C.c_float, C.c_float, P]),
+    "cr_cull_noalloc": (C.c_int, [P, u32, P, u32, C.POINTER(cr_config), C.POINTER(cr_camera),
+                                  C.c_int, C.c_int, P, P, P]),
     "cr_pack": (C.c_int, [P, P, C.POINTER(cr_pack_input), u64, C.POINTER(cr_pack_params),
                           C.c_int, P]),
     "cr_pack_chunks": (C.c_int, [P, P, P, P, u32, C.POINTER(cr_pack_params), C.c_int, P,

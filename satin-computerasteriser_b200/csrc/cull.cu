@@ -15,6 +15,10 @@
 //      `chunkPoints` survivor points; the last CTA publishes the totals (the
 //      CUDA counterpart of the indirect argument buffer).
 #include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
 
 #include "cr_device.cuh"
 #include "cr_internal.h"
@@ -269,6 +273,129 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s) {
     cull_compact<<<ctas, kCullThreads, 0, s>>>(cloud->d_cull_tmp, cloud->d_cull_cta,
                                                cloud->d_visible, cloud->d_chunks, cp,
                                                cloud->d_counters);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free cull (cr_cull_noalloc)
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory: plug-ins whose host application
+// owns every device allocation (a fixed budget or its own allocator), and
+// real-time loops that cannot afford cudaMalloc's implicit device-wide
+// synchronisation in the middle of a frame.  For them this variant of the
+// cull takes device inputs and outputs from the caller and keeps its only
+// scratch — one survivor count per 256-slot CTA — in the file-scope array
+// below, which every GPU that loads the library holds until the process
+// exits.  Every slot of the scratch a call reads is written by the same call
+// first, so nothing has to start at zero.  All calls share the one array:
+// two calls that overlap on the GPU race on it.
+
+namespace {
+
+constexpr uint32_t kNoAllocMaxSlots = 1u << 20;  // 1,048,576 batch slots
+constexpr uint32_t kNoAllocMaxCtas = kNoAllocMaxSlots / kCullThreads;
+
+static __device__ __align__(256) uint32_t g_noalloc_cta_counts[kNoAllocMaxCtas];
+
+__global__ void __launch_bounds__(kCullThreads)
+    cull_noalloc_count(CullArgs a, uint32_t *cta_counts) {
+    __shared__ uint32_t warp_counts[kCullThreads / 32];
+    const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
+    CullRec rec;
+    const bool keep = gid < a.nbatches && cull_slot(a, gid, rec);
+    const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
+    if ((threadIdx.x & 31) == 0) warp_counts[threadIdx.x >> 5] = __popc(ballot);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t total = 0;
+        for (int w = 0; w < kCullThreads / 32; ++w) total += warp_counts[w];
+        cta_counts[blockIdx.x] = total;
+    }
+}
+
+__global__ void __launch_bounds__(kCullThreads)
+    cull_noalloc_write(CullArgs a, const uint32_t *cta_counts, cr_visible_batch *out,
+                       uint32_t *count_out) {
+    __shared__ uint32_t part[kCullThreads / 32], warp_counts[kCullThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t s = 0;
+    for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kCullThreads) s += cta_counts[i];
+    s = __reduce_add_sync(0xffffffffu, s);
+    if (lane == 0) part[warp] = s;
+    const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
+    CullRec rec;
+    const bool keep = gid < a.nbatches && cull_slot(a, gid, rec);
+    const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) warp_counts[warp] = __popc(ballot);
+    __syncthreads();
+    uint32_t offset = 0, before = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kCullThreads / 32; ++w) {
+        offset += part[w];
+        if (w < warp) before += warp_counts[w];
+        total += warp_counts[w];
+    }
+    if (keep) out[offset + before + __popc(ballot & ((1u << lane) - 1u))] = rec.vb;
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *count_out = offset + total;
+}
+
+std::mutex g_noalloc_mutex;
+std::vector<uint32_t *> g_noalloc_scratch;  // device address of the array, per device
+
+// The array's device address on the current device; the first call on a
+// device looks it up (cudaGetSymbolAddress), later calls reuse it.
+cr_status noalloc_scratch(uint32_t **out) {
+    int dev = 0;
+    CR_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if ((size_t)dev >= g_noalloc_scratch.size()) g_noalloc_scratch.resize(dev + 1, nullptr);
+    if (!g_noalloc_scratch[dev]) {
+        void *p = nullptr;
+        CR_CUDA(cudaGetSymbolAddress(&p, g_noalloc_cta_counts));
+        g_noalloc_scratch[dev] = static_cast<uint32_t *>(p);
+    }
+    *out = g_noalloc_scratch[dev];
+    return CR_OK;
+}
+
+}  // namespace
+
+extern "C" CR_API cr_status cr_cull_noalloc(const cr_raster_batch *batches, uint32_t nbatches,
+                                            const cr_raster_file *files, uint32_t nfiles,
+                                            const cr_config *config, const cr_camera *camera,
+                                            int width, int height, cr_visible_batch *visible,
+                                            uint32_t *count, void *stream) {
+    if (!config || !camera || !count || (nbatches && (!batches || !visible)) || !files ||
+        nfiles == 0)
+        return cri::fail(CR_ERR_INVALID_ARGUMENT, "null argument or empty file table");
+    if (width <= 0 || height <= 0)
+        return cri::fail(CR_ERR_INVALID_ARGUMENT, "width and height must be positive");
+    if (nbatches > kNoAllocMaxSlots)
+        return cri::fail(CR_ERR_CAPACITY,
+                         "cr_cull_noalloc handles at most 1048576 batch slots (got " +
+                             std::to_string(nbatches) + ")");
+    uint32_t *scratch = nullptr;
+    cr_status st = noalloc_scratch(&scratch);
+    if (st) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (nbatches == 0) {
+        CR_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t), s));
+        return CR_OK;
+    }
+    CullUniforms u;
+    std::memcpy(u.view, camera->view, sizeof(u.view));
+    std::memcpy(u.proj, camera->projection, sizeof(u.proj));
+    u.width = width;
+    u.height = height;
+    u.enableFrustumCulling = config->enableFrustumCulling != 0;
+    u.lodBias = config->lodBias;
+    u.enableCLOD = config->enableCLOD != 0;
+    CullArgs a{batches, nbatches, files, nfiles, nullptr, nullptr, (uint32_t)kMinChunkPoints, u};
+    const uint32_t ctas = (nbatches + kCullThreads - 1) / kCullThreads;
+    cull_noalloc_count<<<ctas, kCullThreads, 0, s>>>(a, scratch);
+    CR_CUDA(cudaGetLastError());
+    cull_noalloc_write<<<ctas, kCullThreads, 0, s>>>(a, scratch, visible, count);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }
