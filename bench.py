@@ -326,7 +326,9 @@ def run_ours(args, dist):
     dom_ms = times[:, dom].astype(np.float64)
     achieved = float(dom_bytes.mean() / (dom_ms.mean() / 1e3) / 1e9)
     peak, peak_kind = measured_peaks()
-    kernel = {"depth": "raster_kernel<0>", "color": "raster_kernel<1>"}.get(PASS_NAMES[dom],
+    # Single-pixel footprints: the depth pass emits fragments (PASS_DEPTH_FRAG
+    # = 3) and the colour pass reads them (PASS_COLOR_FRAG = 4).
+    kernel = {"depth": "raster_kernel<3>", "color": "raster_kernel<4>"}.get(PASS_NAMES[dom],
                                                                          PASS_NAMES[dom])
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
@@ -357,7 +359,11 @@ def run_ours(args, dist):
            "scaling": "weak", "vs_baseline": None, "dtype": "f32+u32",
            "data": "synthetic (seeded fractal heightfield, generated and packed on the GPU)",
            "config": config_dict(args), "e2e": e2e, "roofline": roofline, "clocks": clocks,
-           "gpu_launches": int(args.steps * (5 if args.mode == "hqs" else 4)),
+           # HQS: cull (classify, compact), depth, colour, resolve, and the
+           # exact re-run's clear, colour and resolve, which return at once
+           # unless a pixel passed 16,843,009 samples; nearest: cull (2),
+           # nearest pass, resolve.
+           "gpu_launches": int(args.steps * (8 if args.mode == "hqs" else 4)),
            "pass_ms": {n: round(float(v), 4) for n, v in zip(PASS_NAMES, avg)},
            "survivor_points_per_frame": int(active.mean()),
            "tuning": ctx.tuning(),

@@ -711,16 +711,17 @@ CR_API cr_status cr_frame_create(cr_context *ctx, int w, int h, cr_frame **out) 
     f->height = h;
     const size_t npix = (size_t)w * h;
     cr_status st;
-    if ((st = dalloc(&f->d_depth, npix * 4)) || (st = dalloc(&f->d_accum, npix * 16)) ||
+    if ((st = dalloc(&f->d_depth, npix * 4)) || (st = dalloc(&f->d_accum, (npix + 1) * 16)) ||
         (st = dalloc(&f->d_nearest, npix * 8)) || (st = dalloc(&f->d_rgba[0], npix * 4)) ||
         (st = dalloc(&f->d_rgba[1], npix * 4)) || (st = dalloc(&f->d_depthf, npix * 4))) {
         std::string d = cr_last_error_detail();
         cr_frame_destroy(f);
         return fail(st, d);
     }
+    f->d_redo = reinterpret_cast<uint32_t *>(f->d_accum + npix);
     cudaStream_t s = ctx->stream;
     cudaMemsetAsync(f->d_depth, 0, npix * 4, s);
-    cudaMemsetAsync(f->d_accum, 0, npix * 16, s);
+    cudaMemsetAsync(f->d_accum, 0, (npix + 1) * 16, s);
     cudaMemsetAsync(f->d_nearest, 0, npix * 8, s);
     cudaMemsetAsync(f->d_rgba[0], 0, npix * 4, s);
     cudaMemsetAsync(f->d_rgba[1], 0, npix * 4, s);
@@ -768,14 +769,24 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
         {
             PassTimer pt(ctx, CR_PASS_CLEAR);
             CR_CUDA(cudaMemsetAsync(f->d_depth, 0, npix * 4, s));
-            CR_CUDA(cudaMemsetAsync(f->d_accum, 0, npix * 16, s));
+            CR_CUDA(cudaMemsetAsync(f->d_accum, 0, (npix + 1) * 16, s));  // + redo flag
         }
         std::vector<cr_cloud *> resident;
+        uint64_t max_samples = 0;  // upper bound on the frame's colour samples
         for (uint32_t i = 0; i < nclouds; ++i)
-            if (clouds[i]->resident > 0) resident.push_back(clouds[i]);
+            if (clouds[i]->resident > 0) {
+                resident.push_back(clouds[i]);
+                max_samples += (uint64_t)clouds[i]->resident * clouds[i]->cap.pointsPerBatch;
+            }
         const CullUniforms cu = make_cull_uniforms(cfg, cam, W, H);
         const RasterUniforms rau = make_raster_uniforms(cfg, cam, W, H);
-        const RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
+        // Packed colour adds while the frame holds fewer than 2^31 samples:
+        // then a pixel's count field reads its true count plus at most 127
+        // carries out of the blue sum, so a read count of at most
+        // kPackedMaxCount proves that no field carried.
+        const bool packed = max_samples < (1ull << 31);
+        RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
+        t.packed = packed ? 1 : 0;
         {
             PassTimer pt(ctx, CR_PASS_CULL);
             for (cr_cloud *c : resident)
@@ -799,7 +810,20 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
         }
         {
             PassTimer pt(ctx, CR_PASS_RESOLVE);
-            if ((st = launch_resolve_hqs(f, ru, s))) return st;
+            if ((st = launch_resolve_hqs(f, ru, s, packed, nullptr))) return st;
+            if (packed) {
+                // Exact re-run, which returns at once unless the resolve set
+                // the redo flag: zero the accumulators, colour pass with one
+                // 32-bit add per field, resolve.
+                RasterTargets tx = t;
+                tx.packed = 0;
+                tx.redo = f->d_redo;
+                if ((st = launch_accum_redo_clear(f, s))) return st;
+                for (cr_cloud *c : resident)
+                    if ((st = launch_raster(c, frags ? PASS_COLOR_FRAG : PASS_COLOR, rau, tx, s)))
+                        return st;
+                if ((st = launch_resolve_hqs(f, ru, s, false, f->d_redo))) return st;
+            }
         }
         f->last_mode = 0;
     } else {

@@ -148,7 +148,8 @@ struct cr_frame {
     cr_context *ctx = nullptr;
     int width = 0, height = 0;
     uint32_t *d_depth = nullptr;            // HQS depth plane (RasterPixel.depth)
-    uint4 *d_accum = nullptr;               // HQS red, green, blue, count
+    uint4 *d_accum = nullptr;               // HQS red, green, blue, count (+1 entry: redo flag)
+    uint32_t *d_redo = nullptr;             // word 0 of d_accum[width * height]
     unsigned long long *d_nearest = nullptr;  // (depth << 32) | ~pointIndex
     uint32_t *d_rgba[2] = {nullptr, nullptr}; // RGBA8 ping-pong (resolve, hole fill)
     float *d_depthf = nullptr;              // resolve R32F depth
@@ -196,7 +197,18 @@ struct RasterTargets {
     uint32_t *depth;              // HQS depth plane
     uint4 *accum;                 // HQS accumulators
     unsigned long long *nearest;  // nearest key plane
+    // Colour adds as two 64-bit words per pixel (R | G << 32, B | count << 32)
+    // instead of four 32-bit ones; exact while a pixel holds at most
+    // kPackedMaxCount samples, which the resolve checks.
+    int packed = 0;
+    // Non-null: the pass runs only if *redo != 0 (the exact re-run of a
+    // frame whose resolve found a pixel past kPackedMaxCount).
+    const uint32_t *redo = nullptr;
 };
+
+// Largest per-pixel sample count whose 8-bit channel sums cannot wrap a
+// 32-bit field: 255 * 16843009 = 2^32 - 1.
+constexpr uint32_t kPackedMaxCount = 16843009u;
 
 cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
                         const RasterTargets &t, cudaStream_t s);
@@ -206,7 +218,12 @@ struct ResolveUniforms {
     float background[4];
 };
 
-cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t s);
+// check: set *f->d_redo when a pixel's count exceeds kPackedMaxCount (the
+// colour pass used packed adds).  redo: run only if *redo != 0.
+cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t s, bool check,
+                             const uint32_t *redo);
+// Zeroes the accumulators if *f->d_redo != 0.
+cr_status launch_accum_redo_clear(cr_frame *f, cudaStream_t s);
 cr_status launch_resolve_nearest(cr_frame *f, const uint32_t *colors, const ResolveUniforms &u,
                                  cudaStream_t s);
 cr_status launch_hole_fill(cr_frame *f, int iterations, cudaStream_t s);

@@ -56,7 +56,7 @@ struct TileCfg<PASS_DEPTH> {
 };
 template <>
 struct TileCfg<PASS_COLOR> {
-    static constexpr int kPx = 2048;
+    static constexpr int kPx = 4096;
     static constexpr int kBytes = kPx * 16;  // R|count, G, B accumulators + settled depth
 };
 template <>
@@ -160,13 +160,25 @@ __device__ __forceinline__ unsigned long long nearest_key(uint32_t depth, uint32
     return ((unsigned long long)depth << 32) | (unsigned long long)(~index);
 }
 
+// Adds one sample group to a pixel's R, G, B and count.  Packed: the uint4
+// as two 64-bit words, R | G << 32 and B | count << 32 — half the global
+// atomics.  A lower field that passes 2^32 would carry into its neighbour;
+// that needs more than kPackedMaxCount samples in the pixel, which the
+// resolve detects (the frame is then re-run unpacked).  Unpacked: one
+// 32-bit add per field.
 __device__ __forceinline__ void color_global(const RasterArgs &a, uint32_t pix, uint32_t r,
                                              uint32_t g, uint32_t b, uint32_t n) {
-    unsigned int *acc = reinterpret_cast<unsigned int *>(&a.t.accum[pix]);
-    atomicAdd(acc + 0, r);
-    atomicAdd(acc + 1, g);
-    atomicAdd(acc + 2, b);
-    atomicAdd(acc + 3, n);
+    if (a.t.packed) {
+        unsigned long long *w = reinterpret_cast<unsigned long long *>(&a.t.accum[pix]);
+        atomicAdd(w, (unsigned long long)r | ((unsigned long long)g << 32));
+        atomicAdd(w + 1, (unsigned long long)b | ((unsigned long long)n << 32));
+    } else {
+        unsigned int *acc = reinterpret_cast<unsigned int *>(&a.t.accum[pix]);
+        atomicAdd(acc + 0, r);
+        atomicAdd(acc + 1, g);
+        atomicAdd(acc + 2, b);
+        atomicAdd(acc + 3, n);
+    }
 }
 
 // Direct path, radius 0: one global atomic per point (batches large on
@@ -313,6 +325,48 @@ __device__ __forceinline__ void do_fragment(const RasterArgs &a, unsigned char *
         emit_direct<PASS_COLOR_FRAG>(a, o);
 }
 
+// Four fragments of one thread in the colour pass, the first `nvalid` of
+// them real.  The settled depths of all four pixels are read (read-only
+// path, or the tile's staged copy) before any accumulation, so the thread
+// waits for one L2 round trip per quad instead of one per fragment.
+__device__ __forceinline__ void color_quad(const RasterArgs &a, unsigned char *smem,
+                                           const ChunkRec &c, bool tiled, uint32_t nvalid,
+                                           const uint4 &xy4, const float4 &z4, const uint4 &co4) {
+    constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
+    uint32_t *acc = reinterpret_cast<uint32_t *>(smem);
+    const uint32_t *sdep = acc + 3 * kPx;
+    const uint32_t xy[4] = {xy4.x, xy4.y, xy4.z, xy4.w};
+    const float nz[4] = {z4.x, z4.y, z4.z, z4.w};
+    const uint32_t col[4] = {co4.x, co4.y, co4.z, co4.w};
+    uint32_t pix[4], closest[4];
+    int l[4];
+    bool in[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int ix = (int)(xy[i] & 0xffffu), iy = (int)(xy[i] >> 16);
+        pix[i] = (uint32_t)(iy * a.u.width + ix);
+        const int lx = ix - c.x0, ly = iy - c.y0;
+        in[i] = tiled && (unsigned)lx < (unsigned)c.tw && (unsigned)ly < (unsigned)c.th;
+        l[i] = in[i] ? ly * c.tw + lx : 0;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        closest[i] = 0u;
+        if ((uint32_t)i < nvalid) closest[i] = in[i] ? sdep[l[i]] : __ldg(a.t.depth + pix[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const bool vis = closest[i] != 0u && nz[i] >= crd::uint_to_depth(closest[i]) * a.keep_scale;
+        const uint32_t r = col[i] & 0xffu, g = (col[i] >> 8) & 0xffu, b = (col[i] >> 16) & 0xffu;
+        if (vis && in[i]) {
+            atomicAdd(acc + l[i], r | (1u << 20));
+            atomicAdd(acc + kPx + l[i], g);
+            atomicAdd(acc + 2 * kPx + l[i], b);
+        }
+        if (vis && !in[i]) color_global(a, pix[i], r, g, b, 1u);
+    }
+}
+
 template <int PASS>
 __device__ __forceinline__ void tile_init(const RasterArgs &a, const ChunkRec &c,
                                           unsigned char *smem) {
@@ -383,6 +437,7 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
     __shared__ BatchShared sb;
     __shared__ __align__(16) ChunkRec rec[2];
     __shared__ __align__(16) uint32_t rec_frags[2][4];
+    if (a.t.redo && *a.t.redo == 0u) return;
     const uint32_t nchunks = a.counters[CNT_CHUNKS];
     uint32_t k = blockIdx.x;
     if (k >= nchunks) return;
@@ -408,8 +463,9 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
             cp_async4(&rec_frags[buf ^ 1][0], a.frag_count + kn);
         cp_async_commit();
         const bool new_file = c.file != sb.file;
+        const uint32_t work = PASS == PASS_COLOR_FRAG ? nfrag : c.count;
         const bool tiled = a.use_tiles && a.radius_zero && c.tw > 0 &&
-                           c.tw * c.th <= TileCfg<PASS>::kPx && c.tw * c.th <= (int)(2 * c.count) &&
+                           c.tw * c.th <= TileCfg<PASS>::kPx && c.tw * c.th <= (int)(2 * work) &&
                            (!is_color(PASS) || c.count < 4096u);
         if (new_file || tiled) {
             __syncthreads();  // everyone has read sb.file
@@ -440,11 +496,8 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
                         z4 = __ldcs(reinterpret_cast<const float4 *>(a.frag_z + base));
                         co4 = __ldcs(reinterpret_cast<const uint4 *>(a.frag_col + base));
                     }
-                    const uint32_t l0 = 4u * q;
-                    do_fragment(a, smem, c, tiled, l0 + 0 < nfrag, xy4.x, z4.x, co4.x);
-                    do_fragment(a, smem, c, tiled, l0 + 1 < nfrag, xy4.y, z4.y, co4.y);
-                    do_fragment(a, smem, c, tiled, l0 + 2 < nfrag, xy4.z, z4.z, co4.z);
-                    do_fragment(a, smem, c, tiled, l0 + 3 < nfrag, xy4.w, z4.w, co4.w);
+                    const uint32_t nv = q < nquads ? min(4u, nfrag - 4u * q) : 0u;
+                    color_quad(a, smem, c, tiled, nv, xy4, z4, co4);
                 }
             } else {
                 for (uint32_t l0 = 0; l0 < nfrag; l0 += kThreads) {

@@ -22,19 +22,24 @@ __device__ __forceinline__ uint32_t pack_rgba(float r, float g, float b, float a
 __global__ void __launch_bounds__(kThreads)
     resolve_hqs(const uint32_t *__restrict__ depth, const uint4 *__restrict__ accum,
                 uint32_t *__restrict__ rgba, float *__restrict__ depthf, uint32_t npix,
-                ResolveUniforms u) {
-    const uint32_t p = blockIdx.x * kThreads + threadIdx.x;
-    if (p >= npix) return;
-    const uint4 acc = accum[p];
-    if (acc.w == 0u) {
-        rgba[p] = pack_rgba(u.background[0], u.background[1], u.background[2], 0.0f);
-        depthf[p] = 0.0f;
-        return;
+                ResolveUniforms u, uint32_t *redo_flag, int check, const uint32_t *redo) {
+    if (redo && *redo == 0u) return;
+    for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < npix; p += gridDim.x * kThreads) {
+        const uint4 acc = accum[p];
+        // Packed colour adds are exact while every count is at most
+        // kPackedMaxCount: past it a channel sum may have carried into its
+        // neighbour field, and the frame's colour pass is re-run exactly.
+        if (check && acc.w > kPackedMaxCount) *redo_flag = 1u;
+        if (acc.w == 0u) {
+            rgba[p] = pack_rgba(u.background[0], u.background[1], u.background[2], 0.0f);
+            depthf[p] = 0.0f;
+            continue;
+        }
+        const float inv = 1.0f / (float)acc.w;
+        rgba[p] = pack_rgba(((float)acc.x * inv) / 255.0f, ((float)acc.y * inv) / 255.0f,
+                            ((float)acc.z * inv) / 255.0f, 1.0f);
+        depthf[p] = crd::uint_to_depth(depth[p]);
     }
-    const float inv = 1.0f / (float)acc.w;
-    rgba[p] = pack_rgba(((float)acc.x * inv) / 255.0f, ((float)acc.y * inv) / 255.0f,
-                        ((float)acc.z * inv) / 255.0f, 1.0f);
-    depthf[p] = crd::uint_to_depth(depth[p]);
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -101,15 +106,33 @@ __global__ void __launch_bounds__(kThreads)
     if (index) index[p] = ~(uint32_t)k;
 }
 
+__global__ void __launch_bounds__(kThreads)
+    accum_redo_clear(uint4 *__restrict__ accum, const uint32_t *redo, uint32_t npix) {
+    if (*redo == 0u) return;
+    for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < npix; p += gridDim.x * kThreads)
+        accum[p] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 }  // namespace
 
-cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t s) {
+cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t s, bool check,
+                             const uint32_t *redo) {
     const uint32_t npix = (uint32_t)f->width * (uint32_t)f->height;
-    resolve_hqs<<<(npix + kThreads - 1) / kThreads, kThreads, 0, s>>>(f->d_depth, f->d_accum,
-                                                                      f->d_rgba[0], f->d_depthf,
-                                                                      npix, u);
+    // One pixel per thread; the gated re-run (rarely needed) uses a small
+    // grid-stride grid so that skipping it costs little.
+    const uint32_t grid = redo ? (uint32_t)f->ctx->sm_count * 4 : (npix + kThreads - 1) / kThreads;
+    resolve_hqs<<<grid, kThreads, 0, s>>>(
+        f->d_depth, f->d_accum, f->d_rgba[0], f->d_depthf, npix, u, f->d_redo, check ? 1 : 0,
+        redo);
     CR_CUDA(cudaGetLastError());
     f->final_rgba = 0;
+    return CR_OK;
+}
+
+cr_status launch_accum_redo_clear(cr_frame *f, cudaStream_t s) {
+    const uint32_t npix = (uint32_t)f->width * (uint32_t)f->height;
+    accum_redo_clear<<<f->ctx->sm_count * 4, kThreads, 0, s>>>(f->d_accum, f->d_redo, npix);
+    CR_CUDA(cudaGetLastError());
     return CR_OK;
 }
 
