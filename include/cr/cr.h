@@ -440,6 +440,43 @@ CR_API cr_status cr_synth_lattice_points(cr_context *ctx, uint64_t seed, uint32_
                                          float hi, float jitter, void *device_records);
 
 /* ------------------------------------------------------------------------ */
+/* Batched views                                                             */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference, whose renderer draws one viewport per
+ * ComputeRasteriser.encode (ComputeRasteriser.swift:277-296).  Renders
+ * `nviews` (1..256) HQS views of the same clouds, view v with camera cams[v]
+ * into frames[v] (distinct frames, any sizes), in one CUDA-graph launch: the
+ * per-view cull, depth, colour, resolve and hole-fill work of all views runs
+ * in shared launches.  models: nclouds column-major model matrices (the
+ * ComputeRasteriserPointCloud.worldMatrix each cloud's file table is
+ * multiplied by, as cr_cloud_update_files does), or NULL for identity.  Each
+ * view's planes are bit-identical to cr_render of that view after
+ * cr_cloud_update_files(cloud, projection * view, model, NULL, NULL).  The
+ * graph is captured on the first call and whenever the frames, clouds,
+ * configuration or tuning change; do not call it while capturing.
+ * Asynchronous; the frames' read functions synchronise.  HQS only
+ * (CR_ERR_UNSUPPORTED for the nearest mode); holeFillIterations <= 64. */
+CR_API cr_status cr_render_multiview(cr_context *ctx, cr_frame *const *frames,
+                                     const cr_camera *cams, uint32_t nviews,
+                                     cr_cloud *const *clouds, const float *models,
+                                     uint32_t nclouds, const cr_config *cfg);
+
+/* Autotuner of cr_render_multiview's launch shape (no counterpart in the
+ * reference): times chunkPoints in {512, 1024, 2048, 4096} (points per
+ * thread = chunkPoints / 256) with and without screen tiles, `reps` renders
+ * each after two warm-up renders, sets the fastest on the context and
+ * returns it (and its ms per render).  With cache_path, a result is appended
+ * to that file as one JSON object per line keyed by a workload signature
+ * (device, SM count, views, pixels, points, configuration), and a later call
+ * with the same signature reads it instead of timing.  Synchronises. */
+CR_API cr_status cr_autotune_multiview(cr_context *ctx, cr_frame *const *frames,
+                                       const cr_camera *cams, uint32_t nviews,
+                                       cr_cloud *const *clouds, const float *models,
+                                       uint32_t nclouds, const cr_config *cfg,
+                                       const char *cache_path, int reps, cr_tuning *best,
+                                       float *best_ms);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free cull                                                      */
 /* ------------------------------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device

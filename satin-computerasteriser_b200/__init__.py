@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 from dataclasses import dataclass, field, fields
 
 import numpy as np
@@ -30,7 +31,7 @@ __all__ = ["Context", "ComputeRasteriserConfiguration", "ComputeRasteriserCapaci
            "VISIBLE_DTYPE", "computeRasteriserThreadsPerGroup", "MODE_HQS", "MODE_NEAREST",
            "identity_files", "matrix_multiply", "GPUPacker", "PackInput", "DeviceBuffer",
            "HostBuffer", "TerrainParams", "synth_terrain", "synth_lattice", "terrain_height",
-           "PASS_NAMES"]
+           "PASS_NAMES", "MultiViewRasteriser"]
 
 PASS_NAMES = ("clear", "cull", "depth", "color", "resolve", "hole_fill")
 
@@ -633,6 +634,25 @@ class _Frame:
         except Exception:
             pass
 
+    # Read-backs (synchronise the context's stream; row 0 = top).
+    def rgba8(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros((self.height, self.width, 4), np.uint8)
+        elif out.nbytes < self.width * self.height * 4 or not out.flags.c_contiguous:
+            raise CRError(1, "out is too small or not contiguous")
+        N.check(N.lib().cr_frame_read_rgba8(self._h, N.ptr(out)))
+        return out
+
+    def depth_f32(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width), np.float32)
+        N.check(N.lib().cr_frame_read_depth_f32(self._h, N.ptr(out)))
+        return out
+
+    def pixels(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width), PIXEL_DTYPE)
+        N.check(N.lib().cr_frame_read_pixels(self._h, N.ptr(out)))
+        return out
+
 
 class PerspectiveCamera:
     """A Satin-style perspective camera: right-handed view (looks down -Z) and
@@ -822,3 +842,80 @@ class ComputeRasteriser:
         if self._frame is None:
             raise CRError(1, "no viewport: call resize or update first")
         return self._frame
+
+
+class MultiViewRasteriser:
+    """Batched HQS rendering of many views of the same clouds in one CUDA-graph
+    launch (cr_render_multiview); no counterpart in the reference, whose
+    ComputeRasteriser draws one viewport per encode.
+
+    ``sizes`` fixes the views' (width, height); ``render(cameras)`` draws view
+    i with cameras[i] into its own frame, bit-identical to a ComputeRasteriser
+    update + encode of that camera at that size.  ``autotune`` picks the
+    launch shape (cr_autotune_multiview), optionally cached in a JSON-lines
+    file.
+    """
+
+    def __init__(self, context: Context, sizes):
+        sizes = list(sizes)
+        if not 1 <= len(sizes) <= 256:
+            raise CRError(1, "between 1 and 256 views")
+        self.context = context
+        self.configuration = ComputeRasteriserConfiguration()
+        self._clouds: list[ComputeRasteriserPointCloud] = []
+        self.frames = [_Frame(context, int(w), int(h)) for w, h in sizes]
+
+    def addPointCloud(self, cloud: ComputeRasteriserPointCloud) -> ComputeRasteriserPointCloud:
+        self._clouds.append(cloud)
+        return cloud
+
+    def removePointCloud(self, cloud: ComputeRasteriserPointCloud):
+        self._clouds = [c for c in self._clouds if c is not cloud]
+
+    @property
+    def viewCount(self) -> int:
+        return len(self.frames)
+
+    def _args(self, cameras):
+        if len(cameras) != len(self.frames):
+            raise CRError(1, "one camera per view")
+        frames = (C.c_void_p * len(self.frames))(*[f.handle.value for f in self.frames])
+        cams = (N.cr_camera * len(cameras))(*[_camera_c(c) for c in cameras])
+        clouds = [c for c in self._clouds if c.visible]
+        arr = (C.c_void_p * max(len(clouds), 1))(*[c.handle.value for c in clouds])
+        models = np.zeros((max(len(clouds), 1), 16), np.float32)
+        for i, c in enumerate(clouds):
+            models[i] = _mat16(c.worldMatrix)
+        return frames, cams, arr, len(clouds), models
+
+    def render(self, cameras):
+        frames, cams, arr, n, models = self._args(cameras)
+        cfg = self.configuration.to_c()
+        N.check(N.lib().cr_render_multiview(self.context.handle, frames, cams, len(self.frames),
+                                            arr, N.ptr(models), n, C.byref(cfg)))
+
+    def autotune(self, cameras, cachePath: str | None = None, reps: int = 5) -> dict:
+        frames, cams, arr, n, models = self._args(cameras)
+        cfg = self.configuration.to_c()
+        best = N.cr_tuning()
+        ms = C.c_float()
+        path = None if cachePath is None else os.fsencode(cachePath)
+        N.check(N.lib().cr_autotune_multiview(self.context.handle, frames, cams,
+                                              len(self.frames), arr, N.ptr(models), n,
+                                              C.byref(cfg), path, int(reps), C.byref(best),
+                                              C.byref(ms)))
+        return {"chunkPoints": best.chunkPoints, "useTiles": bool(best.useTiles),
+                "ms": float(ms.value)}
+
+    def outputRGBA8(self, view: int, out: np.ndarray | None = None) -> np.ndarray:
+        return self.frames[view].rgba8(out)
+
+    def depthTexture(self, view: int) -> np.ndarray:
+        return self.frames[view].depth_f32()
+
+    def pixels(self, view: int) -> np.ndarray:
+        return self.frames[view].pixels()
+
+    def close(self):
+        for f in self.frames:
+            f.close()

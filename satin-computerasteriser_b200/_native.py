@@ -140,6 +140,10 @@ PROTOTYPES = {
     "cr_synth_lattice_points": (C.c_int, [P, u64, u32, C.c_float, C.c_float, C.c_float, P]),
     "cr_cull_noalloc": (C.c_int, [P, u32, P, u32, C.POINTER(cr_config), C.POINTER(cr_camera),
                                   C.c_int, C.c_int, P, P, P]),
+    "cr_render_multiview": (C.c_int, [P, P, P, u32, P, P, u32, C.POINTER(cr_config)]),
+    "cr_autotune_multiview": (C.c_int, [P, P, P, u32, P, P, u32, C.POINTER(cr_config),
+                                        C.c_char_p, C.c_int, C.POINTER(cr_tuning),
+                                        C.POINTER(C.c_float)]),
     "cr_pack": (C.c_int, [P, P, C.POINTER(cr_pack_input), u64, C.POINTER(cr_pack_params),
                           C.c_int, P]),
     "cr_pack_chunks": (C.c_int, [P, P, P, P, u32, C.POINTER(cr_pack_params), C.c_int, P,

@@ -277,13 +277,7 @@ cr_status validate_render(cr_context *ctx, cr_frame *frame, const cr_config *cfg
                           const cr_camera *cam) {
     if (!ctx || !frame || !cfg || !cam) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
     if (frame->ctx != ctx) return fail(CR_ERR_INVALID_ARGUMENT, "frame belongs to another context");
-    if (cfg->mode != CR_MODE_HIGH_QUALITY_AVERAGE && cfg->mode != CR_MODE_NEAREST_POINT)
-        return fail(CR_ERR_INVALID_ARGUMENT, "config.mode must be 0 (HQS) or 1 (nearest)");
-    if (cfg->pointSizeMode != 0 && cfg->pointSizeMode != 1)
-        return fail(CR_ERR_INVALID_ARGUMENT, "config.pointSizeMode must be 0 or 1");
-    std::string why;
-    if (config_unsupported(cfg, why)) return fail(CR_ERR_UNSUPPORTED, why);
-    return CR_OK;
+    return validate_config(cfg);
 }
 
 // encodeNearestIndexPass (ComputeRasteriser.swift:505-522) into the frame's key plane.
@@ -307,6 +301,16 @@ int trunc_i(float x) {
 }
 
 }  // namespace
+
+cr_status validate_config(const cr_config *cfg) {
+    if (cfg->mode != CR_MODE_HIGH_QUALITY_AVERAGE && cfg->mode != CR_MODE_NEAREST_POINT)
+        return fail(CR_ERR_INVALID_ARGUMENT, "config.mode must be 0 (HQS) or 1 (nearest)");
+    if (cfg->pointSizeMode != 0 && cfg->pointSizeMode != 1)
+        return fail(CR_ERR_INVALID_ARGUMENT, "config.pointSizeMode must be 0 or 1");
+    std::string why;
+    if (config_unsupported(cfg, why)) return fail(CR_ERR_UNSUPPORTED, why);
+    return CR_OK;
+}
 
 // ===========================================================================
 // Exported API
@@ -401,6 +405,7 @@ CR_API cr_status cr_context_destroy(cr_context *ctx) {
         pack_scratch_free(*ctx->pack);
         delete ctx->pack;
     }
+    if (ctx->views) views_destroy(ctx->views);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CR_OK;

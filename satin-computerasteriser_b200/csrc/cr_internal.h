@@ -40,6 +40,8 @@ enum CounterSlot : int {
 };
 
 struct PackScratch;
+struct ViewsState;
+void views_destroy(ViewsState *s);
 
 // One survivor of the cull with the per-batch values the point passes need
 // (cull_classify output, 64 bytes).
@@ -72,10 +74,12 @@ constexpr int kMinChunkPoints = 256;
 
 struct cr_context {
     PackScratch *pack = nullptr;  // grow-only packer scratch
+    ViewsState *views = nullptr;  // buffers and graphs of the last batched render
     int device = 0;
     cudaStream_t stream = nullptr;
     int sm_count = 0;
-    int blocks_per_sm[5] = {0, 0, 0, 0, 0};  // occupancy of the persistent point passes
+    int blocks_per_sm[5] = {0, 0, 0, 0, 0};        // occupancy of the persistent point passes
+    int blocks_per_sm_views[5] = {0, 0, 0, 0, 0};  // the same, batched-view kernels
     int chunk_points = 2048;           // points per chunk work record
     bool use_tiles = true;             // shared-memory screen tiles
     // Profiling: a ring of frames, each with a start/stop event per pass.
@@ -167,7 +171,26 @@ struct CullUniforms {
     int enableFrustumCulling, lodBias, enableCLOD;
 };
 
+// Arguments of the cull of one view of one cloud (inputs, scratch, outputs).
+struct CullArgs {
+    const cr_raster_batch *batches;
+    uint32_t nbatches;
+    const cr_raster_file *files;
+    uint32_t nfiles;
+    CullRec *tmp;           // nbatches records
+    uint32_t *cta_counts;   // 2 per 256-slot CTA
+    uint32_t chunk_points;
+    CullUniforms u;
+    cr_visible_batch *visible;  // nbatches
+    ChunkRec *chunks;           // chunk capacity of the cloud
+    uint32_t *counters;         // CNT_COUNT words
+};
+
 cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s);
+// Culls of several views in one pair of launches; d_args holds one CullArgs
+// per view (device memory).
+cr_status launch_cull_views(const CullArgs *d_args, uint32_t nslots, uint32_t nviews,
+                            cudaStream_t s);
 // Chunk records a cloud may need at the given chunk size.
 uint64_t chunk_capacity(const cr_capacity &cap, int chunk_points);
 
@@ -213,6 +236,40 @@ constexpr uint32_t kPackedMaxCount = 16843009u;
 cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
                         const RasterTargets &t, cudaStream_t s);
 
+// Mode, point-size mode and the unsupported colour effects of a configuration.
+cr_status validate_config(const cr_config *cfg);
+// Occupancy of the batched-view point passes (call before capturing them).
+void raster_prepare_views(cr_context *ctx);
+
+// Batched views: at most kMaxViews views per call.
+constexpr uint32_t kMaxViews = 256;
+
+// One view of a batched render (device memory): its frame's planes and
+// camera.  pix_begin is the exclusive prefix of width * height over the
+// views (the per-pixel kernels walk all views' pixels as one range).
+struct ViewDesc {
+    uint32_t *depth;
+    uint4 *accum;
+    unsigned long long *nearest;
+    uint32_t *rgba[2];  // resolve target and hole-fill ping-pong
+    float *depthf;
+    int width, height;
+    uint32_t pix_begin, pad;
+    float view[16], proj[16];
+};
+static_assert(sizeof(ViewDesc) == 192, "ViewDesc is 192 bytes");
+
+// The point pass `pass` (PASS_DEPTH / PASS_COLOR / PASS_NEAREST) of one cloud
+// over all views in one launch.  Chunk records of view v start at
+// chunks + v * chunk_stride and its counters at counters + v * CNT_COUNT;
+// its file table at files + v * nfiles.  u carries the configuration (the
+// per-view sizes and cameras come from views).
+cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
+                              const RasterTargets &t, const ViewDesc *views, uint32_t nviews,
+                              const cr_raster_file *files, uint32_t nfiles,
+                              const ChunkRec *chunks, uint32_t chunk_stride,
+                              uint32_t *counters, cudaStream_t s);
+
 struct ResolveUniforms {
     int width, height;
     float background[4];
@@ -224,13 +281,28 @@ cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t
                              const uint32_t *redo);
 // Zeroes the accumulators if *f->d_redo != 0.
 cr_status launch_accum_redo_clear(cr_frame *f, cudaStream_t s);
+
+// Batched views (all views' pixels as one range, total_pix in all):
+// zero every view's depth plane and accumulators, and *redo_flag.
+cr_status launch_clear_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
+                             uint32_t *redo_flag, int sm_count, cudaStream_t s);
+// Zero the accumulators if *redo_flag != 0.
+cr_status launch_accum_redo_clear_views(const ViewDesc *views, uint32_t nviews,
+                                        uint32_t total_pix, const uint32_t *redo_flag,
+                                        int sm_count, cudaStream_t s);
+// Resolve of every view (check / redo as launch_resolve_hqs).
+cr_status launch_resolve_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
+                               const ResolveUniforms &u, uint32_t *redo_flag, bool check,
+                               const uint32_t *redo, int sm_count, cudaStream_t s);
+// One hole-fill iteration of every view: rgba[src] -> rgba[1 - src].
+cr_status launch_hole_fill_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
+                                 int src, int sm_count, cudaStream_t s);
 cr_status launch_resolve_nearest(cr_frame *f, const uint32_t *colors, const ResolveUniforms &u,
                                  cudaStream_t s);
 cr_status launch_hole_fill(cr_frame *f, int iterations, cudaStream_t s);
 cr_status launch_split_nearest(const unsigned long long *keys, uint32_t *depth_out,
                                uint32_t *index_out, size_t n, cudaStream_t s);
 
-int raster_blocks_per_sm(int pass);
 
 cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, uint64_t count,
                    const cr_pack_params *prm, int on_device, uint32_t first_slot,

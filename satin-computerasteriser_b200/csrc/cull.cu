@@ -27,16 +27,6 @@ namespace {
 
 constexpr int kCullThreads = 256;
 
-struct CullArgs {
-    const cr_raster_batch *batches;
-    uint32_t nbatches;
-    const cr_raster_file *files;
-    uint32_t nfiles;
-    CullRec *tmp;
-    uint32_t *cta_counts;
-    uint32_t chunk_points;
-    CullUniforms u;
-};
 
 // Screen rectangle (buffer rows, widened by two pixels, clamped) covering the
 // projection of the batch AABB's eight corners; tw = 0 when a corner lies
@@ -126,7 +116,7 @@ __device__ __forceinline__ uint32_t nchunks(uint32_t active, uint32_t c) {
     return (active + c - 1u) / c;
 }
 
-__global__ void __launch_bounds__(kCullThreads) cull_classify(CullArgs a) {
+__device__ __forceinline__ void classify_body(const CullArgs &a) {
     __shared__ uint32_t warp_counts[kCullThreads / 32];
     __shared__ uint32_t warp_chunks[kCullThreads / 32];
     const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
@@ -159,9 +149,13 @@ __global__ void __launch_bounds__(kCullThreads) cull_classify(CullArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(kCullThreads)
-    cull_compact(const CullRec *tmp, const uint32_t *cta_counts, cr_visible_batch *out,
-                 ChunkRec *chunks, uint32_t chunk_points, uint32_t *counters) {
+__device__ __forceinline__ void compact_body(const CullArgs &a) {
+    const CullRec *tmp = a.tmp;
+    const uint32_t *cta_counts = a.cta_counts;
+    cr_visible_batch *out = a.visible;
+    ChunkRec *chunks = a.chunks;
+    const uint32_t chunk_points = a.chunk_points;
+    uint32_t *counters = a.counters;
     __shared__ uint32_t part_v[kCullThreads / 32], part_c[kCullThreads / 32];
     __shared__ uint32_t scan_w[kCullThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -240,6 +234,18 @@ __global__ void __launch_bounds__(kCullThreads)
     }
 }
 
+__global__ void __launch_bounds__(kCullThreads) cull_classify(CullArgs a) { classify_body(a); }
+__global__ void __launch_bounds__(kCullThreads) cull_compact(CullArgs a) { compact_body(a); }
+
+// Batched views: blockIdx.y selects the view's arguments (its uniforms, file
+// table and output ranges); the slots and the point pool are shared.
+__global__ void __launch_bounds__(kCullThreads) cull_classify_views(const CullArgs *av) {
+    classify_body(av[blockIdx.y]);
+}
+__global__ void __launch_bounds__(kCullThreads) cull_compact_views(const CullArgs *av) {
+    compact_body(av[blockIdx.y]);
+}
+
 __global__ void cull_empty(uint32_t *counters) {
     counters[CNT_VISIBLE] = 0u;
     counters[CNT_ARGS_X] = 0u;
@@ -266,13 +272,23 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s) {
     }
     const uint32_t cp = (uint32_t)std::max(cloud->ctx->chunk_points, kMinChunkPoints);
     const uint32_t ctas = (n + kCullThreads - 1) / kCullThreads;
-    CullArgs a{cloud->d_batches, n, cloud->d_files, (uint32_t)cloud->files.size(),
-               cloud->d_cull_tmp, cloud->d_cull_cta, cp, u};
+    CullArgs a{cloud->d_batches, n,  cloud->d_files,   (uint32_t)cloud->files.size(),
+               cloud->d_cull_tmp, cloud->d_cull_cta, cp, u, cloud->d_visible, cloud->d_chunks,
+               cloud->d_counters};
     cull_classify<<<ctas, kCullThreads, 0, s>>>(a);
     CR_CUDA(cudaGetLastError());
-    cull_compact<<<ctas, kCullThreads, 0, s>>>(cloud->d_cull_tmp, cloud->d_cull_cta,
-                                               cloud->d_visible, cloud->d_chunks, cp,
-                                               cloud->d_counters);
+    cull_compact<<<ctas, kCullThreads, 0, s>>>(a);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+cr_status launch_cull_views(const CullArgs *d_args, uint32_t nslots, uint32_t nviews,
+                            cudaStream_t s) {
+    if (nslots == 0 || nviews == 0) return CR_OK;
+    const dim3 grid((nslots + kCullThreads - 1) / kCullThreads, nviews);
+    cull_classify_views<<<grid, kCullThreads, 0, s>>>(d_args);
+    CR_CUDA(cudaGetLastError());
+    cull_compact_views<<<grid, kCullThreads, 0, s>>>(d_args);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

@@ -88,7 +88,49 @@ struct RasterArgs {
     float *frag_z;
     uint32_t *frag_col;
     uint32_t *frag_count;
+    // Batched views (MV kernels): per-view frames, culls and file tables.
+    const ViewDesc *views;
+    uint32_t nviews;
+    uint32_t nfiles;        // files per view; view v's table starts at files + v * nfiles
+    uint32_t chunk_stride;  // view v's chunk records start at chunks + v * chunk_stride
 };
+
+// The frame and camera of the view whose chunk a CTA is drawing (MV kernels).
+struct ViewState {
+    int width, height;
+    uint32_t *depth;
+    uint4 *accum;
+    unsigned long long *nearest;
+    float view[16], proj[16];
+};
+__shared__ ViewState s_view;
+
+// Frame and camera of the point being drawn: the kernel's own (one view) or
+// the current chunk's view (batched views).
+template <bool MV>
+__device__ __forceinline__ int view_w(const RasterArgs &a) { return MV ? s_view.width : a.u.width; }
+template <bool MV>
+__device__ __forceinline__ int view_h(const RasterArgs &a) { return MV ? s_view.height : a.u.height; }
+template <bool MV>
+__device__ __forceinline__ uint32_t *view_depth(const RasterArgs &a) {
+    return MV ? s_view.depth : a.t.depth;
+}
+template <bool MV>
+__device__ __forceinline__ uint4 *view_accum(const RasterArgs &a) {
+    return MV ? s_view.accum : a.t.accum;
+}
+template <bool MV>
+__device__ __forceinline__ unsigned long long *view_nearest(const RasterArgs &a) {
+    return MV ? s_view.nearest : a.t.nearest;
+}
+template <bool MV>
+__device__ __forceinline__ const float *view_view(const RasterArgs &a) {
+    return MV ? s_view.view : a.u.view;
+}
+template <bool MV>
+__device__ __forceinline__ const float *view_proj(const RasterArgs &a) {
+    return MV ? s_view.proj : a.u.proj;
+}
 
 struct BatchShared {
     float T[16];      // file.transform
@@ -116,7 +158,7 @@ __device__ __forceinline__ bool keep_point(const RasterArgs &a, const ChunkRec &
 
 // decodePoint + projection + clip + pixel (DepthPass/Shaders.metal:188-211,
 // ColorPass/Shaders.metal:70-104, NearestDepth/Shaders.metal:68-85).
-template <int PASS>
+template <int PASS, bool MV>
 __device__ __forceinline__ void project_point(const RasterArgs &a, const BatchShared &sb,
                                               const ChunkRec &c, uint32_t lo, uint32_t me,
                                               uint32_t hi, PointOut &o) {
@@ -140,7 +182,7 @@ __device__ __forceinline__ void project_point(const RasterArgs &a, const BatchSh
     const float nx = clip.x / clip.w, ny = clip.y / clip.w, nz = clip.z / clip.w;
     if (nx < -1.0f || ny < -1.0f || nx > 1.0f || ny > 1.0f || nz > 1.0f) ok = false;
     if (PASS == PASS_NEAREST ? (nz <= 0.0f) : (nz < 0.0f)) ok = false;
-    const int W = a.u.width, H = a.u.height;
+    const int W = view_w<MV>(a), H = view_h<MV>(a);
     o.ix = (int)((nx * 0.5f + 0.5f) * (float)W);
     const int iy = (int)((ny * 0.5f + 0.5f) * (float)H);
     if (o.ix < 0 || o.ix >= W || iy < 0 || iy >= H) ok = false;
@@ -166,14 +208,15 @@ __device__ __forceinline__ unsigned long long nearest_key(uint32_t depth, uint32
 // that needs more than kPackedMaxCount samples in the pixel, which the
 // resolve detects (the frame is then re-run unpacked).  Unpacked: one
 // 32-bit add per field.
+template <bool MV>
 __device__ __forceinline__ void color_global(const RasterArgs &a, uint32_t pix, uint32_t r,
                                              uint32_t g, uint32_t b, uint32_t n) {
     if (a.t.packed) {
-        unsigned long long *w = reinterpret_cast<unsigned long long *>(&a.t.accum[pix]);
+        unsigned long long *w = reinterpret_cast<unsigned long long *>(&view_accum<MV>(a)[pix]);
         atomicAdd(w, (unsigned long long)r | ((unsigned long long)g << 32));
         atomicAdd(w + 1, (unsigned long long)b | ((unsigned long long)n << 32));
     } else {
-        unsigned int *acc = reinterpret_cast<unsigned int *>(&a.t.accum[pix]);
+        unsigned int *acc = reinterpret_cast<unsigned int *>(&view_accum<MV>(a)[pix]);
         atomicAdd(acc + 0, r);
         atomicAdd(acc + 1, g);
         atomicAdd(acc + 2, b);
@@ -183,42 +226,42 @@ __device__ __forceinline__ void color_global(const RasterArgs &a, uint32_t pix, 
 
 // Direct path, radius 0: one global atomic per point (batches large on
 // screen, where points rarely share a pixel).
-template <int PASS>
+template <int PASS, bool MV>
 __device__ __forceinline__ void emit_direct(const RasterArgs &a, const PointOut &o) {
-    const uint32_t pix = (uint32_t)(o.iy * a.u.width + o.ix);
+    const uint32_t pix = (uint32_t)(o.iy * view_w<MV>(a) + o.ix);
     if (is_depth(PASS)) {
-        if (o.ok) atomicMax(&a.t.depth[pix], o.depth);
+        if (o.ok) atomicMax(&view_depth<MV>(a)[pix], o.depth);
     } else if (is_color(PASS)) {
-        const uint32_t closest = o.ok ? a.t.depth[pix] : 0u;
+        const uint32_t closest = o.ok ? view_depth<MV>(a)[pix] : 0u;
         const bool vis = closest != 0u && o.nz >= crd::uint_to_depth(closest) * a.keep_scale;
         if (vis)
-            color_global(a, pix, o.color & 0xffu, (o.color >> 8) & 0xffu, (o.color >> 16) & 0xffu,
+            color_global<MV>(a, pix, o.color & 0xffu, (o.color >> 8) & 0xffu, (o.color >> 16) & 0xffu,
                          1u);
     } else {
-        if (o.ok) atomicMax(&a.t.nearest[pix], nearest_key(o.depth, o.pointIndex));
+        if (o.ok) atomicMax(&view_nearest<MV>(a)[pix], nearest_key(o.depth, o.pointIndex));
     }
 }
 
 // Tile path, radius 0: shared-memory accumulation, global atomics for points
 // that round outside the rectangle.  Colour tiles hold R | count << 20, G and
 // B per pixel in 32-bit words (exact while a chunk has at most 4095 points).
-template <int PASS>
+template <int PASS, bool MV>
 __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ChunkRec &c,
                                           unsigned char *smem, const PointOut &o) {
     const int lx = o.ix - c.x0, ly = o.iy - c.y0;
     const bool inside = (unsigned)lx < (unsigned)c.tw && (unsigned)ly < (unsigned)c.th;
     const bool in_tile = o.ok && inside, outside = o.ok && !inside;
-    const uint32_t pix = (uint32_t)(o.iy * a.u.width + o.ix);
+    const uint32_t pix = (uint32_t)(o.iy * view_w<MV>(a) + o.ix);
     const int l = inside ? ly * c.tw + lx : 0;
     if (is_depth(PASS)) {
         if (in_tile) atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
-        if (outside) atomicMax(&a.t.depth[pix], o.depth);
+        if (outside) atomicMax(&view_depth<MV>(a)[pix], o.depth);
     } else if (is_color(PASS)) {
         constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
         uint32_t *acc = reinterpret_cast<uint32_t *>(smem);
         const uint32_t *sdep = acc + 3 * kPx;
         uint32_t closest = sdep[l];
-        if (outside) closest = a.t.depth[pix];
+        if (outside) closest = view_depth<MV>(a)[pix];
         const bool vis = o.ok && closest != 0u &&
                          o.nz >= crd::uint_to_depth(closest) * a.keep_scale;
         const uint32_t r = o.color & 0xffu, g = (o.color >> 8) & 0xffu,
@@ -228,24 +271,24 @@ __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ChunkRec &c
             atomicAdd(acc + kPx + l, g);
             atomicAdd(acc + 2 * kPx + l, b);
         }
-        if (vis && !inside) color_global(a, pix, r, g, b, 1u);
+        if (vis && !inside) color_global<MV>(a, pix, r, g, b, 1u);
     } else {
         const unsigned long long k = nearest_key(o.depth, o.pointIndex);
         if (in_tile) atomicMax(reinterpret_cast<unsigned long long *>(smem) + l, k);
-        if (outside) atomicMax(&a.t.nearest[pix], k);
+        if (outside) atomicMax(&view_nearest<MV>(a)[pix], k);
     }
 }
 
 // General footprint (radius from pointFootprintRadius), global atomics.
-template <int PASS>
+template <int PASS, bool MV>
 __device__ __forceinline__ void emit_footprint(const RasterArgs &a, const BatchShared &sb,
                                                const PointOut &o) {
     if (!o.ok) return;
     const crd::PointSize ps{a.u.pointSizeMode, a.u.minimumPointSize, a.u.maximumPointSize,
                             a.u.pointSizeScale};
     const int rad =
-        crd::footprint_radius(o.px, o.py, o.pz, sb.world, a.u.view, a.u.proj, a.u.height, ps);
-    const int W = a.u.width, H = a.u.height;
+        crd::footprint_radius(o.px, o.py, o.pz, sb.world, view_view<MV>(a), view_proj<MV>(a), view_h<MV>(a), ps);
+    const int W = view_w<MV>(a), H = view_h<MV>(a);
     for (int oy = -rad; oy <= rad; ++oy) {
         for (int ox = -rad; ox <= rad; ++ox) {
             if (!crd::inside_footprint(ox, oy, rad)) continue;
@@ -253,15 +296,15 @@ __device__ __forceinline__ void emit_footprint(const RasterArgs &a, const BatchS
             if (tx < 0 || tx >= W || ty < 0 || ty >= H) continue;
             const uint32_t pix = (uint32_t)(ty * W + tx);
             if (is_depth(PASS)) {
-                atomicMax(&a.t.depth[pix], o.depth);
+                atomicMax(&view_depth<MV>(a)[pix], o.depth);
             } else if (is_color(PASS)) {
-                const uint32_t closest = a.t.depth[pix];
+                const uint32_t closest = view_depth<MV>(a)[pix];
                 if (closest == 0u) continue;
                 if (!(o.nz >= crd::uint_to_depth(closest) * a.keep_scale)) continue;
-                color_global(a, pix, o.color & 0xffu, (o.color >> 8) & 0xffu,
+                color_global<MV>(a, pix, o.color & 0xffu, (o.color >> 8) & 0xffu,
                              (o.color >> 16) & 0xffu, 1u);
             } else {
-                atomicMax(&a.t.nearest[pix], nearest_key(o.depth, o.pointIndex));
+                atomicMax(&view_nearest<MV>(a)[pix], nearest_key(o.depth, o.pointIndex));
             }
         }
     }
@@ -288,7 +331,7 @@ __device__ __forceinline__ void emit_fragment(const RasterArgs &a, const ChunkRe
 }
 
 // One point; every lane of the warp calls this (warp-uniform early outs).
-template <int PASS>
+template <int PASS, bool MV>
 __device__ __forceinline__ void do_point(const RasterArgs &a, const BatchShared &sb,
                                          unsigned char *smem, const ChunkRec &c, bool tiled,
                                          bool valid, uint32_t local, uint32_t lvl, uint32_t lo,
@@ -298,14 +341,14 @@ __device__ __forceinline__ void do_point(const RasterArgs &a, const BatchShared 
     o.color = color;
     o.ok = valid && keep_point(a, c, o.pointIndex, lvl);
     if (!__any_sync(kFull, o.ok)) return;
-    project_point<PASS>(a, sb, c, lo, me, hi, o);
+    project_point<PASS, MV>(a, sb, c, lo, me, hi, o);
     if (!__any_sync(kFull, o.ok)) return;
     if (!a.radius_zero)
-        emit_footprint<PASS>(a, sb, o);
+        emit_footprint<PASS, MV>(a, sb, o);
     else if (tiled)
-        emit_tile<PASS>(a, c, smem, o);
+        emit_tile<PASS, MV>(a, c, smem, o);
     else
-        emit_direct<PASS>(a, o);
+        emit_direct<PASS, MV>(a, o);
     if (PASS == PASS_DEPTH_FRAG) emit_fragment(a, c, o);
 }
 
@@ -320,9 +363,9 @@ __device__ __forceinline__ void do_fragment(const RasterArgs &a, unsigned char *
     o.nz = nz;
     o.color = color;
     if (tiled)
-        emit_tile<PASS_COLOR_FRAG>(a, c, smem, o);
+        emit_tile<PASS_COLOR_FRAG, false>(a, c, smem, o);
     else
-        emit_direct<PASS_COLOR_FRAG>(a, o);
+        emit_direct<PASS_COLOR_FRAG, false>(a, o);
 }
 
 // Four fragments of one thread in the colour pass, the first `nvalid` of
@@ -344,7 +387,7 @@ __device__ __forceinline__ void color_quad(const RasterArgs &a, unsigned char *s
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int ix = (int)(xy[i] & 0xffffu), iy = (int)(xy[i] >> 16);
-        pix[i] = (uint32_t)(iy * a.u.width + ix);
+        pix[i] = (uint32_t)(iy * view_w<false>(a) + ix);
         const int lx = ix - c.x0, ly = iy - c.y0;
         in[i] = tiled && (unsigned)lx < (unsigned)c.tw && (unsigned)ly < (unsigned)c.th;
         l[i] = in[i] ? ly * c.tw + lx : 0;
@@ -352,7 +395,7 @@ __device__ __forceinline__ void color_quad(const RasterArgs &a, unsigned char *s
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         closest[i] = 0u;
-        if ((uint32_t)i < nvalid) closest[i] = in[i] ? sdep[l[i]] : __ldg(a.t.depth + pix[i]);
+        if ((uint32_t)i < nvalid) closest[i] = in[i] ? sdep[l[i]] : __ldg(view_depth<false>(a) + pix[i]);
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -363,11 +406,11 @@ __device__ __forceinline__ void color_quad(const RasterArgs &a, unsigned char *s
             atomicAdd(acc + kPx + l[i], g);
             atomicAdd(acc + 2 * kPx + l[i], b);
         }
-        if (vis && !in[i]) color_global(a, pix[i], r, g, b, 1u);
+        if (vis && !in[i]) color_global<false>(a, pix[i], r, g, b, 1u);
     }
 }
 
-template <int PASS>
+template <int PASS, bool MV>
 __device__ __forceinline__ void tile_init(const RasterArgs &a, const ChunkRec &c,
                                           unsigned char *smem) {
     const int n = c.tw * c.th;
@@ -381,31 +424,31 @@ __device__ __forceinline__ void tile_init(const RasterArgs &a, const ChunkRec &c
             acc[kPx + l] = 0u;
             acc[2 * kPx + l] = 0u;
             const int gx = c.x0 + l % c.tw, gy = c.y0 + l / c.tw;
-            acc[3 * kPx + l] = a.t.depth[gy * a.u.width + gx];
+            acc[3 * kPx + l] = view_depth<MV>(a)[gy * view_w<MV>(a) + gx];
         } else {
             reinterpret_cast<unsigned long long *>(smem)[l] = 0ull;
         }
     }
 }
 
-template <int PASS>
+template <int PASS, bool MV>
 __device__ __forceinline__ void tile_flush(const RasterArgs &a, const ChunkRec &c,
                                            const unsigned char *smem) {
     const int n = c.tw * c.th;
     for (int l = threadIdx.x; l < n; l += kThreads) {
-        const uint32_t pix = (uint32_t)((c.y0 + l / c.tw) * a.u.width + c.x0 + l % c.tw);
+        const uint32_t pix = (uint32_t)((c.y0 + l / c.tw) * view_w<MV>(a) + c.x0 + l % c.tw);
         if (is_depth(PASS)) {
             const uint32_t v = reinterpret_cast<const uint32_t *>(smem)[l];
-            if (v) atomicMax(&a.t.depth[pix], v);
+            if (v) atomicMax(&view_depth<MV>(a)[pix], v);
         } else if (is_color(PASS)) {
             constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
             const uint32_t *acc = reinterpret_cast<const uint32_t *>(smem);
             const uint32_t rc = acc[l];
             const uint32_t cnt = rc >> 20;
-            if (cnt) color_global(a, pix, rc & 0xfffffu, acc[kPx + l], acc[2 * kPx + l], cnt);
+            if (cnt) color_global<MV>(a, pix, rc & 0xfffffu, acc[kPx + l], acc[2 * kPx + l], cnt);
         } else {
             const unsigned long long k = reinterpret_cast<const unsigned long long *>(smem)[l];
-            if (k) atomicMax(&a.t.nearest[pix], k);
+            if (k) atomicMax(&view_nearest<MV>(a)[pix], k);
         }
     }
 }
@@ -428,21 +471,71 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// Largest view v with begin[v] <= k (views without chunks share their
+// begin with the next view, so the view found holds chunk k).
+__device__ __forceinline__ uint32_t find_view(const uint32_t *begin, uint32_t nviews, uint32_t k) {
+    uint32_t lo = 0, hi = nviews;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (begin[mid] <= k)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
 // Persistent pass over the chunk records (static grid-stride schedule): the
 // record of the CTA's next chunk is copied into shared memory with cp.async
-// while the current chunk is processed.
-template <int PASS>
+// while the current chunk is processed.  Batched views (MV): the chunks of
+// all views form one index space, view after view; each CTA scans the
+// per-view chunk counts once, finds a chunk's view by binary search and
+// switches frame, camera and file table when the view changes.
+template <int PASS, bool MV>
 __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ BatchShared sb;
     __shared__ __align__(16) ChunkRec rec[2];
     __shared__ __align__(16) uint32_t rec_frags[2][4];
+    __shared__ uint32_t s_vbegin[MV ? kMaxViews + 1 : 1];
+    __shared__ uint32_t s_wsum[kThreads / 32];
     if (a.t.redo && *a.t.redo == 0u) return;
-    const uint32_t nchunks = a.counters[CNT_CHUNKS];
+    uint32_t nchunks;
+    if (MV) {
+        // Exclusive prefix of the views' chunk counts (at most kMaxViews views).
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        uint32_t x = threadIdx.x < a.nviews ? a.counters[threadIdx.x * CNT_COUNT + CNT_CHUNKS] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_wsum[warp] = x;
+        __syncthreads();
+        for (int w = 0; w < warp; ++w) x += s_wsum[w];
+        s_vbegin[threadIdx.x + 1] = x;
+        if (threadIdx.x == 0) s_vbegin[0] = 0u;
+        __syncthreads();
+        nchunks = s_vbegin[a.nviews];
+    } else {
+        nchunks = a.counters[CNT_CHUNKS];
+    }
     uint32_t k = blockIdx.x;
     if (k >= nchunks) return;
-    if (threadIdx.x < 4) cp_async16(reinterpret_cast<uint4 *>(&rec[0]) + threadIdx.x,
-                                    reinterpret_cast<const uint4 *>(a.chunks + k) + threadIdx.x);
+    // View of chunk kk and the address of its record.
+    auto locate = [&](uint32_t kk, uint32_t &view) -> const ChunkRec * {
+        if (!MV) {
+            view = 0u;
+            return a.chunks + kk;
+        }
+        view = find_view(s_vbegin, a.nviews, kk);
+        return a.chunks + (size_t)view * a.chunk_stride + (kk - s_vbegin[view]);
+    };
+    uint32_t cur_view, next_view = 0u, loaded_view = 0xffffffffu;
+    const ChunkRec *src = locate(k, cur_view);
+    if (threadIdx.x < 4)
+        cp_async16(reinterpret_cast<uint4 *>(&rec[0]) + threadIdx.x,
+                   reinterpret_cast<const uint4 *>(src) + threadIdx.x);
     if (PASS == PASS_COLOR_FRAG && threadIdx.x == 4) cp_async4(&rec_frags[0][0], a.frag_count + k);
     cp_async_commit();
     if (threadIdx.x == 0) {
@@ -450,34 +543,54 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
         s_frag_count = 0u;
     }
     int buf = 0;
-    for (; k < nchunks; k += gridDim.x, buf ^= 1) {
+    for (; k < nchunks; k += gridDim.x, buf ^= 1, cur_view = next_view) {
         cp_async_wait_all();
         __syncthreads();  // rec[buf] complete; the previous chunk is fully done
         const ChunkRec c = rec[buf];
         const uint32_t nfrag = PASS == PASS_COLOR_FRAG ? rec_frags[buf][0] : 0u;
         const uint32_t kn = k + gridDim.x;
-        if (kn < nchunks && threadIdx.x < 4)
-            cp_async16(reinterpret_cast<uint4 *>(&rec[buf ^ 1]) + threadIdx.x,
-                       reinterpret_cast<const uint4 *>(a.chunks + kn) + threadIdx.x);
-        if (PASS == PASS_COLOR_FRAG && kn < nchunks && threadIdx.x == 4)
-            cp_async4(&rec_frags[buf ^ 1][0], a.frag_count + kn);
+        if (kn < nchunks) {
+            const ChunkRec *nsrc = locate(kn, next_view);
+            if (threadIdx.x < 4)
+                cp_async16(reinterpret_cast<uint4 *>(&rec[buf ^ 1]) + threadIdx.x,
+                           reinterpret_cast<const uint4 *>(nsrc) + threadIdx.x);
+            if (PASS == PASS_COLOR_FRAG && threadIdx.x == 4)
+                cp_async4(&rec_frags[buf ^ 1][0], a.frag_count + kn);
+        }
         cp_async_commit();
-        const bool new_file = c.file != sb.file;
+        const uint32_t file_id = MV ? cur_view * a.nfiles + c.file : c.file;
+        const bool new_file = file_id != sb.file;
         const uint32_t work = PASS == PASS_COLOR_FRAG ? nfrag : c.count;
         const bool tiled = a.use_tiles && a.radius_zero && c.tw > 0 &&
                            c.tw * c.th <= TileCfg<PASS>::kPx && c.tw * c.th <= (int)(2 * work) &&
                            (!is_color(PASS) || c.count < 4096u);
         if (new_file || tiled) {
-            __syncthreads();  // everyone has read sb.file
+            __syncthreads();  // everyone has read sb.file (and the view state)
             if (new_file) {
-                const cr_raster_file *file = &a.files[c.file];
+                const cr_raster_file *file = &a.files[file_id];
                 if (threadIdx.x < 16)
                     sb.T[threadIdx.x] = file->transform[threadIdx.x];
                 else if (threadIdx.x < 32)
                     sb.world[threadIdx.x - 16] = file->world[threadIdx.x - 16];
-                if (threadIdx.x == 0) sb.file = c.file;
+                if (threadIdx.x == 0) sb.file = file_id;
             }
-            if (tiled) tile_init<PASS>(a, c, smem);
+            if (MV && cur_view != loaded_view) {  // a new view always brings a new file id
+                const ViewDesc &vd = a.views[cur_view];
+                if (threadIdx.x >= 32 && threadIdx.x < 48)
+                    s_view.view[threadIdx.x - 32] = vd.view[threadIdx.x - 32];
+                else if (threadIdx.x >= 48 && threadIdx.x < 64)
+                    s_view.proj[threadIdx.x - 48] = vd.proj[threadIdx.x - 48];
+                else if (threadIdx.x == 64) {
+                    s_view.width = vd.width;
+                    s_view.height = vd.height;
+                    s_view.depth = vd.depth;
+                    s_view.accum = vd.accum;
+                    s_view.nearest = vd.nearest;
+                }
+                loaded_view = cur_view;
+                if (tiled) __syncthreads();  // the tile's set-up reads the view state
+            }
+            if (tiled) tile_init<PASS, MV>(a, c, smem);
             __syncthreads();
         }
         const bool need_med = c.level <= 1, need_high = c.level == 0;
@@ -526,13 +639,13 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
                         co4 = __ldg(reinterpret_cast<const uint4 *>(a.colors + base));
                 }
                 const uint32_t l0 = 4u * q;
-                do_point<PASS>(a, sb, smem, c, tiled, qv && l0 + 0 < c.count, l0 + 0,
+                do_point<PASS, MV>(a, sb, smem, c, tiled, qv && l0 + 0 < c.count, l0 + 0,
                                lv4 & 0xffu, lo4.x, me4.x, hi4.x, co4.x);
-                do_point<PASS>(a, sb, smem, c, tiled, qv && l0 + 1 < c.count, l0 + 1,
+                do_point<PASS, MV>(a, sb, smem, c, tiled, qv && l0 + 1 < c.count, l0 + 1,
                                (lv4 >> 8) & 0xffu, lo4.y, me4.y, hi4.y, co4.y);
-                do_point<PASS>(a, sb, smem, c, tiled, qv && l0 + 2 < c.count, l0 + 2,
+                do_point<PASS, MV>(a, sb, smem, c, tiled, qv && l0 + 2 < c.count, l0 + 2,
                                (lv4 >> 16) & 0xffu, lo4.z, me4.z, hi4.z, co4.z);
-                do_point<PASS>(a, sb, smem, c, tiled, qv && l0 + 3 < c.count, l0 + 3,
+                do_point<PASS, MV>(a, sb, smem, c, tiled, qv && l0 + 3 < c.count, l0 + 3,
                                lv4 >> 24, lo4.w, me4.w, hi4.w, co4.w);
             }
         } else {
@@ -546,12 +659,12 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
                 const uint32_t me = (v && need_med) ? a.med[i] : 0u;
                 const uint32_t hi = (v && need_high) ? a.high[i] : 0u;
                 const uint32_t co = (v && kNeedColor) ? a.colors[i] : 0u;
-                do_point<PASS>(a, sb, smem, c, tiled, v, local, lv, lo, me, hi, co);
+                do_point<PASS, MV>(a, sb, smem, c, tiled, v, local, lv, lo, me, hi, co);
             }
         }
         if (tiled || PASS == PASS_DEPTH_FRAG) {
             __syncthreads();
-            if (tiled) tile_flush<PASS>(a, c, smem);
+            if (tiled) tile_flush<PASS, MV>(a, c, smem);
             if (PASS == PASS_DEPTH_FRAG && threadIdx.x == 0) {
                 a.frag_count[k] = s_frag_count;
                 s_frag_count = 0u;
@@ -561,31 +674,29 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
     cp_async_wait_all();
 }
 
-template <int PASS>
+template <int PASS, bool MV>
 int blocks_per_sm_for() {
     int n = 0;
-    cudaFuncSetAttribute(raster_kernel<PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(raster_kernel<PASS, MV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          TileCfg<PASS>::kBytes);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, raster_kernel<PASS>, kThreads,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, raster_kernel<PASS, MV>, kThreads,
                                                       TileCfg<PASS>::kBytes) != cudaSuccess)
         n = 1;
     return n < 1 ? 1 : n;
 }
 
-}  // namespace
-
+template <bool MV>
 int raster_blocks_per_sm(int pass) {
     switch (pass) {
-    case PASS_DEPTH: return blocks_per_sm_for<PASS_DEPTH>();
-    case PASS_COLOR: return blocks_per_sm_for<PASS_COLOR>();
-    case PASS_DEPTH_FRAG: return blocks_per_sm_for<PASS_DEPTH_FRAG>();
-    case PASS_COLOR_FRAG: return blocks_per_sm_for<PASS_COLOR_FRAG>();
-    default: return blocks_per_sm_for<PASS_NEAREST>();
+    case PASS_DEPTH: return blocks_per_sm_for<PASS_DEPTH, MV>();
+    case PASS_COLOR: return blocks_per_sm_for<PASS_COLOR, MV>();
+    case PASS_DEPTH_FRAG: return blocks_per_sm_for<PASS_DEPTH_FRAG, false>();
+    case PASS_COLOR_FRAG: return blocks_per_sm_for<PASS_COLOR_FRAG, false>();
+    default: return blocks_per_sm_for<PASS_NEAREST, MV>();
     }
 }
 
-cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
-                        const RasterTargets &t, cudaStream_t s) {
+RasterArgs make_args(cr_cloud *cloud, const RasterUniforms &u, const RasterTargets &t) {
     RasterArgs a;
     a.chunks = cloud->d_chunks;
     a.files = cloud->d_files;
@@ -606,25 +717,65 @@ cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &
     a.frag_z = cloud->d_frag_z;
     a.frag_col = cloud->d_frag_col;
     a.frag_count = cloud->d_frag_count;
+    a.views = nullptr;
+    a.nviews = 0;
+    a.nfiles = 0;
+    a.chunk_stride = 0;
+    return a;
+}
+
+template <int PASS, bool MV>
+void launch_pass(const RasterArgs &a, int grid, cudaStream_t s) {
+    raster_kernel<PASS, MV><<<grid, kThreads, TileCfg<PASS>::kBytes, s>>>(a);
+}
+
+}  // namespace
+
+cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
+                        const RasterTargets &t, cudaStream_t s) {
+    const RasterArgs a = make_args(cloud, u, t);
     cr_context *ctx = cloud->ctx;
-    if (ctx->blocks_per_sm[pass] == 0) ctx->blocks_per_sm[pass] = raster_blocks_per_sm(pass);
+    if (ctx->blocks_per_sm[pass] == 0) ctx->blocks_per_sm[pass] = raster_blocks_per_sm<false>(pass);
     const int grid = ctx->sm_count * ctx->blocks_per_sm[pass];
     switch (pass) {
-    case PASS_DEPTH:
-        raster_kernel<PASS_DEPTH><<<grid, kThreads, TileCfg<PASS_DEPTH>::kBytes, s>>>(a);
-        break;
-    case PASS_COLOR:
-        raster_kernel<PASS_COLOR><<<grid, kThreads, TileCfg<PASS_COLOR>::kBytes, s>>>(a);
-        break;
-    case PASS_DEPTH_FRAG:
-        raster_kernel<PASS_DEPTH_FRAG><<<grid, kThreads, TileCfg<PASS_DEPTH>::kBytes, s>>>(a);
-        break;
-    case PASS_COLOR_FRAG:
-        raster_kernel<PASS_COLOR_FRAG><<<grid, kThreads, TileCfg<PASS_COLOR>::kBytes, s>>>(a);
-        break;
-    default:
-        raster_kernel<PASS_NEAREST><<<grid, kThreads, TileCfg<PASS_NEAREST>::kBytes, s>>>(a);
-        break;
+    case PASS_DEPTH: launch_pass<PASS_DEPTH, false>(a, grid, s); break;
+    case PASS_COLOR: launch_pass<PASS_COLOR, false>(a, grid, s); break;
+    case PASS_DEPTH_FRAG: launch_pass<PASS_DEPTH_FRAG, false>(a, grid, s); break;
+    case PASS_COLOR_FRAG: launch_pass<PASS_COLOR_FRAG, false>(a, grid, s); break;
+    default: launch_pass<PASS_NEAREST, false>(a, grid, s); break;
+    }
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+void raster_prepare_views(cr_context *ctx) {
+    for (int p : {PASS_DEPTH, PASS_COLOR, PASS_NEAREST})
+        if (ctx->blocks_per_sm_views[p] == 0) ctx->blocks_per_sm_views[p] = raster_blocks_per_sm<true>(p);
+}
+
+cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
+                              const RasterTargets &t, const ViewDesc *views, uint32_t nviews,
+                              const cr_raster_file *files, uint32_t nfiles,
+                              const ChunkRec *chunks, uint32_t chunk_stride,
+                              uint32_t *counters, cudaStream_t s) {
+    if (pass == PASS_DEPTH_FRAG || pass == PASS_COLOR_FRAG || nviews == 0 || nviews > kMaxViews)
+        return cri::fail(CR_ERR_INTERNAL, "batched views: unsupported pass or view count");
+    RasterArgs a = make_args(cloud, u, t);
+    a.chunks = chunks;
+    a.files = files;
+    a.counters = counters;
+    a.views = views;
+    a.nviews = nviews;
+    a.nfiles = nfiles;
+    a.chunk_stride = chunk_stride;
+    cr_context *ctx = cloud->ctx;
+    if (ctx->blocks_per_sm_views[pass] == 0)
+        ctx->blocks_per_sm_views[pass] = raster_blocks_per_sm<true>(pass);
+    const int grid = ctx->sm_count * ctx->blocks_per_sm_views[pass];
+    switch (pass) {
+    case PASS_DEPTH: launch_pass<PASS_DEPTH, true>(a, grid, s); break;
+    case PASS_COLOR: launch_pass<PASS_COLOR, true>(a, grid, s); break;
+    default: launch_pass<PASS_NEAREST, true>(a, grid, s); break;
     }
     CR_CUDA(cudaGetLastError());
     return CR_OK;

@@ -8,6 +8,8 @@
 // The reference writes an rgba8Unorm texture and an R32Float depth texture;
 // here both are linear device buffers (row 0 = top row, as the passes flip
 // y), one uint32 per pixel holding R | G<<8 | B<<16 | A<<24.
+#include <algorithm>
+
 #include "cr_device.cuh"
 #include "cr_internal.h"
 
@@ -17,6 +19,21 @@ constexpr int kThreads = 256;
 
 __device__ __forceinline__ uint32_t pack_rgba(float r, float g, float b, float a) {
     return crd::unorm8(r) | (crd::unorm8(g) << 8) | (crd::unorm8(b) << 16) | (crd::unorm8(a) << 24);
+}
+
+// resolveUpdate of one pixel (count path).
+__device__ __forceinline__ void resolve_pixel(const uint4 acc, uint32_t depth,
+                                              const ResolveUniforms &u, uint32_t &rgba,
+                                              float &depthf) {
+    if (acc.w == 0u) {
+        rgba = pack_rgba(u.background[0], u.background[1], u.background[2], 0.0f);
+        depthf = 0.0f;
+        return;
+    }
+    const float inv = 1.0f / (float)acc.w;
+    rgba = pack_rgba(((float)acc.x * inv) / 255.0f, ((float)acc.y * inv) / 255.0f,
+                     ((float)acc.z * inv) / 255.0f, 1.0f);
+    depthf = crd::uint_to_depth(depth);
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -30,15 +47,8 @@ __global__ void __launch_bounds__(kThreads)
         // kPackedMaxCount: past it a channel sum may have carried into its
         // neighbour field, and the frame's colour pass is re-run exactly.
         if (check && acc.w > kPackedMaxCount) *redo_flag = 1u;
-        if (acc.w == 0u) {
-            rgba[p] = pack_rgba(u.background[0], u.background[1], u.background[2], 0.0f);
-            depthf[p] = 0.0f;
-            continue;
-        }
-        const float inv = 1.0f / (float)acc.w;
-        rgba[p] = pack_rgba(((float)acc.x * inv) / 255.0f, ((float)acc.y * inv) / 255.0f,
-                            ((float)acc.z * inv) / 255.0f, 1.0f);
-        depthf[p] = crd::uint_to_depth(depth[p]);
+        // The depth plane is read only where the pixel was covered.
+        resolve_pixel(acc, acc.w ? depth[p] : 0u, u, rgba[p], depthf[p]);
     }
 }
 
@@ -66,16 +76,11 @@ __device__ __forceinline__ float unorm_ch(uint32_t v, int ch) {
     return (float)((v >> (8 * ch)) & 0xffu) / 255.0f;
 }
 
-__global__ void __launch_bounds__(kThreads)
-    hole_fill(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, int w, int h) {
-    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int y = blockIdx.y * (kThreads / 32) + (threadIdx.x >> 5);
-    if (x >= w || y >= h) return;
+// holeFillUpdate of pixel (x, y) of a w x h image.
+__device__ __forceinline__ uint32_t hole_fill_pixel(const uint32_t *__restrict__ src, int x, int y,
+                                                    int w, int h) {
     const uint32_t center = src[(size_t)y * w + x];
-    if (unorm_ch(center, 3) >= 0.5f) {
-        dst[(size_t)y * w + x] = center;
-        return;
-    }
+    if (unorm_ch(center, 3) >= 0.5f) return center;
     float sr = 0.0f, sg = 0.0f, sb = 0.0f, cnt = 0.0f;
 #pragma unroll
     for (int oy = -1; oy <= 1; ++oy) {
@@ -93,7 +98,92 @@ __global__ void __launch_bounds__(kThreads)
             }
         }
     }
-    dst[(size_t)y * w + x] = cnt > 0.0f ? pack_rgba(sr / cnt, sg / cnt, sb / cnt, 1.0f) : center;
+    return cnt > 0.0f ? pack_rgba(sr / cnt, sg / cnt, sb / cnt, 1.0f) : center;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    hole_fill(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, int w, int h) {
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int y = blockIdx.y * (kThreads / 32) + (threadIdx.x >> 5);
+    if (x >= w || y >= h) return;
+    dst[(size_t)y * w + x] = hole_fill_pixel(src, x, y, w, h);
+}
+
+// ---------------------------------------------------------------------------
+// Batched views: every view's pixels form one range [0, total_pix), view
+// after view (ViewDesc::pix_begin); a thread finds its pixel's view by
+// binary search over the views' begins, staged in shared memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void stage_begins(const ViewDesc *views, uint32_t nviews,
+                                             uint32_t total_pix, uint32_t *begin) {
+    for (uint32_t v = threadIdx.x; v <= nviews; v += kThreads)
+        begin[v] = v < nviews ? views[v].pix_begin : total_pix;
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t view_of_pixel(const uint32_t *begin, uint32_t nviews,
+                                                  uint32_t p) {
+    uint32_t lo = 0, hi = nviews;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (begin[mid] <= p)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Zeroes every view's accumulators and (not only_if_flag) depth plane and
+// the redo flag; only_if_flag: the accumulators alone, and only if the flag
+// is set.
+__global__ void __launch_bounds__(kThreads)
+    clear_views(const ViewDesc *__restrict__ views, uint32_t nviews, uint32_t total_pix,
+                uint32_t *redo_flag, int only_if_flag) {
+    __shared__ uint32_t begin[kMaxViews + 1];
+    if (only_if_flag && *redo_flag == 0u) return;
+    stage_begins(views, nviews, total_pix, begin);
+    if (!only_if_flag && blockIdx.x == 0 && threadIdx.x == 0) *redo_flag = 0u;
+    for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < total_pix;
+         p += gridDim.x * kThreads) {
+        const uint32_t v = view_of_pixel(begin, nviews, p);
+        const uint32_t q = p - begin[v];
+        const ViewDesc &vd = views[v];
+        vd.accum[q] = make_uint4(0u, 0u, 0u, 0u);
+        if (!only_if_flag) vd.depth[q] = 0u;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    resolve_views(const ViewDesc *__restrict__ views, uint32_t nviews, uint32_t total_pix,
+                  ResolveUniforms u, uint32_t *redo_flag, int check, const uint32_t *redo) {
+    __shared__ uint32_t begin[kMaxViews + 1];
+    if (redo && *redo == 0u) return;
+    stage_begins(views, nviews, total_pix, begin);
+    for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < total_pix;
+         p += gridDim.x * kThreads) {
+        const uint32_t v = view_of_pixel(begin, nviews, p);
+        const uint32_t q = p - begin[v];
+        const ViewDesc &vd = views[v];
+        const uint4 acc = vd.accum[q];
+        if (check && acc.w > kPackedMaxCount) *redo_flag = 1u;
+        resolve_pixel(acc, acc.w ? vd.depth[q] : 0u, u, vd.rgba[0][q], vd.depthf[q]);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    hole_fill_views(const ViewDesc *__restrict__ views, uint32_t nviews, uint32_t total_pix,
+                    int src) {
+    __shared__ uint32_t begin[kMaxViews + 1];
+    stage_begins(views, nviews, total_pix, begin);
+    for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < total_pix;
+         p += gridDim.x * kThreads) {
+        const uint32_t v = view_of_pixel(begin, nviews, p);
+        const uint32_t q = p - begin[v];
+        const ViewDesc &vd = views[v];
+        const int x = (int)(q % (uint32_t)vd.width), y = (int)(q / (uint32_t)vd.width);
+        vd.rgba[1 - src][q] = hole_fill_pixel(vd.rgba[src], x, y, vd.width, vd.height);
+    }
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -164,6 +254,47 @@ cr_status launch_split_nearest(const unsigned long long *keys, uint32_t *depth_o
     if (n == 0) return CR_OK;
     split_nearest<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(keys, depth_out,
                                                                                index_out, n);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+static uint32_t views_grid(uint32_t total_pix, int sm_count) {
+    const uint32_t need = (total_pix + kThreads - 1) / kThreads;
+    const uint32_t cap = (uint32_t)sm_count * 8u;
+    return std::max<uint32_t>(1u, std::min(need, cap));
+}
+
+cr_status launch_clear_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
+                             uint32_t *redo_flag, int sm_count, cudaStream_t s) {
+    clear_views<<<views_grid(total_pix, sm_count), kThreads, 0, s>>>(views, nviews, total_pix,
+                                                                     redo_flag, 0);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+cr_status launch_accum_redo_clear_views(const ViewDesc *views, uint32_t nviews,
+                                        uint32_t total_pix, const uint32_t *redo_flag,
+                                        int sm_count, cudaStream_t s) {
+    clear_views<<<sm_count * 4, kThreads, 0, s>>>(views, nviews, total_pix,
+                                                  const_cast<uint32_t *>(redo_flag), 1);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+cr_status launch_resolve_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
+                               const ResolveUniforms &u, uint32_t *redo_flag, bool check,
+                               const uint32_t *redo, int sm_count, cudaStream_t s) {
+    const uint32_t grid = redo ? (uint32_t)sm_count * 4 : views_grid(total_pix, sm_count);
+    resolve_views<<<grid, kThreads, 0, s>>>(views, nviews, total_pix, u, redo_flag, check ? 1 : 0,
+                                           redo);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+cr_status launch_hole_fill_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
+                                 int src, int sm_count, cudaStream_t s) {
+    hole_fill_views<<<views_grid(total_pix, sm_count), kThreads, 0, s>>>(views, nviews, total_pix,
+                                                                         src);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

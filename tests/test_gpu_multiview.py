@@ -1,0 +1,163 @@
+"""Batched views (cr_render_multiview): every view bit-identical to a
+per-view ComputeRasteriser update + encode of the same camera and size.
+
+The per-view path with single-pixel footprints runs the fragment passes
+(depth pass emits fragments, colour pass reads them); the batched path
+decodes and projects the points again in its colour pass.  The two must
+agree bit for bit on every plane: depth, R, G, B, count, RGBA8, depth f32.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from scenes import blob_cloud, lattice_cloud, to_product_packed
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(cr):
+    return cr.Context(0)
+
+
+def make_cloud(cr, orc, ctx, pos, rgba, ppb=1024):
+    packed = orc.pack(pos, colors_rgba8=rgba, pointsPerBatch=ppb)
+    return cr.ComputeRasteriserPointCloud(ctx, packed=to_product_packed(cr, packed))
+
+
+def cameras(cr, sizes, seed, radius=2.5):
+    rng = np.random.default_rng(seed)
+    cams = []
+    for w, h in sizes:
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        cam = cr.PerspectiveCamera(position=tuple(d * rng.uniform(0.8, 1.2) * radius),
+                                   near=0.01, far=100.0, fov=float(rng.uniform(40, 75)),
+                                   aspect=w / h)
+        cam.lookAt(tuple(rng.uniform(-0.2, 0.2, 3)))
+        cams.append(cam)
+    return cams
+
+
+def per_view(cr, ctx, clouds, cfg, cam, size):
+    ras = cr.ComputeRasteriser(ctx)
+    ras.configuration = cfg
+    for c in clouds:
+        ras.addPointCloud(c)
+    ras.resize(size)
+    ras.update(cam)
+    ras.encode()
+    return ras.outputRGBA8(), ras.depthTexture(), ras.pixels()
+
+
+def assert_views_match(cr, ctx, mv, clouds, cfg, cams, sizes):
+    for i, (cam, size) in enumerate(zip(cams, sizes)):
+        rgba, depthf, px = per_view(cr, ctx, clouds, cfg, cam, size)
+        assert np.array_equal(mv.outputRGBA8(i), rgba), f"view {i} rgba"
+        assert np.array_equal(mv.depthTexture(i).view(np.uint32), depthf.view(np.uint32)), i
+        got = mv.pixels(i)
+        for f in ("depth", "red", "green", "blue", "count"):
+            assert np.array_equal(got[f], px[f]), f"view {i} {f}"
+        assert px["count"].any(), f"view {i} drew nothing"
+
+
+SIZES = [(64, 64), (128, 96), (320, 180), (96, 160), (200, 150), (32, 32), (256, 256)]
+
+
+def test_batched_views_match_per_view_renders(cr, orc, ctx):
+    pos, rgba = lattice_cloud(40, 11)
+    cloud = make_cloud(cr, orc, ctx, pos, rgba)
+    mv = cr.MultiViewRasteriser(ctx, SIZES)
+    mv.addPointCloud(cloud)
+    cams = cameras(cr, SIZES, 5)
+    mv.render(cams)
+    assert_views_match(cr, ctx, mv, [cloud], mv.configuration, cams, SIZES)
+
+
+def test_graph_replay_with_new_cameras(cr, orc, ctx):
+    """Three calls with different cameras reuse the captured graph (alternating
+    staging blocks); each call's images match its own per-view renders."""
+    pos, rgba = blob_cloud(60000, 4)
+    cloud = make_cloud(cr, orc, ctx, pos, rgba)
+    mv = cr.MultiViewRasteriser(ctx, SIZES[:4])
+    mv.addPointCloud(cloud)
+    for seed in (1, 2, 3):
+        cams = cameras(cr, SIZES[:4], seed)
+        mv.render(cams)
+        assert_views_match(cr, ctx, mv, [cloud], mv.configuration, cams, SIZES[:4])
+
+
+def test_batched_views_two_clouds_models_and_options(cr, orc, ctx):
+    pos, rgba = blob_cloud(30000, 7)
+    a = make_cloud(cr, orc, ctx, pos, rgba)
+    pos2, rgba2 = lattice_cloud(24, 8, lo=-0.6, hi=0.6)
+    b = make_cloud(cr, orc, ctx, pos2, rgba2, ppb=512)
+    b.position = (0.3, -0.2, 0.1)
+    cfg = cr.ComputeRasteriserConfiguration(depthTolerance=0.05, holeFillIterations=2,
+                                            backgroundColor=(0.2, 0.4, 0.6, 1.0))
+    mv = cr.MultiViewRasteriser(ctx, SIZES[:5])
+    mv.configuration = cfg
+    mv.addPointCloud(a)
+    mv.addPointCloud(b)
+    cams = cameras(cr, SIZES[:5], 9)
+    mv.render(cams)
+    assert_views_match(cr, ctx, mv, [a, b], cfg, cams, SIZES[:5])
+
+
+@pytest.mark.parametrize("variant", ["footprint", "no_clod", "colorize"])
+def test_batched_views_config_variants(cr, orc, ctx, variant):
+    pos, rgba = lattice_cloud(32, 3)
+    cloud = make_cloud(cr, orc, ctx, pos, rgba)
+    kw = {"footprint": dict(minimumPointSize=1.0, maximumPointSize=4.0, pointSizeScale=3.0),
+          "no_clod": dict(enableCLOD=False, enableLODDither=False),
+          "colorize": dict(colorizeChunks=True)}[variant]
+    cfg = cr.ComputeRasteriserConfiguration(**kw)
+    sizes = SIZES[:3]
+    mv = cr.MultiViewRasteriser(ctx, sizes)
+    mv.configuration = cfg
+    mv.addPointCloud(cloud)
+    cams = cameras(cr, sizes, 21)
+    mv.render(cams)
+    assert_views_match(cr, ctx, mv, [cloud], cfg, cams, sizes)
+
+
+def test_autotune_sets_and_caches_the_launch_shape(cr, orc, ctx, tmp_path):
+    pos, rgba = blob_cloud(40000, 12)
+    cloud = make_cloud(cr, orc, ctx, pos, rgba)
+    mv = cr.MultiViewRasteriser(ctx, SIZES[:3])
+    mv.addPointCloud(cloud)
+    cams = cameras(cr, SIZES[:3], 2)
+    path = os.path.join(tmp_path, "tune.jsonl")
+    try:
+        best = mv.autotune(cams, cachePath=path, reps=2)
+        assert best["chunkPoints"] in (512, 1024, 2048, 4096)
+        assert ctx.tuning()["chunkPoints"] == best["chunkPoints"]
+        lines = open(path).read().splitlines()
+        assert len(lines) == 1 and '"candidates"' in lines[0]
+        again = mv.autotune(cams, cachePath=path, reps=2)
+        assert again["chunkPoints"] == best["chunkPoints"]
+        assert again["useTiles"] == best["useTiles"]
+        assert len(open(path).read().splitlines()) == 1  # read, not re-timed
+        mv.render(cams)
+        assert_views_match(cr, ctx, mv, [cloud], mv.configuration, cams, SIZES[:3])
+    finally:
+        ctx.set_tuning(chunkPoints=2048, useTiles=True)
+
+
+def test_batched_views_reject_bad_arguments(cr, orc, ctx):
+    pos, rgba = blob_cloud(2000, 1)
+    cloud = make_cloud(cr, orc, ctx, pos, rgba)
+    mv = cr.MultiViewRasteriser(ctx, [(16, 16), (8, 8)])
+    mv.addPointCloud(cloud)
+    cams = cameras(cr, [(16, 16), (8, 8)], 1)
+    with pytest.raises(cr.CRError):
+        mv.render(cams[:1])
+    mv.configuration = cr.ComputeRasteriserConfiguration(mode=cr.MODE_NEAREST)
+    with pytest.raises(cr.CRError) as e:
+        mv.render(cams)
+    assert e.value.status == 4  # CR_ERR_UNSUPPORTED
+    mv.configuration = cr.ComputeRasteriserConfiguration()
+    mv.frames[1] = mv.frames[0]
+    with pytest.raises(cr.CRError):
+        mv.render(cams)
