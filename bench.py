@@ -67,6 +67,10 @@ def parse_args():
                     help="points per work record of the point passes (launch tuning)")
     ap.add_argument("--tiles", type=int, default=None, choices=[0, 1],
                     help="shared-memory screen tiles on/off (launch tuning)")
+    ap.add_argument("--mv-views", type=int, default=64,
+                    help="views of the batched multi-view comparison (0 = skip it)")
+    ap.add_argument("--mv-points", type=int, default=50_000_000)
+    ap.add_argument("--mv-reps", type=int, default=5)
     return ap.parse_args()
 
 
@@ -146,33 +150,91 @@ def pass_bytes(visible):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region.
+
+    NVML (the device found by its PCI bus id, so the index CUDA sees does not
+    matter) polled every millisecond in a thread; only samples between
+    begin() and end() count.  Falls back to nvidia-smi at 200 ms."""
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
+        self.samples = []  # (t, sm_mhz, reasons mask)
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        self._t0 = self._t1 = None
+        self._nvml = None
         self.proc = None
         self.lines = []
-        self._t = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.device)
+        bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
+            nv, h = self._handle()
+            self._nvml = nv
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def poll():
+                while not self._stop.is_set():
+                    self.samples.append((time.perf_counter(),
+                                         float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                         int(get_reasons(h))))
+                    time.sleep(0.001)
+
+            self._t = threading.Thread(target=poll, daemon=True)
             self._t.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+            while not self.samples:
+                time.sleep(0.001)
+        except Exception:  # no NVML: nvidia-smi
+            self._nvml = None
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                     "--format=csv,noheader,nounits", "-lms", "200"],
+                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self._t = threading.Thread(target=self._read, daemon=True)
+                self._t.start()
+                time.sleep(0.3)
+            except (FileNotFoundError, OSError):
+                self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def begin(self):
+        self._t0 = time.perf_counter()
+
+    def end(self):
+        self._t1 = time.perf_counter()
+        time.sleep(0.003)  # one more sample after the region
+
     def stop(self) -> dict:
+        if self._nvml is not None:
+            self._stop.set()
+            self._t.join(timeout=2)
+            inside = [x for x in self.samples if self._t0 <= x[0] <= self._t1]
+            if not inside:  # region shorter than one poll: the first sample after it
+                inside = [x for x in self.samples if x[0] > self._t1][:1]
+            reasons = sorted(n for n, bit in self.REASONS.items()
+                             if any(m & bit for _, _, m in inside))
+            return {"sm_mhz": statistics.median(x[1] for x in inside) if inside else None,
+                    "sm_max_mhz": self.max_mhz, "reasons": reasons, "samples": len(inside),
+                    "source": "nvml 1 ms"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -198,7 +260,7 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi 200 ms"}
 
 
 def measured_peaks():
@@ -299,14 +361,15 @@ def run_ours(args, dist):
     dist.barrier()
     ctx.synchronize()
     sampler.start()
-    time.sleep(0.3)
     timed = order[args.warmup:]
+    sampler.begin()
     ev0.record(stream)
     for p in timed:
         ras.update(cams[p])
         ras.encode()
     ev1.record(stream)
     ev1.synchronize()
+    sampler.end()
     clocks = sampler.stop()
     ctx.synchronize()
     dist.barrier()
@@ -372,7 +435,92 @@ def run_ours(args, dist):
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"], out["parity"] = cpu_baseline(args, cr, ctx, ras, cloud, cams)
     pinned.close()
+    if args.mv_views > 0:
+        out["multiview"] = run_multiview(args, cr, ctx, torch, dist)
     return out
+
+
+MV_SIZES = ((256, 256), (512, 512), (1280, 720), (1920, 1080))
+
+
+def run_multiview(args, cr, ctx, torch, dist):
+    """Batched views against per-view renders: a heightfield of
+    --mv-points points (seed 0xC0FFEE04), --mv-views cameras at seeded poses
+    with sizes drawn uniformly from 256^2, 512^2, 1280x720 and 1920x1080.
+    Per-view: one ComputeRasteriser update + encode per view.  Batched: one
+    MultiViewRasteriser.render of all views (one CUDA-graph launch), launch
+    shape from the autotuner.  Both timed with CUDA events on the library
+    stream over --mv-reps repetitions; every view's RGBA8, depth and R, G, B,
+    count planes are compared bit for bit."""
+    seed = 0xC0FFEE04
+    params = cr.TerrainParams(seed=seed)
+    mv_args = argparse.Namespace(points=args.mv_points)
+    cloud, _ = build_cloud(cr, ctx, mv_args, params)
+    rng = np.random.default_rng(seed ^ dist.rank)
+    sizes = [MV_SIZES[i] for i in rng.integers(0, len(MV_SIZES), args.mv_views)]
+    cams = make_poses(cr, params, args.mv_views, seed ^ dist.rank, 1.0)
+    for cam, (w, h) in zip(cams, sizes):
+        cam.aspect = w / h
+    saved = ctx.tuning()
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=f"cuda:{dist.local}")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    ras = cr.ComputeRasteriser(ctx)
+    ras.addPointCloud(cloud)
+
+    def per_view():
+        for cam, size in zip(cams, sizes):
+            ras.resize(size)
+            ras.update(cam)
+            ras.encode()
+
+    for _ in range(2):
+        per_view()
+    ctx.synchronize()
+    ev0.record(stream)
+    for _ in range(args.mv_reps):
+        per_view()
+    ev1.record(stream)
+    ev1.synchronize()
+    per_view_ms = ev0.elapsed_time(ev1) / args.mv_reps
+
+    mv = cr.MultiViewRasteriser(ctx, sizes)
+    mv.addPointCloud(cloud)
+    tuned = mv.autotune(cams, reps=3)
+    for _ in range(2):
+        mv.render(cams)
+    ctx.synchronize()
+    ev0.record(stream)
+    for _ in range(args.mv_reps):
+        mv.render(cams)
+    ev1.record(stream)
+    ev1.synchronize()
+    batched_ms = ev0.elapsed_time(ev1) / args.mv_reps
+
+    exact = True
+    for i, (cam, size) in enumerate(zip(cams, sizes)):
+        ras.resize(size)
+        ras.update(cam)
+        ras.encode()
+        a, b = ras.pixels(), mv.pixels(i)
+        exact &= all(np.array_equal(a[f], b[f]) for f in ("depth", "red", "green", "blue",
+                                                          "count"))
+        exact &= bool(np.array_equal(ras.outputRGBA8(), mv.outputRGBA8(i)))
+        exact &= bool(np.array_equal(ras.depthTexture().view(np.uint32),
+                                     mv.depthTexture(i).view(np.uint32)))
+    ctx.set_tuning(chunkPoints=saved["chunkPoints"], useTiles=saved["useTiles"],
+                   viewGroupPixels=saved["viewGroupPixels"])
+    mv.close()
+    cloud.close()
+    n = args.mv_views
+    return {"views": n, "points": args.mv_points,
+            "sizes": {f"{w}x{h}": sizes.count((w, h)) for w, h in MV_SIZES},
+            "per_view_ms": round(per_view_ms, 4), "batched_ms": round(batched_ms, 4),
+            "speedup": round(per_view_ms / batched_ms, 3),
+            "batched_gpts_per_s": round(n * args.mv_points / (batched_ms / 1e3) / 1e9, 2),
+            "bit_exact": bool(exact), "tuning": tuned,
+            "timing": "CUDA events on the library stream, mean of --mv-reps repetitions "
+                      "after 2 warm-ups; per-view includes each view's host calls"}
 
 
 def cpu_baseline(args, cr, ctx, ras, cloud, cams):

@@ -402,8 +402,14 @@ CR_API cr_status cr_context_pass_times(cr_context *ctx, int32_t nframes, float *
  * nearest passes (>= 256); useTiles: accumulate compact batches in
  * shared-memory screen tiles.  Results do not depend on either value. */
 typedef struct cr_tuning {
-    int32_t chunkPoints; /* default 2048 */
-    int32_t useTiles;    /* default 1    */
+    int32_t chunkPoints;     /* default 2048 */
+    int32_t useTiles;        /* default 1    */
+    /* Batched views: the depth and colour passes run over groups of
+     * consecutive views of at most this many pixels in all (a view larger
+     * than the budget forms its own group), so that a group's fragments
+     * stay in L2 between the two passes; 0 = all views in one group.
+     * Default 4194304. */
+    int32_t viewGroupPixels;
 } cr_tuning;
 
 CR_API cr_status cr_context_get_tuning(cr_context *ctx, cr_tuning *out);
@@ -462,9 +468,10 @@ CR_API cr_status cr_render_multiview(cr_context *ctx, cr_frame *const *frames,
                                      uint32_t nclouds, const cr_config *cfg);
 
 /* Autotuner of cr_render_multiview's launch shape (no counterpart in the
- * reference): times chunkPoints in {512, 1024, 2048, 4096} (points per
- * thread = chunkPoints / 256) with and without screen tiles, `reps` renders
- * each after two warm-up renders, sets the fastest on the context and
+ * reference): times 15 candidates of chunkPoints {1024, 2048, 4096} (points
+ * per thread = chunkPoints / 256), screen tiles on / off and the view-group
+ * budget viewGroupPixels {1, 2, 4, 8 Mpx, all}, `reps` renders each after
+ * two warm-up renders, sets the fastest on the context and
  * returns it (and its ms per render).  With cache_path, a result is appended
  * to that file as one JSON object per line keyed by a workload signature
  * (device, SM count, views, pixels, points, configuration), and a later call

@@ -103,13 +103,17 @@ class Context:
     def tuning(self) -> dict:
         t = N.cr_tuning()
         N.check(N.lib().cr_context_get_tuning(self._h, C.byref(t)))
-        return {"chunkPoints": t.chunkPoints, "useTiles": bool(t.useTiles)}
+        return {"chunkPoints": t.chunkPoints, "useTiles": bool(t.useTiles),
+                "viewGroupPixels": t.viewGroupPixels}
 
-    def set_tuning(self, chunkPoints: int | None = None, useTiles: bool | None = None):
+    def set_tuning(self, chunkPoints: int | None = None, useTiles: bool | None = None,
+                   viewGroupPixels: int | None = None):
         """Launch tuning of the point passes (results do not depend on it)."""
         cur = self.tuning()
         t = N.cr_tuning(int(cur["chunkPoints"] if chunkPoints is None else chunkPoints),
-                        int(cur["useTiles"] if useTiles is None else useTiles))
+                        int(cur["useTiles"] if useTiles is None else useTiles),
+                        int(cur["viewGroupPixels"] if viewGroupPixels is None
+                            else viewGroupPixels))
         N.check(N.lib().cr_context_set_tuning(self._h, C.byref(t)))
 
     def set_profiling(self, enable: bool):
@@ -905,7 +909,7 @@ class MultiViewRasteriser:
                                               C.byref(cfg), path, int(reps), C.byref(best),
                                               C.byref(ms)))
         return {"chunkPoints": best.chunkPoints, "useTiles": bool(best.useTiles),
-                "ms": float(ms.value)}
+                "viewGroupPixels": best.viewGroupPixels, "ms": float(ms.value)}
 
     def outputRGBA8(self, view: int, out: np.ndarray | None = None) -> np.ndarray:
         return self.frames[view].rgba8(out)

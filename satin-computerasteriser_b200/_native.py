@@ -72,7 +72,8 @@ class cr_synth_terrain(C.Structure):
 
 
 class cr_tuning(C.Structure):
-    _fields_ = [("chunkPoints", C.c_int32), ("useTiles", C.c_int32)]
+    _fields_ = [("chunkPoints", C.c_int32), ("useTiles", C.c_int32),
+                ("viewGroupPixels", C.c_int32)]
 
 
 class cr_cloud_info(C.Structure):

@@ -209,7 +209,7 @@ cr_status allocate_cloud(cr_cloud *c, cr_capacity cap, const cr_raster_file *fil
     if ((st = dalloc(&c->d_batches, nb * sizeof(cr_raster_batch))) ||
         (st = dalloc(&c->d_visible, nb * sizeof(cr_visible_batch))) ||
         (st = dalloc(&c->d_cull_tmp, ctas * 256 * sizeof(CullRec))) ||
-        (st = dalloc(&c->d_cull_cta, ctas * 2 * sizeof(uint32_t))) ||
+        (st = dalloc(&c->d_cull_cta, ctas * kCullCtaWords * sizeof(uint32_t))) ||
         (st = dalloc(&c->d_counters, CNT_COUNT * sizeof(uint32_t))))
         return st;
     c->chunk_cap = chunk_capacity(cap, kMinChunkPoints);
@@ -1033,6 +1033,7 @@ CR_API cr_status cr_context_get_tuning(cr_context *ctx, cr_tuning *out) {
     if (!ctx || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
     out->chunkPoints = ctx->chunk_points;
     out->useTiles = ctx->use_tiles ? 1 : 0;
+    out->viewGroupPixels = ctx->view_group_pixels;
     return CR_OK;
 }
 
@@ -1040,8 +1041,11 @@ CR_API cr_status cr_context_set_tuning(cr_context *ctx, const cr_tuning *t) {
     if (!ctx || !t) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
     if (t->chunkPoints < kMinChunkPoints || t->chunkPoints > 65536)
         return fail(CR_ERR_INVALID_ARGUMENT, "chunkPoints must be in [256, 65536]");
+    if (t->viewGroupPixels < 0)
+        return fail(CR_ERR_INVALID_ARGUMENT, "viewGroupPixels must be >= 0");
     ctx->chunk_points = t->chunkPoints;
     ctx->use_tiles = t->useTiles != 0;
+    ctx->view_group_pixels = t->viewGroupPixels;
     return CR_OK;
 }
 

@@ -36,6 +36,7 @@ enum CounterSlot : int {
     CNT_ARGS_Y = 5,
     CNT_ARGS_Z = 6,
     CNT_ERROR = 7,       // first device-side error code (0 = none)
+    CNT_POINTS = 8,      // fragment span of the last cull's survivors (chunks rounded to 4)
     CNT_COUNT = 32
 };
 
@@ -81,6 +82,7 @@ struct cr_context {
     int blocks_per_sm[5] = {0, 0, 0, 0, 0};        // occupancy of the persistent point passes
     int blocks_per_sm_views[5] = {0, 0, 0, 0, 0};  // the same, batched-view kernels
     int chunk_points = 2048;           // points per chunk work record
+    int view_group_pixels = 4194304;   // batched views: pixels per depth/colour group
     bool use_tiles = true;             // shared-memory screen tiles
     // Profiling: a ring of frames, each with a start/stop event per pass.
     static constexpr int kProfRing = 256;
@@ -171,6 +173,10 @@ struct CullUniforms {
     int enableFrustumCulling, lodBias, enableCLOD;
 };
 
+// Words per 256-slot CTA in CullArgs::cta_counts: survivors, chunk records,
+// fragment span.
+constexpr uint32_t kCullCtaWords = 3;
+
 // Arguments of the cull of one view of one cloud (inputs, scratch, outputs).
 struct CullArgs {
     const cr_raster_batch *batches;
@@ -178,12 +184,14 @@ struct CullArgs {
     const cr_raster_file *files;
     uint32_t nfiles;
     CullRec *tmp;           // nbatches records
-    uint32_t *cta_counts;   // 2 per 256-slot CTA
+    uint32_t *cta_counts;   // kCullCtaWords per 256-slot CTA
     uint32_t chunk_points;
     CullUniforms u;
     cr_visible_batch *visible;  // nbatches
     ChunkRec *chunks;           // chunk capacity of the cloud
     uint32_t *counters;         // CNT_COUNT words
+    uint32_t *chunk_poff;       // per chunk record: offset of its fragments within the
+                                // view's fragment span, a multiple of 4 (NULL: not written)
 };
 
 cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s);
@@ -259,16 +267,31 @@ struct ViewDesc {
 };
 static_assert(sizeof(ViewDesc) == 192, "ViewDesc is 192 bytes");
 
-// The point pass `pass` (PASS_DEPTH / PASS_COLOR / PASS_NEAREST) of one cloud
-// over all views in one launch.  Chunk records of view v start at
-// chunks + v * chunk_stride and its counters at counters + v * CNT_COUNT;
-// its file table at files + v * nfiles.  u carries the configuration (the
-// per-view sizes and cameras come from views).
+// Fragment arena of one cloud's batched views: view v's fragments occupy
+// [prefix of the views' fragment spans, + its span); chunk record j of view
+// v has its count at count[v * chunk_stride + j] and its offset within the
+// view's span at poff[same].  cap entries; *overflow is set by the depth
+// pass when the spans exceed cap (the colour pass then decodes the points).
+struct ViewsFragments {
+    uint32_t *xy;
+    float *z;
+    uint32_t *col;
+    uint32_t *count;
+    const uint32_t *poff;
+    unsigned long long cap;
+    uint32_t *overflow;
+};
+
+// The point pass `pass` of one cloud over all views in one launch.  Chunk
+// records of view v start at chunks + v * chunk_stride and its counters at
+// counters + v * CNT_COUNT; its file table at files + v * nfiles.  u carries
+// the configuration (the per-view sizes and cameras come from views).
+// PASS_DEPTH_FRAG / PASS_COLOR_FRAG need frags.
 cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
                               const RasterTargets &t, const ViewDesc *views, uint32_t nviews,
                               const cr_raster_file *files, uint32_t nfiles,
                               const ChunkRec *chunks, uint32_t chunk_stride,
-                              uint32_t *counters, cudaStream_t s);
+                              uint32_t *counters, const ViewsFragments *frags, cudaStream_t s);
 
 struct ResolveUniforms {
     int width, height;
@@ -282,18 +305,20 @@ cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t
 // Zeroes the accumulators if *f->d_redo != 0.
 cr_status launch_accum_redo_clear(cr_frame *f, cudaStream_t s);
 
-// Batched views (all views' pixels as one range, total_pix in all):
-// zero every view's depth plane and accumulators, and *redo_flag.
-cr_status launch_clear_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
-                             uint32_t *redo_flag, int sm_count, cudaStream_t s);
-// Zero the accumulators if *redo_flag != 0.
+// Batched views: every view's pixels form one range, view after view
+// (ViewDesc::pix_begin); views [0, nviews) of `views` cover [pix0, pix0+npix).
+// Zero those views' depth planes and accumulators (and *redo_flag if
+// zero_flag).
+cr_status launch_clear_views(const ViewDesc *views, uint32_t nviews, uint32_t pix0, uint32_t npix,
+                             uint32_t *redo_flag, bool zero_flag, int sm_count, cudaStream_t s);
+// Zero every view's accumulators if *redo_flag != 0 (views from view 0).
 cr_status launch_accum_redo_clear_views(const ViewDesc *views, uint32_t nviews,
                                         uint32_t total_pix, const uint32_t *redo_flag,
                                         int sm_count, cudaStream_t s);
-// Resolve of every view (check / redo as launch_resolve_hqs).
-cr_status launch_resolve_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
-                               const ResolveUniforms &u, uint32_t *redo_flag, bool check,
-                               const uint32_t *redo, int sm_count, cudaStream_t s);
+// Resolve of those views (check / redo as launch_resolve_hqs).
+cr_status launch_resolve_views(const ViewDesc *views, uint32_t nviews, uint32_t pix0,
+                               uint32_t npix, const ResolveUniforms &u, uint32_t *redo_flag,
+                               bool check, const uint32_t *redo, int sm_count, cudaStream_t s);
 // One hole-fill iteration of every view: rgba[src] -> rgba[1 - src].
 cr_status launch_hole_fill_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
                                  int src, int sm_count, cudaStream_t s);

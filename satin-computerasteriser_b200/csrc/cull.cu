@@ -116,9 +116,19 @@ __device__ __forceinline__ uint32_t nchunks(uint32_t active, uint32_t c) {
     return (active + c - 1u) / c;
 }
 
+__device__ __forceinline__ uint32_t round4(uint32_t n) { return (n + 3u) & ~3u; }
+
+// Fragment span of a survivor: its chunks' point counts, each rounded up to
+// a multiple of four, so that every chunk's fragments start 16-byte aligned.
+__device__ __forceinline__ uint32_t fragment_span(uint32_t active, uint32_t c) {
+    const uint32_t nc = nchunks(active, c);
+    return nc == 0u ? 0u : (nc - 1u) * round4(c) + round4(active - (nc - 1u) * c);
+}
+
 __device__ __forceinline__ void classify_body(const CullArgs &a) {
     __shared__ uint32_t warp_counts[kCullThreads / 32];
     __shared__ uint32_t warp_chunks[kCullThreads / 32];
+    __shared__ uint32_t warp_points[kCullThreads / 32];
     const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     CullRec rec;
@@ -127,68 +137,36 @@ __device__ __forceinline__ void classify_body(const CullArgs &a) {
     const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
     const uint32_t ch = __reduce_add_sync(
         0xffffffffu, keep ? nchunks(rec.vb.activePoints, a.chunk_points) : 0u);
+    const uint32_t pts = __reduce_add_sync(
+        0xffffffffu, keep ? fragment_span(rec.vb.activePoints, a.chunk_points) : 0u);
     if (lane == 0) {
         warp_counts[warp] = __popc(ballot);
         warp_chunks[warp] = ch;
+        warp_points[warp] = pts;
     }
     __syncthreads();
-    uint32_t before = 0, total = 0, total_chunks = 0;
+    uint32_t before = 0, total = 0, total_chunks = 0, total_points = 0;
 #pragma unroll
     for (int w = 0; w < kCullThreads / 32; ++w) {
         if (w < warp) before += warp_counts[w];
         total += warp_counts[w];
         total_chunks += warp_chunks[w];
+        total_points += warp_points[w];
     }
     if (keep) {
         const uint32_t pos = before + __popc(ballot & ((1u << lane) - 1u));
         a.tmp[blockIdx.x * kCullThreads + pos] = rec;
     }
     if (threadIdx.x == 0) {
-        a.cta_counts[2 * blockIdx.x] = total;
-        a.cta_counts[2 * blockIdx.x + 1] = total_chunks;
+        a.cta_counts[kCullCtaWords * blockIdx.x] = total;
+        a.cta_counts[kCullCtaWords * blockIdx.x + 1] = total_chunks;
+        a.cta_counts[kCullCtaWords * blockIdx.x + 2] = total_points;
     }
 }
 
-__device__ __forceinline__ void compact_body(const CullArgs &a) {
-    const CullRec *tmp = a.tmp;
-    const uint32_t *cta_counts = a.cta_counts;
-    cr_visible_batch *out = a.visible;
-    ChunkRec *chunks = a.chunks;
-    const uint32_t chunk_points = a.chunk_points;
-    uint32_t *counters = a.counters;
-    __shared__ uint32_t part_v[kCullThreads / 32], part_c[kCullThreads / 32];
-    __shared__ uint32_t scan_w[kCullThreads / 32];
+// Exclusive block-wide prefix of one value per thread (256 threads).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t c, uint32_t *scan_w) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // Exclusive prefix of the survivor and chunk counts of the CTAs before this one.
-    uint32_t sv = 0, sc = 0;
-    for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kCullThreads) {
-        sv += cta_counts[2 * i];
-        sc += cta_counts[2 * i + 1];
-    }
-    sv = __reduce_add_sync(0xffffffffu, sv);
-    sc = __reduce_add_sync(0xffffffffu, sc);
-    if (lane == 0) {
-        part_v[warp] = sv;
-        part_c[warp] = sc;
-    }
-    __syncthreads();
-    uint32_t off_v = 0, off_c = 0;
-#pragma unroll
-    for (int w = 0; w < kCullThreads / 32; ++w) {
-        off_v += part_v[w];
-        off_c += part_c[w];
-    }
-    const uint32_t mine = cta_counts[2 * blockIdx.x];
-    const uint32_t mine_chunks = cta_counts[2 * blockIdx.x + 1];
-    // One survivor per thread (a CTA holds at most 256): ordered copy and an
-    // exclusive scan of the chunk counts for the chunk record offsets.
-    CullRec r;
-    uint32_t c = 0;
-    if (threadIdx.x < mine) {
-        r = tmp[blockIdx.x * kCullThreads + threadIdx.x];
-        out[off_v + threadIdx.x] = r.vb;
-        c = nchunks(r.vb.activePoints, chunk_points);
-    }
     uint32_t x = c;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -201,7 +179,59 @@ __device__ __forceinline__ void compact_body(const CullArgs &a) {
 #pragma unroll
     for (int w = 0; w < kCullThreads / 32; ++w)
         if (w < warp) wbase += scan_w[w];
-    const uint32_t base = off_c + wbase + (x - c);
+    return wbase + (x - c);
+}
+
+__device__ __forceinline__ void compact_body(const CullArgs &a) {
+    const CullRec *tmp = a.tmp;
+    const uint32_t *cta_counts = a.cta_counts;
+    cr_visible_batch *out = a.visible;
+    ChunkRec *chunks = a.chunks;
+    const uint32_t chunk_points = a.chunk_points;
+    uint32_t *counters = a.counters;
+    __shared__ uint32_t part_v[kCullThreads / 32], part_c[kCullThreads / 32],
+        part_p[kCullThreads / 32];
+    __shared__ uint32_t scan_c[kCullThreads / 32], scan_p[kCullThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // Exclusive prefix of the survivor, chunk and point counts of the CTAs before this one.
+    uint32_t sv = 0, sc = 0, sp = 0;
+    for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kCullThreads) {
+        sv += cta_counts[kCullCtaWords * i];
+        sc += cta_counts[kCullCtaWords * i + 1];
+        sp += cta_counts[kCullCtaWords * i + 2];
+    }
+    sv = __reduce_add_sync(0xffffffffu, sv);
+    sc = __reduce_add_sync(0xffffffffu, sc);
+    sp = __reduce_add_sync(0xffffffffu, sp);
+    if (lane == 0) {
+        part_v[warp] = sv;
+        part_c[warp] = sc;
+        part_p[warp] = sp;
+    }
+    __syncthreads();
+    uint32_t off_v = 0, off_c = 0, off_p = 0;
+#pragma unroll
+    for (int w = 0; w < kCullThreads / 32; ++w) {
+        off_v += part_v[w];
+        off_c += part_c[w];
+        off_p += part_p[w];
+    }
+    const uint32_t mine = cta_counts[kCullCtaWords * blockIdx.x];
+    const uint32_t mine_chunks = cta_counts[kCullCtaWords * blockIdx.x + 1];
+    const uint32_t mine_points = cta_counts[kCullCtaWords * blockIdx.x + 2];
+    // One survivor per thread (a CTA holds at most 256): ordered copy and
+    // exclusive scans of the chunk and point counts for the chunk record
+    // offsets and the chunks' point offsets.
+    CullRec r;
+    uint32_t c = 0, n = 0;
+    if (threadIdx.x < mine) {
+        r = tmp[blockIdx.x * kCullThreads + threadIdx.x];
+        out[off_v + threadIdx.x] = r.vb;
+        c = nchunks(r.vb.activePoints, chunk_points);
+        n = fragment_span(r.vb.activePoints, chunk_points);
+    }
+    const uint32_t base = off_c + block_exclusive_scan(c, scan_c);
+    const uint32_t pbase = off_p + block_exclusive_scan(n, scan_p);
     for (uint32_t j = 0; j < c; ++j) {
         ChunkRec k;
         k.first = r.first + j * chunk_points;
@@ -221,6 +251,7 @@ __device__ __forceinline__ void compact_body(const CullArgs &a) {
         k.tw = r.tw;
         k.th = r.th;
         chunks[base + j] = k;
+        if (a.chunk_poff) a.chunk_poff[base + j] = pbase + j * round4(chunk_points);
     }
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
         // cullFinalizeUpdate (CullFinalize/Shaders.metal:3-14): {count, 1, 1}.
@@ -231,6 +262,7 @@ __device__ __forceinline__ void compact_body(const CullArgs &a) {
         counters[CNT_WORK_DEPTH] = 0u;
         counters[CNT_WORK_COLOR] = 0u;
         counters[CNT_CHUNKS] = off_c + mine_chunks;
+        counters[CNT_POINTS] = off_p + mine_points;
     }
 }
 
@@ -254,6 +286,7 @@ __global__ void cull_empty(uint32_t *counters) {
     counters[CNT_WORK_DEPTH] = 0u;
     counters[CNT_WORK_COLOR] = 0u;
     counters[CNT_CHUNKS] = 0u;
+    counters[CNT_POINTS] = 0u;
 }
 
 }  // namespace
@@ -274,7 +307,7 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s) {
     const uint32_t ctas = (n + kCullThreads - 1) / kCullThreads;
     CullArgs a{cloud->d_batches, n,  cloud->d_files,   (uint32_t)cloud->files.size(),
                cloud->d_cull_tmp, cloud->d_cull_cta, cp, u, cloud->d_visible, cloud->d_chunks,
-               cloud->d_counters};
+               cloud->d_counters, nullptr};
     cull_classify<<<ctas, kCullThreads, 0, s>>>(a);
     CR_CUDA(cudaGetLastError());
     cull_compact<<<ctas, kCullThreads, 0, s>>>(a);

@@ -93,6 +93,12 @@ struct RasterArgs {
     uint32_t nviews;
     uint32_t nfiles;        // files per view; view v's table starts at files + v * nfiles
     uint32_t chunk_stride;  // view v's chunk records start at chunks + v * chunk_stride
+    // Batched views with fragments: chunk record -> offset in its view's
+    // fragment span; the arena's capacity; set by the depth pass when the
+    // views' spans do not fit (the colour pass then decodes the points).
+    const uint32_t *chunk_poff;
+    unsigned long long frag_cap;
+    uint32_t *frag_overflow;
 };
 
 // The frame and camera of the view whose chunk a CTA is drawing (MV kernels).
@@ -132,6 +138,62 @@ __device__ __forceinline__ const float *view_proj(const RasterArgs &a) {
     return MV ? s_view.proj : a.u.proj;
 }
 
+// The current view's size and planes in registers: read once per chunk, not
+// per point (loads from shared memory could not be hoisted past the
+// shared-memory atomics); for one view, the kernel's own parameters.
+template <bool MV>
+struct ViewRegsT;
+template <>
+struct ViewRegsT<true> {
+    int W, H;
+    uint32_t *depth;
+    uint4 *accum;
+    unsigned long long *nearest;
+};
+template <>
+struct ViewRegsT<false> {  // reads the kernel parameters where used
+    const RasterArgs &a;
+    __device__ __forceinline__ ViewRegsT(const RasterArgs &args) : a(args) {}
+};
+template <bool MV>
+__device__ __forceinline__ int vw(const ViewRegsT<MV> &r);
+template <>
+__device__ __forceinline__ int vw<true>(const ViewRegsT<true> &r) { return r.W; }
+template <>
+__device__ __forceinline__ int vw<false>(const ViewRegsT<false> &r) { return r.a.u.width; }
+template <bool MV>
+__device__ __forceinline__ int vh(const ViewRegsT<MV> &r);
+template <>
+__device__ __forceinline__ int vh<true>(const ViewRegsT<true> &r) { return r.H; }
+template <>
+__device__ __forceinline__ int vh<false>(const ViewRegsT<false> &r) { return r.a.u.height; }
+template <bool MV>
+__device__ __forceinline__ uint32_t *vdepth(const ViewRegsT<MV> &r);
+template <>
+__device__ __forceinline__ uint32_t *vdepth<true>(const ViewRegsT<true> &r) { return r.depth; }
+template <>
+__device__ __forceinline__ uint32_t *vdepth<false>(const ViewRegsT<false> &r) { return r.a.t.depth; }
+template <bool MV>
+__device__ __forceinline__ uint4 *vaccum(const ViewRegsT<MV> &r);
+template <>
+__device__ __forceinline__ uint4 *vaccum<true>(const ViewRegsT<true> &r) { return r.accum; }
+template <>
+__device__ __forceinline__ uint4 *vaccum<false>(const ViewRegsT<false> &r) { return r.a.t.accum; }
+template <bool MV>
+__device__ __forceinline__ unsigned long long *vnearest(const ViewRegsT<MV> &r);
+template <>
+__device__ __forceinline__ unsigned long long *vnearest<true>(const ViewRegsT<true> &r) {
+    return r.nearest;
+}
+template <>
+__device__ __forceinline__ unsigned long long *vnearest<false>(const ViewRegsT<false> &r) {
+    return r.a.t.nearest;
+}
+__device__ __forceinline__ ViewRegsT<true> view_regs_mv() {
+    return ViewRegsT<true>{s_view.width, s_view.height, s_view.depth, s_view.accum,
+                           s_view.nearest};
+}
+
 struct BatchShared {
     float T[16];      // file.transform
     float world[16];  // file.world (footprint only)
@@ -159,7 +221,7 @@ __device__ __forceinline__ bool keep_point(const RasterArgs &a, const ChunkRec &
 // decodePoint + projection + clip + pixel (DepthPass/Shaders.metal:188-211,
 // ColorPass/Shaders.metal:70-104, NearestDepth/Shaders.metal:68-85).
 template <int PASS, bool MV>
-__device__ __forceinline__ void project_point(const RasterArgs &a, const BatchShared &sb,
+__device__ __forceinline__ void project_point(const RasterArgs &a, const ViewRegsT<MV> &vr, const BatchShared &sb,
                                               const ChunkRec &c, uint32_t lo, uint32_t me,
                                               uint32_t hi, PointOut &o) {
     // Branch-free split-precision decode: a word the chunk's level does not
@@ -182,7 +244,7 @@ __device__ __forceinline__ void project_point(const RasterArgs &a, const BatchSh
     const float nx = clip.x / clip.w, ny = clip.y / clip.w, nz = clip.z / clip.w;
     if (nx < -1.0f || ny < -1.0f || nx > 1.0f || ny > 1.0f || nz > 1.0f) ok = false;
     if (PASS == PASS_NEAREST ? (nz <= 0.0f) : (nz < 0.0f)) ok = false;
-    const int W = view_w<MV>(a), H = view_h<MV>(a);
+    const int W = vw<MV>(vr), H = vh<MV>(vr);
     o.ix = (int)((nx * 0.5f + 0.5f) * (float)W);
     const int iy = (int)((ny * 0.5f + 0.5f) * (float)H);
     if (o.ix < 0 || o.ix >= W || iy < 0 || iy >= H) ok = false;
@@ -202,6 +264,28 @@ __device__ __forceinline__ unsigned long long nearest_key(uint32_t depth, uint32
     return ((unsigned long long)depth << 32) | (unsigned long long)(~index);
 }
 
+// Reductions into the frame planes (global memory).  Written as red.global
+// on explicitly global addresses: the batched-view passes take the plane
+// pointers from shared memory, where the compiler cannot tell their
+// address space, and would otherwise emit generic atomics that wait for a
+// returned value.
+__device__ __forceinline__ void red_add_u32(uint32_t *p, uint32_t v) {
+    asm volatile("red.global.add.u32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v)
+                 : "memory");
+}
+__device__ __forceinline__ void red_add_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v)
+                 : "memory");
+}
+__device__ __forceinline__ void red_max_u32(uint32_t *p, uint32_t v) {
+    asm volatile("red.global.max.u32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v)
+                 : "memory");
+}
+__device__ __forceinline__ void red_max_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("red.global.max.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v)
+                 : "memory");
+}
+
 // Adds one sample group to a pixel's R, G, B and count.  Packed: the uint4
 // as two 64-bit words, R | G << 32 and B | count << 32 — half the global
 // atomics.  A lower field that passes 2^32 would carry into its neighbour;
@@ -209,36 +293,36 @@ __device__ __forceinline__ unsigned long long nearest_key(uint32_t depth, uint32
 // resolve detects (the frame is then re-run unpacked).  Unpacked: one
 // 32-bit add per field.
 template <bool MV>
-__device__ __forceinline__ void color_global(const RasterArgs &a, uint32_t pix, uint32_t r,
+__device__ __forceinline__ void color_global(const RasterArgs &a, const ViewRegsT<MV> &vr, uint32_t pix, uint32_t r,
                                              uint32_t g, uint32_t b, uint32_t n) {
     if (a.t.packed) {
-        unsigned long long *w = reinterpret_cast<unsigned long long *>(&view_accum<MV>(a)[pix]);
-        atomicAdd(w, (unsigned long long)r | ((unsigned long long)g << 32));
-        atomicAdd(w + 1, (unsigned long long)b | ((unsigned long long)n << 32));
+        unsigned long long *w = reinterpret_cast<unsigned long long *>(&vaccum<MV>(vr)[pix]);
+        red_add_u64(w, (unsigned long long)r | ((unsigned long long)g << 32));
+        red_add_u64(w + 1, (unsigned long long)b | ((unsigned long long)n << 32));
     } else {
-        unsigned int *acc = reinterpret_cast<unsigned int *>(&view_accum<MV>(a)[pix]);
-        atomicAdd(acc + 0, r);
-        atomicAdd(acc + 1, g);
-        atomicAdd(acc + 2, b);
-        atomicAdd(acc + 3, n);
+        unsigned int *acc = reinterpret_cast<unsigned int *>(&vaccum<MV>(vr)[pix]);
+        red_add_u32(acc + 0, r);
+        red_add_u32(acc + 1, g);
+        red_add_u32(acc + 2, b);
+        red_add_u32(acc + 3, n);
     }
 }
 
 // Direct path, radius 0: one global atomic per point (batches large on
 // screen, where points rarely share a pixel).
 template <int PASS, bool MV>
-__device__ __forceinline__ void emit_direct(const RasterArgs &a, const PointOut &o) {
-    const uint32_t pix = (uint32_t)(o.iy * view_w<MV>(a) + o.ix);
+__device__ __forceinline__ void emit_direct(const RasterArgs &a, const ViewRegsT<MV> &vr, const PointOut &o) {
+    const uint32_t pix = (uint32_t)(o.iy * vw<MV>(vr) + o.ix);
     if (is_depth(PASS)) {
-        if (o.ok) atomicMax(&view_depth<MV>(a)[pix], o.depth);
+        if (o.ok) red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
     } else if (is_color(PASS)) {
-        const uint32_t closest = o.ok ? view_depth<MV>(a)[pix] : 0u;
+        const uint32_t closest = o.ok ? vdepth<MV>(vr)[pix] : 0u;
         const bool vis = closest != 0u && o.nz >= crd::uint_to_depth(closest) * a.keep_scale;
         if (vis)
-            color_global<MV>(a, pix, o.color & 0xffu, (o.color >> 8) & 0xffu, (o.color >> 16) & 0xffu,
+            color_global<MV>(a, vr, pix, o.color & 0xffu, (o.color >> 8) & 0xffu, (o.color >> 16) & 0xffu,
                          1u);
     } else {
-        if (o.ok) atomicMax(&view_nearest<MV>(a)[pix], nearest_key(o.depth, o.pointIndex));
+        if (o.ok) red_max_u64(&vnearest<MV>(vr)[pix], nearest_key(o.depth, o.pointIndex));
     }
 }
 
@@ -246,22 +330,22 @@ __device__ __forceinline__ void emit_direct(const RasterArgs &a, const PointOut 
 // that round outside the rectangle.  Colour tiles hold R | count << 20, G and
 // B per pixel in 32-bit words (exact while a chunk has at most 4095 points).
 template <int PASS, bool MV>
-__device__ __forceinline__ void emit_tile(const RasterArgs &a, const ChunkRec &c,
+__device__ __forceinline__ void emit_tile(const RasterArgs &a, const ViewRegsT<MV> &vr, const ChunkRec &c,
                                           unsigned char *smem, const PointOut &o) {
     const int lx = o.ix - c.x0, ly = o.iy - c.y0;
     const bool inside = (unsigned)lx < (unsigned)c.tw && (unsigned)ly < (unsigned)c.th;
     const bool in_tile = o.ok && inside, outside = o.ok && !inside;
-    const uint32_t pix = (uint32_t)(o.iy * view_w<MV>(a) + o.ix);
+    const uint32_t pix = (uint32_t)(o.iy * vw<MV>(vr) + o.ix);
     const int l = inside ? ly * c.tw + lx : 0;
     if (is_depth(PASS)) {
         if (in_tile) atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
-        if (outside) atomicMax(&view_depth<MV>(a)[pix], o.depth);
+        if (outside) red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
     } else if (is_color(PASS)) {
         constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
         uint32_t *acc = reinterpret_cast<uint32_t *>(smem);
         const uint32_t *sdep = acc + 3 * kPx;
         uint32_t closest = sdep[l];
-        if (outside) closest = view_depth<MV>(a)[pix];
+        if (outside) closest = vdepth<MV>(vr)[pix];
         const bool vis = o.ok && closest != 0u &&
                          o.nz >= crd::uint_to_depth(closest) * a.keep_scale;
         const uint32_t r = o.color & 0xffu, g = (o.color >> 8) & 0xffu,
@@ -271,24 +355,24 @@ __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ChunkRec &c
             atomicAdd(acc + kPx + l, g);
             atomicAdd(acc + 2 * kPx + l, b);
         }
-        if (vis && !inside) color_global<MV>(a, pix, r, g, b, 1u);
+        if (vis && !inside) color_global<MV>(a, vr, pix, r, g, b, 1u);
     } else {
         const unsigned long long k = nearest_key(o.depth, o.pointIndex);
         if (in_tile) atomicMax(reinterpret_cast<unsigned long long *>(smem) + l, k);
-        if (outside) atomicMax(&view_nearest<MV>(a)[pix], k);
+        if (outside) red_max_u64(&vnearest<MV>(vr)[pix], k);
     }
 }
 
 // General footprint (radius from pointFootprintRadius), global atomics.
 template <int PASS, bool MV>
-__device__ __forceinline__ void emit_footprint(const RasterArgs &a, const BatchShared &sb,
+__device__ __forceinline__ void emit_footprint(const RasterArgs &a, const ViewRegsT<MV> &vr, const BatchShared &sb,
                                                const PointOut &o) {
     if (!o.ok) return;
     const crd::PointSize ps{a.u.pointSizeMode, a.u.minimumPointSize, a.u.maximumPointSize,
                             a.u.pointSizeScale};
     const int rad =
-        crd::footprint_radius(o.px, o.py, o.pz, sb.world, view_view<MV>(a), view_proj<MV>(a), view_h<MV>(a), ps);
-    const int W = view_w<MV>(a), H = view_h<MV>(a);
+        crd::footprint_radius(o.px, o.py, o.pz, sb.world, view_view<MV>(a), view_proj<MV>(a), vh<MV>(vr), ps);
+    const int W = vw<MV>(vr), H = vh<MV>(vr);
     for (int oy = -rad; oy <= rad; ++oy) {
         for (int ox = -rad; ox <= rad; ++ox) {
             if (!crd::inside_footprint(ox, oy, rad)) continue;
@@ -296,15 +380,15 @@ __device__ __forceinline__ void emit_footprint(const RasterArgs &a, const BatchS
             if (tx < 0 || tx >= W || ty < 0 || ty >= H) continue;
             const uint32_t pix = (uint32_t)(ty * W + tx);
             if (is_depth(PASS)) {
-                atomicMax(&view_depth<MV>(a)[pix], o.depth);
+                red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
             } else if (is_color(PASS)) {
-                const uint32_t closest = view_depth<MV>(a)[pix];
+                const uint32_t closest = vdepth<MV>(vr)[pix];
                 if (closest == 0u) continue;
                 if (!(o.nz >= crd::uint_to_depth(closest) * a.keep_scale)) continue;
-                color_global<MV>(a, pix, o.color & 0xffu, (o.color >> 8) & 0xffu,
+                color_global<MV>(a, vr, pix, o.color & 0xffu, (o.color >> 8) & 0xffu,
                              (o.color >> 16) & 0xffu, 1u);
             } else {
-                atomicMax(&view_nearest<MV>(a)[pix], nearest_key(o.depth, o.pointIndex));
+                red_max_u64(&vnearest<MV>(vr)[pix], nearest_key(o.depth, o.pointIndex));
             }
         }
     }
@@ -313,9 +397,9 @@ __device__ __forceinline__ void emit_footprint(const RasterArgs &a, const BatchS
 // Shared count of the fragments the current chunk has kept.
 __shared__ uint32_t s_frag_count;
 
-// Appends the warp's kept points to the chunk's fragment range [first, first+n):
+// Appends the warp's kept points to the chunk's fragment range [fbase, fbase+n):
 // one shared-memory atomic per warp, lanes placed by ballot rank.
-__device__ __forceinline__ void emit_fragment(const RasterArgs &a, const ChunkRec &c,
+__device__ __forceinline__ void emit_fragment(const RasterArgs &a, uint32_t fbase,
                                               const PointOut &o) {
     const uint32_t ballot = __ballot_sync(kFull, o.ok);
     const int lane = threadIdx.x & 31;
@@ -323,7 +407,7 @@ __device__ __forceinline__ void emit_fragment(const RasterArgs &a, const ChunkRe
     if (lane == 0) base = atomicAdd(&s_frag_count, __popc(ballot));
     base = __shfl_sync(kFull, base, 0);
     if (o.ok) {
-        const uint32_t i = c.first + base + __popc(ballot & ((1u << lane) - 1u));
+        const uint32_t i = fbase + base + __popc(ballot & ((1u << lane) - 1u));
         a.frag_xy[i] = (uint32_t)o.ix | ((uint32_t)o.iy << 16);
         a.frag_z[i] = o.nz;
         a.frag_col[i] = o.color;
@@ -332,28 +416,30 @@ __device__ __forceinline__ void emit_fragment(const RasterArgs &a, const ChunkRe
 
 // One point; every lane of the warp calls this (warp-uniform early outs).
 template <int PASS, bool MV>
-__device__ __forceinline__ void do_point(const RasterArgs &a, const BatchShared &sb,
+__device__ __forceinline__ void do_point(const RasterArgs &a, const ViewRegsT<MV> &vr, const BatchShared &sb,
                                          unsigned char *smem, const ChunkRec &c, bool tiled,
                                          bool valid, uint32_t local, uint32_t lvl, uint32_t lo,
-                                         uint32_t me, uint32_t hi, uint32_t color) {
+                                         uint32_t me, uint32_t hi, uint32_t color, uint32_t fbase,
+                                         bool emit) {
     PointOut o;
     o.pointIndex = c.first + local;
     o.color = color;
     o.ok = valid && keep_point(a, c, o.pointIndex, lvl);
     if (!__any_sync(kFull, o.ok)) return;
-    project_point<PASS, MV>(a, sb, c, lo, me, hi, o);
+    project_point<PASS, MV>(a, vr, sb, c, lo, me, hi, o);
     if (!__any_sync(kFull, o.ok)) return;
     if (!a.radius_zero)
-        emit_footprint<PASS, MV>(a, sb, o);
+        emit_footprint<PASS, MV>(a, vr, sb, o);
     else if (tiled)
-        emit_tile<PASS, MV>(a, c, smem, o);
+        emit_tile<PASS, MV>(a, vr, c, smem, o);
     else
-        emit_direct<PASS, MV>(a, o);
-    if (PASS == PASS_DEPTH_FRAG) emit_fragment(a, c, o);
+        emit_direct<PASS, MV>(a, vr, o);
+    if (PASS == PASS_DEPTH_FRAG && emit) emit_fragment(a, fbase, o);
 }
 
 // One fragment of the colour pass (PASS_COLOR_FRAG); every lane calls this.
-__device__ __forceinline__ void do_fragment(const RasterArgs &a, unsigned char *smem,
+template <bool MV>
+__device__ __forceinline__ void do_fragment(const RasterArgs &a, const ViewRegsT<MV> &vr, unsigned char *smem,
                                             const ChunkRec &c, bool tiled, bool valid,
                                             uint32_t xy, float nz, uint32_t color) {
     PointOut o;
@@ -363,16 +449,17 @@ __device__ __forceinline__ void do_fragment(const RasterArgs &a, unsigned char *
     o.nz = nz;
     o.color = color;
     if (tiled)
-        emit_tile<PASS_COLOR_FRAG, false>(a, c, smem, o);
+        emit_tile<PASS_COLOR_FRAG, MV>(a, vr, c, smem, o);
     else
-        emit_direct<PASS_COLOR_FRAG, false>(a, o);
+        emit_direct<PASS_COLOR_FRAG, MV>(a, vr, o);
 }
 
 // Four fragments of one thread in the colour pass, the first `nvalid` of
 // them real.  The settled depths of all four pixels are read (read-only
 // path, or the tile's staged copy) before any accumulation, so the thread
 // waits for one L2 round trip per quad instead of one per fragment.
-__device__ __forceinline__ void color_quad(const RasterArgs &a, unsigned char *smem,
+template <bool MV>
+__device__ __forceinline__ void color_quad(const RasterArgs &a, const ViewRegsT<MV> &vr, unsigned char *smem,
                                            const ChunkRec &c, bool tiled, uint32_t nvalid,
                                            const uint4 &xy4, const float4 &z4, const uint4 &co4) {
     constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
@@ -387,7 +474,7 @@ __device__ __forceinline__ void color_quad(const RasterArgs &a, unsigned char *s
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int ix = (int)(xy[i] & 0xffffu), iy = (int)(xy[i] >> 16);
-        pix[i] = (uint32_t)(iy * view_w<false>(a) + ix);
+        pix[i] = (uint32_t)(iy * vw<MV>(vr) + ix);
         const int lx = ix - c.x0, ly = iy - c.y0;
         in[i] = tiled && (unsigned)lx < (unsigned)c.tw && (unsigned)ly < (unsigned)c.th;
         l[i] = in[i] ? ly * c.tw + lx : 0;
@@ -395,7 +482,7 @@ __device__ __forceinline__ void color_quad(const RasterArgs &a, unsigned char *s
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         closest[i] = 0u;
-        if ((uint32_t)i < nvalid) closest[i] = in[i] ? sdep[l[i]] : __ldg(view_depth<false>(a) + pix[i]);
+        if ((uint32_t)i < nvalid) closest[i] = in[i] ? sdep[l[i]] : __ldg(vdepth<MV>(vr) + pix[i]);
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -406,7 +493,7 @@ __device__ __forceinline__ void color_quad(const RasterArgs &a, unsigned char *s
             atomicAdd(acc + kPx + l[i], g);
             atomicAdd(acc + 2 * kPx + l[i], b);
         }
-        if (vis && !in[i]) color_global<false>(a, pix[i], r, g, b, 1u);
+        if (vis && !in[i]) color_global<MV>(a, vr, pix[i], r, g, b, 1u);
     }
 }
 
@@ -432,23 +519,23 @@ __device__ __forceinline__ void tile_init(const RasterArgs &a, const ChunkRec &c
 }
 
 template <int PASS, bool MV>
-__device__ __forceinline__ void tile_flush(const RasterArgs &a, const ChunkRec &c,
+__device__ __forceinline__ void tile_flush(const RasterArgs &a, const ViewRegsT<MV> &vr, const ChunkRec &c,
                                            const unsigned char *smem) {
     const int n = c.tw * c.th;
     for (int l = threadIdx.x; l < n; l += kThreads) {
-        const uint32_t pix = (uint32_t)((c.y0 + l / c.tw) * view_w<MV>(a) + c.x0 + l % c.tw);
+        const uint32_t pix = (uint32_t)((c.y0 + l / c.tw) * vw<MV>(vr) + c.x0 + l % c.tw);
         if (is_depth(PASS)) {
             const uint32_t v = reinterpret_cast<const uint32_t *>(smem)[l];
-            if (v) atomicMax(&view_depth<MV>(a)[pix], v);
+            if (v) red_max_u32(&vdepth<MV>(vr)[pix], v);
         } else if (is_color(PASS)) {
             constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
             const uint32_t *acc = reinterpret_cast<const uint32_t *>(smem);
             const uint32_t rc = acc[l];
             const uint32_t cnt = rc >> 20;
-            if (cnt) color_global<MV>(a, pix, rc & 0xfffffu, acc[kPx + l], acc[2 * kPx + l], cnt);
+            if (cnt) color_global<MV>(a, vr, pix, rc & 0xfffffu, acc[kPx + l], acc[2 * kPx + l], cnt);
         } else {
             const unsigned long long k = reinterpret_cast<const unsigned long long *>(smem)[l];
-            if (k) atomicMax(&view_nearest<MV>(a)[pix], k);
+            if (k) red_max_u64(&vnearest<MV>(vr)[pix], k);
         }
     }
 }
@@ -492,70 +579,100 @@ __device__ __forceinline__ uint32_t find_view(const uint32_t *begin, uint32_t nv
 // per-view chunk counts once, finds a chunk's view by binary search and
 // switches frame, camera and file table when the view changes.
 template <int PASS, bool MV>
-__global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
+__device__ __forceinline__ void raster_body(const RasterArgs &a) {
+    constexpr bool kFrag = PASS == PASS_DEPTH_FRAG || PASS == PASS_COLOR_FRAG;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ BatchShared sb;
     __shared__ __align__(16) ChunkRec rec[2];
-    __shared__ __align__(16) uint32_t rec_frags[2][4];
+    __shared__ __align__(16) uint32_t rec_frags[2][4];  // frag count, span offset
     __shared__ uint32_t s_vbegin[MV ? kMaxViews + 1 : 1];
+    __shared__ unsigned long long s_pbegin[MV && kFrag ? kMaxViews + 1 : 1];
     __shared__ uint32_t s_wsum[kThreads / 32];
     if (a.t.redo && *a.t.redo == 0u) return;
     uint32_t nchunks;
+    bool emit = true;  // fragments fit the arena (batched views)
     if (MV) {
-        // Exclusive prefix of the views' chunk counts (at most kMaxViews views).
+        // Exclusive prefixes over the views (at most kMaxViews) of their chunk
+        // counts and, with fragments, of their fragment spans.
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        uint32_t x = threadIdx.x < a.nviews ? a.counters[threadIdx.x * CNT_COUNT + CNT_CHUNKS] : 0u;
+        const uint32_t* vc = a.counters + threadIdx.x * CNT_COUNT;
+        uint32_t x = threadIdx.x < a.nviews ? vc[CNT_CHUNKS] : 0u;
+        unsigned long long y = (kFrag && threadIdx.x < a.nviews) ? vc[CNT_POINTS] : 0ull;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(kFull, x, o);
-            if (lane >= o) x += y;
+            const uint32_t xs = __shfl_up_sync(kFull, x, o);
+            const unsigned long long ys = __shfl_up_sync(kFull, y, o);
+            if (lane >= o) {
+                x += xs;
+                y += ys;
+            }
         }
         if (lane == 31) s_wsum[warp] = x;
+        if (kFrag && lane == 31) s_pbegin[warp] = y;
         __syncthreads();
-        for (int w = 0; w < warp; ++w) x += s_wsum[w];
+        for (int w = 0; w < warp; ++w) {
+            x += s_wsum[w];
+            if (kFrag) y += s_pbegin[w];
+        }
+        __syncthreads();
         s_vbegin[threadIdx.x + 1] = x;
-        if (threadIdx.x == 0) s_vbegin[0] = 0u;
+        if (kFrag) s_pbegin[threadIdx.x + 1] = y;
+        if (threadIdx.x == 0) {
+            s_vbegin[0] = 0u;
+            if (kFrag) s_pbegin[0] = 0ull;
+        }
         __syncthreads();
         nchunks = s_vbegin[a.nviews];
+        if (kFrag) {
+            emit = s_pbegin[a.nviews] <= a.frag_cap;
+            if (PASS == PASS_DEPTH_FRAG && blockIdx.x == 0 && threadIdx.x == 0)
+                *a.frag_overflow = emit ? 0u : 1u;
+        }
     } else {
         nchunks = a.counters[CNT_CHUNKS];
     }
     uint32_t k = blockIdx.x;
     if (k >= nchunks) return;
-    // View of chunk kk and the address of its record.
-    auto locate = [&](uint32_t kk, uint32_t &view) -> const ChunkRec * {
+    // View of chunk kk and the index of its record (also its fragment-count slot).
+    auto locate = [&](uint32_t kk, uint32_t &view) -> uint32_t {
         if (!MV) {
             view = 0u;
-            return a.chunks + kk;
+            return kk;
         }
         view = find_view(s_vbegin, a.nviews, kk);
-        return a.chunks + (size_t)view * a.chunk_stride + (kk - s_vbegin[view]);
+        return view * a.chunk_stride + (kk - s_vbegin[view]);
+    };
+    auto fetch = [&](uint32_t slot, int b) {
+        if (threadIdx.x < 4)
+            cp_async16(reinterpret_cast<uint4 *>(&rec[b]) + threadIdx.x,
+                       reinterpret_cast<const uint4 *>(a.chunks + slot) + threadIdx.x);
+        if (PASS == PASS_COLOR_FRAG && threadIdx.x == 4)
+            cp_async4(&rec_frags[b][0], a.frag_count + slot);
+        if (MV && kFrag && threadIdx.x == 5) cp_async4(&rec_frags[b][1], a.chunk_poff + slot);
     };
     uint32_t cur_view, next_view = 0u, loaded_view = 0xffffffffu;
-    const ChunkRec *src = locate(k, cur_view);
-    if (threadIdx.x < 4)
-        cp_async16(reinterpret_cast<uint4 *>(&rec[0]) + threadIdx.x,
-                   reinterpret_cast<const uint4 *>(src) + threadIdx.x);
-    if (PASS == PASS_COLOR_FRAG && threadIdx.x == 4) cp_async4(&rec_frags[0][0], a.frag_count + k);
+    uint32_t cur_slot = locate(k, cur_view), next_slot = 0u;
+    fetch(cur_slot, 0);
     cp_async_commit();
     if (threadIdx.x == 0) {
         sb.file = 0xffffffffu;
         s_frag_count = 0u;
     }
     int buf = 0;
-    for (; k < nchunks; k += gridDim.x, buf ^= 1, cur_view = next_view) {
+    for (; k < nchunks; k += gridDim.x, buf ^= 1, cur_view = next_view, cur_slot = next_slot) {
         cp_async_wait_all();
         __syncthreads();  // rec[buf] complete; the previous chunk is fully done
         const ChunkRec c = rec[buf];
         const uint32_t nfrag = PASS == PASS_COLOR_FRAG ? rec_frags[buf][0] : 0u;
+        const uint32_t fslot = cur_slot;
+        // First fragment of the chunk: pool index space (one view), or the
+        // view's fragment span in the arena (batched views).
+        const uint32_t fbase =
+            MV ? (kFrag ? (uint32_t)(s_pbegin[cur_view] + rec_frags[buf][1]) : 0u) : c.first;
         const uint32_t kn = k + gridDim.x;
         if (kn < nchunks) {
-            const ChunkRec *nsrc = locate(kn, next_view);
-            if (threadIdx.x < 4)
-                cp_async16(reinterpret_cast<uint4 *>(&rec[buf ^ 1]) + threadIdx.x,
-                           reinterpret_cast<const uint4 *>(nsrc) + threadIdx.x);
-            if (PASS == PASS_COLOR_FRAG && threadIdx.x == 4)
-                cp_async4(&rec_frags[buf ^ 1][0], a.frag_count + kn);
+            next_slot = locate(kn, next_view);
+            fetch(next_slot, buf ^ 1);
         }
         cp_async_commit();
         const uint32_t file_id = MV ? cur_view * a.nfiles + c.file : c.file;
@@ -593,15 +710,23 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
             if (tiled) tile_init<PASS, MV>(a, c, smem);
             __syncthreads();
         }
+        // The view's size and planes: registers (batched views, read once
+        // per chunk) or the kernel's parameters (one view).
+        const ViewRegsT<MV> vr = [&] {
+            if constexpr (MV)
+                return view_regs_mv();
+            else
+                return ViewRegsT<false>(a);
+        }();
         const bool need_med = c.level <= 1, need_high = c.level == 0;
         constexpr bool kNeedColor = PASS == PASS_COLOR || PASS == PASS_DEPTH_FRAG;
         if (PASS == PASS_COLOR_FRAG) {
             // The chunk's fragments, four per thread when 16-byte aligned.
-            if ((c.first & 3u) == 0u) {
+            if ((fbase & 3u) == 0u) {
                 const uint32_t nquads = (nfrag + 3u) >> 2;
                 for (uint32_t q0 = 0; q0 < nquads; q0 += kThreads) {
                     const uint32_t q = q0 + threadIdx.x;
-                    const uint32_t base = c.first + 4u * q;
+                    const uint32_t base = fbase + 4u * q;
                     uint4 xy4 = make_uint4(0, 0, 0, 0), co4 = xy4;
                     float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (q < nquads) {
@@ -610,14 +735,14 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
                         co4 = __ldcs(reinterpret_cast<const uint4 *>(a.frag_col + base));
                     }
                     const uint32_t nv = q < nquads ? min(4u, nfrag - 4u * q) : 0u;
-                    color_quad(a, smem, c, tiled, nv, xy4, z4, co4);
+                    color_quad<MV>(a, vr, smem, c, tiled, nv, xy4, z4, co4);
                 }
             } else {
                 for (uint32_t l0 = 0; l0 < nfrag; l0 += kThreads) {
                     const uint32_t l = l0 + threadIdx.x;
                     const bool v = l < nfrag;
-                    const uint32_t i = c.first + (v ? l : 0u);
-                    do_fragment(a, smem, c, tiled, v, v ? a.frag_xy[i] : 0u, v ? a.frag_z[i] : 0.f,
+                    const uint32_t i = fbase + (v ? l : 0u);
+                    do_fragment<MV>(a, vr, smem, c, tiled, v, v ? a.frag_xy[i] : 0u, v ? a.frag_z[i] : 0.f,
                                 v ? a.frag_col[i] : 0u);
                 }
             }
@@ -639,14 +764,14 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
                         co4 = __ldg(reinterpret_cast<const uint4 *>(a.colors + base));
                 }
                 const uint32_t l0 = 4u * q;
-                do_point<PASS, MV>(a, sb, smem, c, tiled, qv && l0 + 0 < c.count, l0 + 0,
-                               lv4 & 0xffu, lo4.x, me4.x, hi4.x, co4.x);
-                do_point<PASS, MV>(a, sb, smem, c, tiled, qv && l0 + 1 < c.count, l0 + 1,
-                               (lv4 >> 8) & 0xffu, lo4.y, me4.y, hi4.y, co4.y);
-                do_point<PASS, MV>(a, sb, smem, c, tiled, qv && l0 + 2 < c.count, l0 + 2,
-                               (lv4 >> 16) & 0xffu, lo4.z, me4.z, hi4.z, co4.z);
-                do_point<PASS, MV>(a, sb, smem, c, tiled, qv && l0 + 3 < c.count, l0 + 3,
-                               lv4 >> 24, lo4.w, me4.w, hi4.w, co4.w);
+                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 0 < c.count, l0 + 0,
+                               lv4 & 0xffu, lo4.x, me4.x, hi4.x, co4.x, fbase, emit);
+                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 1 < c.count, l0 + 1,
+                               (lv4 >> 8) & 0xffu, lo4.y, me4.y, hi4.y, co4.y, fbase, emit);
+                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 2 < c.count, l0 + 2,
+                               (lv4 >> 16) & 0xffu, lo4.z, me4.z, hi4.z, co4.z, fbase, emit);
+                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 3 < c.count, l0 + 3,
+                               lv4 >> 24, lo4.w, me4.w, hi4.w, co4.w, fbase, emit);
             }
         } else {
             // Unaligned start (pointsPerBatch not a multiple of 4): one point per thread.
@@ -659,14 +784,14 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
                 const uint32_t me = (v && need_med) ? a.med[i] : 0u;
                 const uint32_t hi = (v && need_high) ? a.high[i] : 0u;
                 const uint32_t co = (v && kNeedColor) ? a.colors[i] : 0u;
-                do_point<PASS, MV>(a, sb, smem, c, tiled, v, local, lv, lo, me, hi, co);
+                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, v, local, lv, lo, me, hi, co, fbase, emit);
             }
         }
         if (tiled || PASS == PASS_DEPTH_FRAG) {
             __syncthreads();
-            if (tiled) tile_flush<PASS, MV>(a, c, smem);
+            if (tiled) tile_flush<PASS, MV>(a, vr, c, smem);
             if (PASS == PASS_DEPTH_FRAG && threadIdx.x == 0) {
-                a.frag_count[k] = s_frag_count;
+                a.frag_count[fslot] = s_frag_count;
                 s_frag_count = 0u;
             }
         }
@@ -675,12 +800,53 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
 }
 
 template <int PASS, bool MV>
+__global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
+    raster_body<PASS, MV>(a);
+}
+
+// The colour pass that decodes the points holds a 64 KB screen tile, so at
+// most three CTAs share an SM whatever their registers; saying so lets the
+// compiler use up to 85 registers per thread instead of spilling.
+template <bool MV>
+__global__ void __launch_bounds__(kThreads, 3) raster_kernel_color(RasterArgs a) {
+    raster_body<PASS_COLOR, MV>(a);
+}
+
+// Colour pass of batched views with fragments: the fragments when the depth
+// pass could store them all, else the decode-and-project pass.
+__global__ void __launch_bounds__(kThreads, 3) color_views_kernel(RasterArgs a) {
+    if (*a.frag_overflow)
+        raster_body<PASS_COLOR, true>(a);
+    else
+        raster_body<PASS_COLOR_FRAG, true>(a);
+}
+
+// The kernel a pass launches.
+template <int PASS, bool MV>
+constexpr auto kernel_for() {
+    if constexpr (PASS == PASS_COLOR)
+        return raster_kernel_color<MV>;
+    else
+        return raster_kernel<PASS, MV>;
+}
+
+template <int PASS, bool MV>
 int blocks_per_sm_for() {
     int n = 0;
-    cudaFuncSetAttribute(raster_kernel<PASS, MV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         TileCfg<PASS>::kBytes);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, raster_kernel<PASS, MV>, kThreads,
-                                                      TileCfg<PASS>::kBytes) != cudaSuccess)
+    constexpr auto k = kernel_for<PASS, MV>();
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, TileCfg<PASS>::kBytes);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kThreads, TileCfg<PASS>::kBytes) !=
+        cudaSuccess)
+        n = 1;
+    return n < 1 ? 1 : n;
+}
+
+int color_views_blocks_per_sm() {
+    int n = 0;
+    constexpr int kBytes = TileCfg<PASS_COLOR>::kBytes;
+    cudaFuncSetAttribute(color_views_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBytes);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, color_views_kernel, kThreads, kBytes) !=
+        cudaSuccess)
         n = 1;
     return n < 1 ? 1 : n;
 }
@@ -690,9 +856,14 @@ int raster_blocks_per_sm(int pass) {
     switch (pass) {
     case PASS_DEPTH: return blocks_per_sm_for<PASS_DEPTH, MV>();
     case PASS_COLOR: return blocks_per_sm_for<PASS_COLOR, MV>();
-    case PASS_DEPTH_FRAG: return blocks_per_sm_for<PASS_DEPTH_FRAG, false>();
-    case PASS_COLOR_FRAG: return blocks_per_sm_for<PASS_COLOR_FRAG, false>();
-    default: return blocks_per_sm_for<PASS_NEAREST, MV>();
+    case PASS_DEPTH_FRAG: return blocks_per_sm_for<PASS_DEPTH_FRAG, MV>();
+    case PASS_COLOR_FRAG:
+        return MV ? color_views_blocks_per_sm() : blocks_per_sm_for<PASS_COLOR_FRAG, false>();
+    default:
+        if constexpr (MV)
+            return 1;  // batched views draw HQS only
+        else
+            return blocks_per_sm_for<PASS_NEAREST, false>();
     }
 }
 
@@ -721,12 +892,15 @@ RasterArgs make_args(cr_cloud *cloud, const RasterUniforms &u, const RasterTarge
     a.nviews = 0;
     a.nfiles = 0;
     a.chunk_stride = 0;
+    a.chunk_poff = nullptr;
+    a.frag_cap = 0;
+    a.frag_overflow = nullptr;
     return a;
 }
 
 template <int PASS, bool MV>
 void launch_pass(const RasterArgs &a, int grid, cudaStream_t s) {
-    raster_kernel<PASS, MV><<<grid, kThreads, TileCfg<PASS>::kBytes, s>>>(a);
+    kernel_for<PASS, MV>()<<<grid, kThreads, TileCfg<PASS>::kBytes, s>>>(a);
 }
 
 }  // namespace
@@ -749,7 +923,7 @@ cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &
 }
 
 void raster_prepare_views(cr_context *ctx) {
-    for (int p : {PASS_DEPTH, PASS_COLOR, PASS_NEAREST})
+    for (int p : {PASS_DEPTH, PASS_COLOR, PASS_DEPTH_FRAG, PASS_COLOR_FRAG})
         if (ctx->blocks_per_sm_views[p] == 0) ctx->blocks_per_sm_views[p] = raster_blocks_per_sm<true>(p);
 }
 
@@ -757,9 +931,10 @@ cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUnif
                               const RasterTargets &t, const ViewDesc *views, uint32_t nviews,
                               const cr_raster_file *files, uint32_t nfiles,
                               const ChunkRec *chunks, uint32_t chunk_stride,
-                              uint32_t *counters, cudaStream_t s) {
-    if (pass == PASS_DEPTH_FRAG || pass == PASS_COLOR_FRAG || nviews == 0 || nviews > kMaxViews)
-        return cri::fail(CR_ERR_INTERNAL, "batched views: unsupported pass or view count");
+                              uint32_t *counters, const ViewsFragments *frags, cudaStream_t s) {
+    const bool frag_pass = pass == PASS_DEPTH_FRAG || pass == PASS_COLOR_FRAG;
+    if (nviews == 0 || nviews > kMaxViews || (frag_pass && !frags) || pass == PASS_NEAREST)
+        return cri::fail(CR_ERR_INTERNAL, "batched views: bad pass arguments");
     RasterArgs a = make_args(cloud, u, t);
     a.chunks = chunks;
     a.files = files;
@@ -768,6 +943,15 @@ cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUnif
     a.nviews = nviews;
     a.nfiles = nfiles;
     a.chunk_stride = chunk_stride;
+    if (frags) {
+        a.frag_xy = frags->xy;
+        a.frag_z = frags->z;
+        a.frag_col = frags->col;
+        a.frag_count = frags->count;
+        a.chunk_poff = frags->poff;
+        a.frag_cap = frags->cap;
+        a.frag_overflow = frags->overflow;
+    }
     cr_context *ctx = cloud->ctx;
     if (ctx->blocks_per_sm_views[pass] == 0)
         ctx->blocks_per_sm_views[pass] = raster_blocks_per_sm<true>(pass);
@@ -775,7 +959,10 @@ cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUnif
     switch (pass) {
     case PASS_DEPTH: launch_pass<PASS_DEPTH, true>(a, grid, s); break;
     case PASS_COLOR: launch_pass<PASS_COLOR, true>(a, grid, s); break;
-    default: launch_pass<PASS_NEAREST, true>(a, grid, s); break;
+    case PASS_DEPTH_FRAG: launch_pass<PASS_DEPTH_FRAG, true>(a, grid, s); break;
+    default:  // PASS_COLOR_FRAG
+        color_views_kernel<<<grid, kThreads, TileCfg<PASS_COLOR>::kBytes, s>>>(a);
+        break;
     }
     CR_CUDA(cudaGetLastError());
     return CR_OK;

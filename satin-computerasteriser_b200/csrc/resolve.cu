@@ -114,10 +114,11 @@ __global__ void __launch_bounds__(kThreads)
 // after view (ViewDesc::pix_begin); a thread finds its pixel's view by
 // binary search over the views' begins, staged in shared memory.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void stage_begins(const ViewDesc *views, uint32_t nviews,
-                                             uint32_t total_pix, uint32_t *begin) {
+// Views [0, nviews) of `views` cover pixels [views[0].pix_begin, end).
+__device__ __forceinline__ void stage_begins(const ViewDesc *views, uint32_t nviews, uint32_t end,
+                                             uint32_t *begin) {
     for (uint32_t v = threadIdx.x; v <= nviews; v += kThreads)
-        begin[v] = v < nviews ? views[v].pix_begin : total_pix;
+        begin[v] = v < nviews ? views[v].pix_begin : end;
     __syncthreads();
 }
 
@@ -138,13 +139,13 @@ __device__ __forceinline__ uint32_t view_of_pixel(const uint32_t *begin, uint32_
 // the redo flag; only_if_flag: the accumulators alone, and only if the flag
 // is set.
 __global__ void __launch_bounds__(kThreads)
-    clear_views(const ViewDesc *__restrict__ views, uint32_t nviews, uint32_t total_pix,
-                uint32_t *redo_flag, int only_if_flag) {
+    clear_views(const ViewDesc *__restrict__ views, uint32_t nviews, uint32_t pix0,
+                uint32_t npix, uint32_t *redo_flag, int only_if_flag, int zero_flag) {
     __shared__ uint32_t begin[kMaxViews + 1];
     if (only_if_flag && *redo_flag == 0u) return;
-    stage_begins(views, nviews, total_pix, begin);
-    if (!only_if_flag && blockIdx.x == 0 && threadIdx.x == 0) *redo_flag = 0u;
-    for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < total_pix;
+    stage_begins(views, nviews, pix0 + npix, begin);
+    if (zero_flag && blockIdx.x == 0 && threadIdx.x == 0) *redo_flag = 0u;
+    for (uint32_t p = pix0 + blockIdx.x * kThreads + threadIdx.x; p < pix0 + npix;
          p += gridDim.x * kThreads) {
         const uint32_t v = view_of_pixel(begin, nviews, p);
         const uint32_t q = p - begin[v];
@@ -155,12 +156,13 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void __launch_bounds__(kThreads)
-    resolve_views(const ViewDesc *__restrict__ views, uint32_t nviews, uint32_t total_pix,
-                  ResolveUniforms u, uint32_t *redo_flag, int check, const uint32_t *redo) {
+    resolve_views(const ViewDesc *__restrict__ views, uint32_t nviews, uint32_t pix0,
+                  uint32_t npix, ResolveUniforms u, uint32_t *redo_flag, int check,
+                  const uint32_t *redo) {
     __shared__ uint32_t begin[kMaxViews + 1];
     if (redo && *redo == 0u) return;
-    stage_begins(views, nviews, total_pix, begin);
-    for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < total_pix;
+    stage_begins(views, nviews, pix0 + npix, begin);
+    for (uint32_t p = pix0 + blockIdx.x * kThreads + threadIdx.x; p < pix0 + npix;
          p += gridDim.x * kThreads) {
         const uint32_t v = view_of_pixel(begin, nviews, p);
         const uint32_t q = p - begin[v];
@@ -175,7 +177,7 @@ __global__ void __launch_bounds__(kThreads)
     hole_fill_views(const ViewDesc *__restrict__ views, uint32_t nviews, uint32_t total_pix,
                     int src) {
     __shared__ uint32_t begin[kMaxViews + 1];
-    stage_begins(views, nviews, total_pix, begin);
+    stage_begins(views, nviews, total_pix, begin);  // all views: pix_begin of view 0 is 0
     for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < total_pix;
          p += gridDim.x * kThreads) {
         const uint32_t v = view_of_pixel(begin, nviews, p);
@@ -264,10 +266,10 @@ static uint32_t views_grid(uint32_t total_pix, int sm_count) {
     return std::max<uint32_t>(1u, std::min(need, cap));
 }
 
-cr_status launch_clear_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
-                             uint32_t *redo_flag, int sm_count, cudaStream_t s) {
-    clear_views<<<views_grid(total_pix, sm_count), kThreads, 0, s>>>(views, nviews, total_pix,
-                                                                     redo_flag, 0);
+cr_status launch_clear_views(const ViewDesc *views, uint32_t nviews, uint32_t pix0, uint32_t npix,
+                             uint32_t *redo_flag, bool zero_flag, int sm_count, cudaStream_t s) {
+    clear_views<<<views_grid(npix, sm_count), kThreads, 0, s>>>(views, nviews, pix0, npix,
+                                                                redo_flag, 0, zero_flag ? 1 : 0);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }
@@ -275,18 +277,18 @@ cr_status launch_clear_views(const ViewDesc *views, uint32_t nviews, uint32_t to
 cr_status launch_accum_redo_clear_views(const ViewDesc *views, uint32_t nviews,
                                         uint32_t total_pix, const uint32_t *redo_flag,
                                         int sm_count, cudaStream_t s) {
-    clear_views<<<sm_count * 4, kThreads, 0, s>>>(views, nviews, total_pix,
-                                                  const_cast<uint32_t *>(redo_flag), 1);
+    clear_views<<<sm_count * 4, kThreads, 0, s>>>(views, nviews, 0, total_pix,
+                                                  const_cast<uint32_t *>(redo_flag), 1, 0);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }
 
-cr_status launch_resolve_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
-                               const ResolveUniforms &u, uint32_t *redo_flag, bool check,
-                               const uint32_t *redo, int sm_count, cudaStream_t s) {
-    const uint32_t grid = redo ? (uint32_t)sm_count * 4 : views_grid(total_pix, sm_count);
-    resolve_views<<<grid, kThreads, 0, s>>>(views, nviews, total_pix, u, redo_flag, check ? 1 : 0,
-                                           redo);
+cr_status launch_resolve_views(const ViewDesc *views, uint32_t nviews, uint32_t pix0,
+                               uint32_t npix, const ResolveUniforms &u, uint32_t *redo_flag,
+                               bool check, const uint32_t *redo, int sm_count, cudaStream_t s) {
+    const uint32_t grid = redo ? (uint32_t)sm_count * 4 : views_grid(npix, sm_count);
+    resolve_views<<<grid, kThreads, 0, s>>>(views, nviews, pix0, npix, u, redo_flag,
+                                           check ? 1 : 0, redo);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

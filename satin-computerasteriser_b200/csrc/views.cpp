@@ -4,24 +4,28 @@
 // The reference draws one viewport per ComputeRasteriser.encode
 // (ComputeRasteriser.swift:277-296, 322-456).  cr_render_multiview draws
 // up to kMaxViews views, each into its own cr_frame, with the same passes in
-// a few launches shared by all views:
-//   clear_views           every view's depth plane and accumulators
-//   cull_*_views          per cloud: blockIdx.y = view, ordered survivor and
-//                         chunk lists per view (fixed strides)
-//   raster_kernel<*, MV>  per cloud and pass: one persistent grid over the
-//                         chunks of all views, each chunk drawn into its view
-//   resolve_views         every view's pixels (+ the exact re-run gate)
-//   hole_fill_views       per iteration
-// The sequence is captured once into a CUDA graph and replayed: the views'
-// cameras, cull arguments and file tables travel in one pinned staging block
-// copied by the graph's first node.  Two staging blocks and two graph
-// executables alternate, so the host fills one while the other may still be
-// copied.  Every view uses the per-view path's arithmetic (the same file
-// table products, cull, passes and integer atomics), so its images are
-// bit-identical to a cr_render of that view alone.
+// launches shared by many views:
+//   cull_*_views          per cloud, all views: blockIdx.y = view, ordered
+//                         survivor and chunk lists per view (fixed strides)
+//   then per group of consecutive views (ctx->view_group_pixels pixels):
+//   clear_views           the group's depth planes and accumulators
+//   raster_kernel<*, MV>  per cloud, depth then colour: one persistent grid
+//                         over the chunks of the group's views
+//   resolve_views         the group's pixels (+ the exact re-run's check)
+//   hole_fill_views       all views, per iteration
+// A group's planes and fragments stay in L2 from its clear to its resolve,
+// as they do for one view at a time.  The sequence is captured once into a
+// CUDA graph and replayed: the views' cameras, cull arguments and file
+// tables travel in one pinned staging block copied by the graph's first
+// node.  Two staging blocks and two graph executables alternate, so the
+// host fills one while the other may still be copied.  Every view uses the
+// per-view path's arithmetic (the same file table products, cull, passes
+// and integer atomics), so its images are bit-identical to a cr_render of
+// that view alone.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -71,10 +75,16 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // Per-cloud cull scratch and outputs for all views.
 struct ViewsCloud {
     CullRec *tmp = nullptr;               // nviews * nslots
-    uint32_t *cta = nullptr;              // nviews * 2 * ctas
+    uint32_t *cta = nullptr;              // nviews * kCullCtaWords * ctas
     cr_visible_batch *visible = nullptr;  // nviews * nslots
     ChunkRec *chunks = nullptr;           // nviews * chunk_stride
     uint32_t *counters = nullptr;         // nviews * CNT_COUNT
+    uint32_t *chunk_poff = nullptr;       // nviews * chunk_stride
+    uint32_t *frag_count = nullptr;       // nviews * chunk_stride
+    uint32_t *frag_xy = nullptr, *frag_col = nullptr;  // frag_cap each
+    float *frag_z = nullptr;
+    uint32_t *frag_overflow = nullptr;
+    unsigned long long frag_cap = 0;
     uint32_t nslots = 0, ctas = 0, nfiles = 0;
     uint64_t chunk_stride = 0;
     size_t args_off = 0, files_off = 0;  // in the staging block
@@ -87,7 +97,13 @@ struct ViewsState {
     std::vector<unsigned char> key;
     uint32_t nviews = 0, total_pix = 0;
     bool packed = false;
+    bool frags = false;  // fragment passes (single-pixel footprints)
     int hole_fill = 0;
+    struct Group {
+        uint32_t v0, nv;      // views [v0, v0 + nv)
+        uint32_t pix0, npix;  // their pixels
+    };
+    std::vector<Group> groups;
     std::vector<ViewsCloud> clouds;
     unsigned char *d_stage = nullptr;  // ViewDesc[nviews] | per cloud: CullArgs[nviews], files
     unsigned char *h_stage[2] = {nullptr, nullptr};
@@ -119,6 +135,12 @@ void views_free(ViewsState *s) {
         dfree(c.visible);
         dfree(c.chunks);
         dfree(c.counters);
+        dfree(c.chunk_poff);
+        dfree(c.frag_count);
+        dfree(c.frag_xy);
+        dfree(c.frag_z);
+        dfree(c.frag_col);
+        dfree(c.frag_overflow);
     }
     s->clouds.clear();
     dfree(s->d_stage);
@@ -176,6 +198,7 @@ std::vector<unsigned char> make_key(cr_context *ctx, cr_frame *const *frames, ui
     put(k, *cfg);  // every field is 4 bytes: no padding
     put(k, ctx->chunk_points);
     put(k, ctx->use_tiles);
+    put(k, ctx->view_group_pixels);
     put(k, packed);
     return k;
 }
@@ -208,14 +231,48 @@ RasterUniforms raster_uniforms(const cr_config *cfg) {
     return u;
 }
 
-// Allocates the per-view buffers for this frame set and cloud set.
+// Fragment span of a full batch (its chunks rounded up to multiples of 4).
+uint64_t batch_fragment_span(uint32_t ppb, uint32_t cp) {
+    const uint64_t nc = (ppb + cp - 1) / cp;
+    return nc == 0 ? 0 : (nc - 1) * ((cp + 3) & ~3u) + ((ppb - (nc - 1) * cp + 3) & ~3ull);
+}
+
+// Allocates the per-view buffers for this frame set and cloud set.  The
+// depth and colour passes run over groups of consecutive views of at most
+// ctx->view_group_pixels pixels (0: one group), so that a group's fragments
+// are still in L2 when its colour pass reads them.  With single-pixel
+// footprints each cloud gets one fragment arena reused by every group: the
+// largest group's worst case (every slot's full batch surviving in each of
+// its views), within an eighth of the free device memory shared by the
+// clouds; a group whose spans exceed it draws its colour pass from the
+// points instead.
 cr_status views_alloc(cr_context *ctx, ViewsState *s, cr_frame *const *frames, uint32_t nviews,
-                      cr_cloud *const *clouds, uint32_t nclouds) {
+                      cr_cloud *const *clouds, uint32_t nclouds, bool frags) {
     s->nviews = nviews;
     uint64_t pix = 0;
     for (uint32_t v = 0; v < nviews; ++v) pix += (uint64_t)frames[v]->width * frames[v]->height;
     if (pix >= (1ull << 31)) return fail(CR_ERR_CAPACITY, "views exceed 2^31 pixels in all");
     s->total_pix = (uint32_t)pix;
+    s->groups.clear();
+    uint32_t largest = 0;
+    {
+        const uint64_t budget = ctx->view_group_pixels > 0 ? (uint64_t)ctx->view_group_pixels : pix;
+        uint32_t first = 0, pix0 = 0;
+        uint64_t acc = 0;
+        for (uint32_t v = 0; v < nviews; ++v) {
+            const uint64_t p = (uint64_t)frames[v]->width * frames[v]->height;
+            if (v > first && acc + p > budget) {
+                s->groups.push_back({first, v - first, pix0, (uint32_t)acc});
+                largest = std::max(largest, v - first);
+                first = v;
+                pix0 += (uint32_t)acc;
+                acc = 0;
+            }
+            acc += p;
+        }
+        s->groups.push_back({first, nviews - first, pix0, (uint32_t)acc});
+        largest = std::max(largest, nviews - first);
+    }
     size_t off = align256(sizeof(ViewDesc) * nviews);
     s->clouds.resize(nclouds);
     const uint32_t cp = (uint32_t)std::max(ctx->chunk_points, kMinChunkPoints);
@@ -229,12 +286,28 @@ cr_status views_alloc(cr_context *ctx, ViewsState *s, cr_frame *const *frames, u
         vc.chunk_stride = chunk_capacity(c->cap, (int)cp);
         const size_t n = (size_t)nviews * std::max(vc.nslots, 1u);
         if ((st = dalloc(&vc.tmp, n * sizeof(CullRec))) ||
-            (st = dalloc(&vc.cta, (size_t)nviews * 2 * std::max(vc.ctas, 1u) * 4)) ||
+            (st = dalloc(&vc.cta, (size_t)nviews * kCullCtaWords * std::max(vc.ctas, 1u) * 4)) ||
             (st = dalloc(&vc.visible, n * sizeof(cr_visible_batch))) ||
             (st = dalloc(&vc.chunks, (size_t)nviews * vc.chunk_stride * sizeof(ChunkRec))) ||
             (st = dalloc(&vc.counters, (size_t)nviews * CNT_COUNT * 4)))
             return st;
         CR_CUDA(cudaMemsetAsync(vc.counters, 0, (size_t)nviews * CNT_COUNT * 4, ctx->stream));
+        if (frags) {
+            size_t free_b = 0, total_b = 0;
+            CR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            const unsigned long long need =
+                (unsigned long long)largest * vc.nslots * batch_fragment_span(c->cap.pointsPerBatch, cp);
+            const unsigned long long budget = free_b / 8 / std::max(nclouds, 1u) / 12;
+            vc.frag_cap = std::min<unsigned long long>({need, budget, 0xfffffff0ull});
+            const size_t slots = (size_t)nviews * vc.chunk_stride;
+            if ((st = dalloc(&vc.chunk_poff, slots * 4)) || (st = dalloc(&vc.frag_count, slots * 4)) ||
+                (st = dalloc(&vc.frag_xy, vc.frag_cap * 4)) ||
+                (st = dalloc(&vc.frag_z, vc.frag_cap * 4)) ||
+                (st = dalloc(&vc.frag_col, vc.frag_cap * 4)) ||
+                (st = dalloc(&vc.frag_overflow, 16)))
+                return st;
+            CR_CUDA(cudaMemsetAsync(vc.frag_overflow, 0, 16, ctx->stream));
+        }
         vc.args_off = off;
         off = align256(off + sizeof(CullArgs) * nviews);
         vc.files_off = off;
@@ -257,8 +330,6 @@ cr_status views_enqueue(cr_context *ctx, ViewsState *s, int b, cr_cloud *const *
     const ViewDesc *views = reinterpret_cast<const ViewDesc *>(s->d_stage);
     cr_status e;
     CR_CUDA(cudaMemcpyAsync(s->d_stage, s->h_stage[b], s->stage_bytes, cudaMemcpyHostToDevice, st));
-    if ((e = launch_clear_views(views, s->nviews, s->total_pix, s->d_redo, ctx->sm_count, st)))
-        return e;
     for (uint32_t i = 0; i < nclouds; ++i) {
         const ViewsCloud &vc = s->clouds[i];
         if (vc.nslots == 0) continue;
@@ -268,25 +339,48 @@ cr_status views_enqueue(cr_context *ctx, ViewsState *s, int b, cr_cloud *const *
     const RasterUniforms u = raster_uniforms(cfg);
     RasterTargets t{nullptr, nullptr, nullptr};
     t.packed = s->packed ? 1 : 0;
-    auto pass = [&](RasterPass p, const RasterTargets &tt) -> cr_status {
+    // Pass p of every cloud over views [v0, v0 + nv).
+    auto pass = [&](RasterPass p, const RasterTargets &tt, uint32_t v0, uint32_t nv) -> cr_status {
         for (uint32_t i = 0; i < nclouds; ++i) {
             const ViewsCloud &vc = s->clouds[i];
             if (vc.nslots == 0) continue;
             const cr_raster_file *files =
-                reinterpret_cast<const cr_raster_file *>(s->d_stage + vc.files_off);
-            cr_status r = launch_raster_views(clouds[i], p, u, tt, views, s->nviews, files,
-                                              vc.nfiles, vc.chunks, (uint32_t)vc.chunk_stride,
-                                              vc.counters, st);
+                reinterpret_cast<const cr_raster_file *>(s->d_stage + vc.files_off) +
+                (size_t)v0 * vc.nfiles;
+            const size_t slot0 = (size_t)v0 * vc.chunk_stride;
+            const ViewsFragments fr{vc.frag_xy,
+                                    vc.frag_z,
+                                    vc.frag_col,
+                                    vc.frag_count ? vc.frag_count + slot0 : nullptr,
+                                    vc.chunk_poff ? vc.chunk_poff + slot0 : nullptr,
+                                    vc.frag_cap,
+                                    vc.frag_overflow};
+            const bool fp = p == PASS_DEPTH_FRAG || p == PASS_COLOR_FRAG;
+            cr_status r = launch_raster_views(clouds[i], p, u, tt, views + v0, nv, files,
+                                              vc.nfiles, vc.chunks + slot0,
+                                              (uint32_t)vc.chunk_stride,
+                                              vc.counters + (size_t)v0 * CNT_COUNT,
+                                              fp ? &fr : nullptr, st);
             if (r) return r;
         }
         return CR_OK;
     };
-    if ((e = pass(PASS_DEPTH, t)) || (e = pass(PASS_COLOR, t))) return e;
     ResolveUniforms ru{0, 0, {cfg->backgroundColor[0], cfg->backgroundColor[1],
                               cfg->backgroundColor[2], cfg->backgroundColor[3]}};
-    if ((e = launch_resolve_views(views, s->nviews, s->total_pix, ru, s->d_redo, s->packed,
-                                  nullptr, ctx->sm_count, st)))
-        return e;
+    // Group after group: clear, depth, colour, resolve, so that the group's
+    // planes (and, with single-pixel footprints, the fragments the depth
+    // pass keeps for the colour pass, through one arena) stay in L2.
+    const RasterPass depth_pass = s->frags ? PASS_DEPTH_FRAG : PASS_DEPTH;
+    const RasterPass color_pass = s->frags ? PASS_COLOR_FRAG : PASS_COLOR;
+    for (size_t gi = 0; gi < s->groups.size(); ++gi) {
+        const ViewsState::Group &g = s->groups[gi];
+        if ((e = launch_clear_views(views + g.v0, g.nv, g.pix0, g.npix, s->d_redo, gi == 0,
+                                    ctx->sm_count, st)) ||
+            (e = pass(depth_pass, t, g.v0, g.nv)) || (e = pass(color_pass, t, g.v0, g.nv)) ||
+            (e = launch_resolve_views(views + g.v0, g.nv, g.pix0, g.npix, ru, s->d_redo,
+                                      s->packed, nullptr, ctx->sm_count, st)))
+            return e;
+    }
     if (s->packed) {
         // Exact re-run, gated on the resolve's flag (as cr_render).
         RasterTargets tx = t;
@@ -294,8 +388,9 @@ cr_status views_enqueue(cr_context *ctx, ViewsState *s, int b, cr_cloud *const *
         tx.redo = s->d_redo;
         if ((e = launch_accum_redo_clear_views(views, s->nviews, s->total_pix, s->d_redo,
                                                ctx->sm_count, st)) ||
-            (e = pass(PASS_COLOR, tx)) ||
-            (e = launch_resolve_views(views, s->nviews, s->total_pix, ru, s->d_redo, false,
+            // The arena holds the last group's fragments only: decode.
+            (e = pass(PASS_COLOR, tx, 0, s->nviews)) ||
+            (e = launch_resolve_views(views, s->nviews, 0, s->total_pix, ru, s->d_redo, false,
                                       s->d_redo, ctx->sm_count, st)))
             return e;
     }
@@ -378,12 +473,13 @@ void views_fill(ViewsState *s, int b, cr_frame *const *frames, const cr_camera *
             a.files = d_files + (size_t)v * vc.nfiles;
             a.nfiles = vc.nfiles;
             a.tmp = vc.tmp + (size_t)v * vc.nslots;
-            a.cta_counts = vc.cta + (size_t)v * 2 * vc.ctas;
+            a.cta_counts = vc.cta + (size_t)v * kCullCtaWords * vc.ctas;
             a.chunk_points = chunk_points;
             a.u = cull_uniforms(cfg, &cams[v], frames[v]->width, frames[v]->height);
             a.visible = vc.visible + (size_t)v * vc.nslots;
             a.chunks = vc.chunks + (size_t)v * vc.chunk_stride;
             a.counters = vc.counters + (size_t)v * CNT_COUNT;
+            a.chunk_poff = vc.chunk_poff ? vc.chunk_poff + (size_t)v * vc.chunk_stride : nullptr;
         }
     }
 }
@@ -446,8 +542,10 @@ CR_API cr_status cr_render_multiview(cr_context *ctx, cr_frame *const *frames,
         } else {
             s = ctx->views = new ViewsState();
         }
-        cr_status st = views_alloc(ctx, s, frames, nviews, resident.data(), nres);
+        const bool frags = std::fmax(cfg->minimumPointSize, cfg->maximumPointSize) <= 1.0f;
+        cr_status st = views_alloc(ctx, s, frames, nviews, resident.data(), nres, frags);
         if (!st) {
+            s->frags = frags;
             s->packed = packed;
             s->hole_fill = std::max(cfg->holeFillIterations, 0);
             st = views_build_graphs(ctx, s, resident.data(), nres, cfg);
@@ -510,21 +608,31 @@ CR_API cr_status cr_autotune_multiview(cr_context *ctx, cr_frame *const *frames,
         while (std::getline(in, line)) {
             if (line.find(tag) == std::string::npos) continue;
             const size_t a = line.find("\"chunkPoints\": "), t = line.find("\"useTiles\": "),
-                         m = line.find("\"ms\": ");
-            if (a == std::string::npos || t == std::string::npos) continue;
+                         gp = line.find("\"viewGroupPixels\": "), m = line.find("\"ms\": ");
+            if (a == std::string::npos || t == std::string::npos || gp == std::string::npos)
+                continue;
             const int cpn = std::atoi(line.c_str() + a + 15);
             const int tiles = std::atoi(line.c_str() + t + 12);
-            if (cpn < kMinChunkPoints || cpn > 65536 || (tiles != 0 && tiles != 1)) continue;
+            const int group = std::atoi(line.c_str() + gp + 19);
+            if (cpn < kMinChunkPoints || cpn > 65536 || (tiles != 0 && tiles != 1) || group < 0)
+                continue;
             ctx->chunk_points = cpn;
             ctx->use_tiles = tiles != 0;
-            if (best_out) *best_out = cr_tuning{cpn, tiles};
+            ctx->view_group_pixels = group;
+            if (best_out) *best_out = cr_tuning{cpn, tiles, group};
             if (best_ms_out)
                 *best_ms_out = m == std::string::npos ? 0.0f : (float)std::atof(line.c_str() + m + 6);
             return CR_OK;
         }
     }
-    const int candidates[][2] = {{512, 1}, {1024, 1}, {2048, 1}, {4096, 1},
-                                 {512, 0}, {1024, 0}, {2048, 0}, {4096, 0}};
+    // {chunkPoints, useTiles, viewGroupPixels}
+    const int candidates[][3] = {
+        {1024, 1, 1048576}, {2048, 1, 1048576}, {4096, 1, 1048576},
+        {1024, 1, 2097152}, {2048, 1, 2097152}, {4096, 1, 2097152},
+        {1024, 1, 4194304}, {2048, 1, 4194304}, {4096, 1, 4194304},
+        {1024, 1, 8388608}, {2048, 1, 8388608}, {4096, 1, 8388608},
+        {2048, 1, 0},       {2048, 0, 2097152}, {2048, 0, 4194304}};
+    constexpr int kCandidates = (int)(sizeof(candidates) / sizeof(candidates[0]));
     cudaEvent_t e0, e1;
     CR_CUDA(cudaEventCreate(&e0));
     CR_CUDA(cudaEventCreate(&e1));
@@ -532,9 +640,10 @@ CR_API cr_status cr_autotune_multiview(cr_context *ctx, cr_frame *const *frames,
     float best_ms = 0.0f;
     int best = -1;
     cr_status st = CR_OK;
-    for (int ci = 0; ci < 8 && !st; ++ci) {
+    for (int ci = 0; ci < kCandidates && !st; ++ci) {
         ctx->chunk_points = candidates[ci][0];
         ctx->use_tiles = candidates[ci][1] != 0;
+        ctx->view_group_pixels = candidates[ci][2];
         for (int w = 0; w < 2 && !st; ++w)
             st = cr_render_multiview(ctx, frames, cams, nviews, clouds, models, nclouds, cfg);
         if (st) break;
@@ -548,7 +657,8 @@ CR_API cr_status cr_autotune_multiview(cr_context *ctx, cr_frame *const *frames,
         cudaEventElapsedTime(&ms, e0, e1);
         ms /= (float)reps;
         results << (ci ? ", " : "") << "{\"chunkPoints\": " << candidates[ci][0]
-                << ", \"useTiles\": " << candidates[ci][1] << ", \"ms\": " << ms << "}";
+                << ", \"useTiles\": " << candidates[ci][1] << ", \"viewGroupPixels\": "
+                << candidates[ci][2] << ", \"ms\": " << ms << "}";
         if (best < 0 || ms < best_ms) {
             best = ci;
             best_ms = ms;
@@ -559,13 +669,15 @@ CR_API cr_status cr_autotune_multiview(cr_context *ctx, cr_frame *const *frames,
     if (st) return st;
     ctx->chunk_points = candidates[best][0];
     ctx->use_tiles = candidates[best][1] != 0;
-    if (best_out) *best_out = cr_tuning{candidates[best][0], candidates[best][1]};
+    ctx->view_group_pixels = candidates[best][2];
+    if (best_out) *best_out = cr_tuning{candidates[best][0], candidates[best][1], candidates[best][2]};
     if (best_ms_out) *best_ms_out = best_ms;
     if (cache_path) {
         std::ofstream out(cache_path, std::ios::app);
         if (!out) return fail(CR_ERR_INVALID_ARGUMENT, "cannot write the autotune cache file");
         out << "{" << tag << ", \"chunkPoints\": " << candidates[best][0]
-            << ", \"useTiles\": " << candidates[best][1] << ", \"ms\": " << best_ms
+            << ", \"useTiles\": " << candidates[best][1] << ", \"viewGroupPixels\": "
+            << candidates[best][2] << ", \"ms\": " << best_ms
             << ", \"candidates\": [" << results.str() << "]}\n";
     }
     return CR_OK;

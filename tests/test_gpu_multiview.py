@@ -131,18 +131,38 @@ def test_autotune_sets_and_caches_the_launch_shape(cr, orc, ctx, tmp_path):
     path = os.path.join(tmp_path, "tune.jsonl")
     try:
         best = mv.autotune(cams, cachePath=path, reps=2)
-        assert best["chunkPoints"] in (512, 1024, 2048, 4096)
+        assert best["chunkPoints"] in (1024, 2048, 4096)
+        assert best["viewGroupPixels"] in (0, 1048576, 2097152, 4194304, 8388608)
         assert ctx.tuning()["chunkPoints"] == best["chunkPoints"]
         lines = open(path).read().splitlines()
         assert len(lines) == 1 and '"candidates"' in lines[0]
         again = mv.autotune(cams, cachePath=path, reps=2)
         assert again["chunkPoints"] == best["chunkPoints"]
         assert again["useTiles"] == best["useTiles"]
+        assert again["viewGroupPixels"] == best["viewGroupPixels"]
         assert len(open(path).read().splitlines()) == 1  # read, not re-timed
         mv.render(cams)
         assert_views_match(cr, ctx, mv, [cloud], mv.configuration, cams, SIZES[:3])
     finally:
-        ctx.set_tuning(chunkPoints=2048, useTiles=True)
+        ctx.set_tuning(chunkPoints=2048, useTiles=True, viewGroupPixels=4194304)
+
+
+@pytest.mark.parametrize("group_pixels", [1, 40000, 0])
+def test_view_groups_do_not_change_results(cr, orc, ctx, group_pixels):
+    """Depth and colour passes over groups of views (one view per group, a
+    few views per group, all views in one group) share one fragment arena;
+    every grouping gives the per-view images."""
+    pos, rgba = blob_cloud(50000, 13)
+    cloud = make_cloud(cr, orc, ctx, pos, rgba)
+    try:
+        ctx.set_tuning(viewGroupPixels=group_pixels)
+        mv = cr.MultiViewRasteriser(ctx, SIZES)
+        mv.addPointCloud(cloud)
+        cams = cameras(cr, SIZES, 17)
+        mv.render(cams)
+        assert_views_match(cr, ctx, mv, [cloud], mv.configuration, cams, SIZES)
+    finally:
+        ctx.set_tuning(viewGroupPixels=4194304)
 
 
 def test_batched_views_reject_bad_arguments(cr, orc, ctx):
