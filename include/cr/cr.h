@@ -446,6 +446,45 @@ CR_API cr_status cr_synth_lattice_points(cr_context *ctx, uint64_t seed, uint32_
                                          float hi, float jitter, void *device_records);
 
 /* ------------------------------------------------------------------------ */
+/* Differentiable colours                                                    */
+/* ------------------------------------------------------------------------ */
+/* An FP32 variant of the HQS colour pass with learnable per-point colours,
+ * beside the unchanged integer path, and its adjoint (no counterpart in the
+ * reference).  All arrays are device memory: colors and dL_dcolors hold 3
+ * floats (R, G, B) per pool point of the cloud (cr_cloud_info.capacity
+ * maxResidentBatches * pointsPerBatch), image and dL_dimage 3 floats per
+ * pixel, row 0 at the top.  The cloud's file table must hold the camera's
+ * transforms (cr_cloud_update_files), as for cr_render.
+ *
+ * cr_hqs_forward_f32: depth pass, then for every sample that passes the
+ * colour pass's depth test (the integer path's visible set) the point's
+ * colour is added to the pixel's FP32 R, G, B sums (reductions flush
+ * subnormals) and one to its 32-bit count; image = sums / count, or the
+ * background where the count is 0.  No hole fill.  One cloud.
+ *
+ * cr_hqs_backward_colors: for every point, recomputes its visible pixels
+ * from the depth plane and counts the forward left in the frame and adds
+ * sum over them of dL_dimage[pixel] / count[pixel] to dL_dcolors[point]
+ * (per channel).  Call it after cr_hqs_forward_f32 with the same frame,
+ * cloud, configuration and camera, before any other render of that cloud
+ * or frame; gradients of several views accumulate.  One thread per point,
+ * no atomics.
+ *
+ * cr_l2_loss: dL_dimage[i] = 2 * scale * (image[i] - target[i]) for n
+ * floats; with loss non-NULL (host), *loss = scale * sum (image - target)^2,
+ * accumulated in FP64, and the call synchronises.
+ *
+ * Asynchronous on the context's stream unless stated. */
+CR_API cr_status cr_hqs_forward_f32(cr_context *ctx, cr_frame *frame, cr_cloud *cloud,
+                                    const cr_config *config, const cr_camera *camera,
+                                    const float *colors, float *image);
+CR_API cr_status cr_hqs_backward_colors(cr_context *ctx, cr_frame *frame, cr_cloud *cloud,
+                                        const cr_config *config, const cr_camera *camera,
+                                        const float *dL_dimage, float *dL_dcolors);
+CR_API cr_status cr_l2_loss(cr_context *ctx, const float *image, const float *target, uint64_t n,
+                            float scale, float *dL_dimage, double *loss);
+
+/* ------------------------------------------------------------------------ */
 /* Batched views                                                             */
 /* ------------------------------------------------------------------------ */
 /* No counterpart in the reference, whose renderer draws one viewport per

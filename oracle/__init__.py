@@ -102,6 +102,10 @@ def _load():
     lib.orc_render.argtypes = [C.POINTER(orc_cloud), C.c_uint32, C.POINTER(orc_config), P, P,
                                C.c_int, C.c_int, P, P, P, P, P, P, P, C.c_uint32, P, C.c_int]
     lib.orc_hole_fill.argtypes = [P, C.c_int, C.c_int, C.c_int]
+    lib.orc_hqs_grad_f64.restype = C.c_int
+    lib.orc_hqs_grad_f64.argtypes = [C.POINTER(orc_cloud), C.POINTER(orc_config), P, P,
+                                     C.c_int, C.c_int, P, P, C.c_double, P, P, P, P,
+                                     C.c_uint32, C.c_double, P, C.c_int]
     lib.orc_nearest_cpu_reference.argtypes = [C.POINTER(orc_cloud), C.c_int, C.c_int, P, P,
                                               C.c_int, P, P]
     lib.orc_pick_scan.restype = C.c_int
@@ -346,6 +350,35 @@ def render(clouds, cfg: Config, view, proj, width: int, height: int, threads: in
     return Frame(rgba.reshape(height, width, 4), depthf.reshape(height, width),
                  depth.reshape(height, width), accum.reshape(height, width, 4),
                  nd.reshape(height, width), ni.reshape(height, width), visible, rc)
+
+
+def hqs_grad_f64(cloud: Cloud, cfg: Config, view, proj, width: int, height: int, colors,
+                 target, scale: float, grad=None, fd_points=None, fd_h: float = 1e-3,
+                 fd=None, threads: int = 1) -> dict:
+    """Differentiable HQS colours in FP64 for one view (orc_hqs_grad_f64):
+    colours (pool points x 3) and target (height x width x 3) in float64.
+    Returns the image, the loss, and grad / fd, which accumulate into the
+    arrays given (several views)."""
+    cc = cloud.to_c()
+    c = cfg.to_c()
+    v, p = _mat(view), _mat(proj)
+    colors = np.ascontiguousarray(colors, np.float64)
+    target = np.ascontiguousarray(target, np.float64)
+    image = np.zeros((height, width, 3), np.float64)
+    loss = np.zeros(1, np.float64)
+    if grad is None:
+        grad = np.zeros_like(colors)
+    pts = None if fd_points is None else np.ascontiguousarray(fd_points, np.uint32)
+    n_fd = 0 if pts is None else len(pts)
+    if n_fd and fd is None:
+        fd = np.zeros((n_fd, 3), np.float64)
+    rc = _load().orc_hqs_grad_f64(C.byref(cc), C.byref(c), _ptr(v), _ptr(p), width, height,
+                                  _ptr(colors), _ptr(target), float(scale), _ptr(image),
+                                  _ptr(loss), _ptr(grad), _ptr(pts), n_fd, float(fd_h),
+                                  _ptr(fd) if n_fd else None, threads)
+    if rc:
+        raise RuntimeError(f"orc_hqs_grad_f64 failed ({rc})")
+    return {"image": image, "loss": float(loss[0]), "grad": grad, "fd": fd}
 
 
 def hole_fill(rgba: np.ndarray, iterations: int) -> np.ndarray:

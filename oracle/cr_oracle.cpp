@@ -658,6 +658,119 @@ int orc_render(const orc_cloud *clouds, uint32_t nclouds, const orc_config *cfg,
     return 0;
 }
 
+// Differentiable HQS colours in FP64 (reference for the FP32 path).  One
+// view of one cloud: the HQS depth pass, then per-pixel FP64 sums of the
+// learnable colours of the points that pass the colour pass's depth test
+// (ColorPass/Shaders.metal:201-214, the same visible set as the integer
+// path) and their count; image = sum / count (background where count = 0);
+// loss = scale * sum over pixels and channels of (image - target)^2.
+// Gradient: dL/dcolor_i = sum over the pixels p where point i is visible of
+// 2 * scale * (image_p - target_p) / count_p.  Central differences: for
+// each listed point and channel, the loss at colour +- h, evaluated over
+// the loss terms that the point's colour changes (the pixels where it is
+// visible), divided by 2h.  Multi-threaded over visible batches with
+// per-thread planes; deterministic (per-thread planes are summed in order).
+// grad and fd are added to (several views accumulate).
+int orc_hqs_grad_f64(const orc_cloud *cloud, const orc_config *cfg, const float view[16],
+                     const float proj[16], int w, int h, const double *colors,
+                     const double *target, double scale, double *image, double *loss,
+                     double *grad, const uint32_t *fd_points, uint32_t n_fd, double fd_h,
+                     double *fd, int threads) {
+    if (w <= 0 || h <= 0) return 1;
+    const size_t npix = (size_t)w * h;
+    const orc_cloud &c = *cloud;
+    std::vector<orc_visible> vis(c.batchCount);
+    const uint32_t nvis = orc_cull(&c, cfg, view, proj, w, h, vis.data(), c.batchCount);
+    std::vector<uint32_t> depth(npix, 0u);
+    pass_args a{&c, vis.data(), nvis, cfg, view, proj, w, h, depth.data(), nullptr, nullptr};
+    run_pass(a, PASS_DEPTH, threads);
+    const float keep = 1.0f - cfg->depthTolerance;
+    // Calls f(pointIndex, pixel) for every (point, footprint pixel) that the
+    // colour pass accumulates, batches [v0, v1).
+    auto visit = [&](uint32_t v0, uint32_t v1, auto &&f) {
+        for (uint32_t v = v0; v < v1; ++v) {
+            const orc_visible &vb = vis[v];
+            const orc_batch &b = c.batches[vb.batchIndex];
+            const orc_file &file = c.files[b.fileIndex];
+            for (uint32_t local = 0; local < vb.activePoints; ++local) {
+                const uint32_t pi = b.firstPoint + local;
+                projected pr;
+                if (!project(c, b, file, vb, pi, *cfg, view, proj, w, h, false, pr)) continue;
+                const int rad = pr.radius;
+                for (int oy = -rad; oy <= rad; ++oy)
+                    for (int ox = -rad; ox <= rad; ++ox) {
+                        if (!inside_footprint(ox, oy, rad)) continue;
+                        const int tx = pr.px + ox, ty = pr.py + oy;
+                        if (tx < 0 || tx >= w || ty < 0 || ty >= h) continue;
+                        const uint32_t pix = (uint32_t)(ty * w + tx);
+                        const uint32_t closest = depth[pix];
+                        if (closest == 0u) continue;
+                        if (!(pr.ndcz >= uint_to_depth(closest) * keep)) continue;
+                        f(pi, pix);
+                    }
+            }
+        }
+    };
+    const int nt = std::max(1, std::min(threads, (int)std::max(nvis, 1u)));
+    std::vector<std::vector<double>> sums(nt, std::vector<double>(npix * 3, 0.0));
+    std::vector<std::vector<uint32_t>> counts(nt, std::vector<uint32_t>(npix, 0u));
+    {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back([&, t]() {
+                const uint32_t v0 = (uint32_t)((uint64_t)nvis * t / nt);
+                const uint32_t v1 = (uint32_t)((uint64_t)nvis * (t + 1) / nt);
+                visit(v0, v1, [&](uint32_t pi, uint32_t pix) {
+                    for (int ch = 0; ch < 3; ++ch) sums[t][pix * 3 + ch] += colors[pi * 3 + ch];
+                    counts[t][pix] += 1u;
+                });
+            });
+        for (auto &th : pool) th.join();
+    }
+    std::vector<double> img(npix * 3), dl(npix * 3);
+    std::vector<uint32_t> cnt(npix, 0u);
+    double L = 0.0;
+    for (size_t p = 0; p < npix; ++p) {
+        for (int t = 0; t < nt; ++t) cnt[p] += counts[t][p];
+        for (int ch = 0; ch < 3; ++ch) {
+            double s = 0.0;
+            for (int t = 0; t < nt; ++t) s += sums[t][p * 3 + ch];
+            const double v = cnt[p] ? s / (double)cnt[p] : (double)cfg->backgroundColor[ch];
+            img[p * 3 + ch] = v;
+            const double d = v - target[p * 3 + ch];
+            L += scale * d * d;
+            dl[p * 3 + ch] = cnt[p] ? 2.0 * scale * d : 0.0;
+        }
+    }
+    if (image) std::memcpy(image, img.data(), npix * 3 * sizeof(double));
+    if (loss) *loss += L;
+    std::vector<char> listed;
+    std::vector<uint32_t> slot;
+    if (fd && n_fd) {
+        uint32_t maxp = 0;
+        for (uint32_t k = 0; k < n_fd; ++k) maxp = std::max(maxp, fd_points[k]);
+        listed.assign((size_t)maxp + 1, 0);
+        slot.assign((size_t)maxp + 1, 0u);
+        for (uint32_t k = 0; k < n_fd; ++k) {
+            listed[fd_points[k]] = 1;
+            slot[fd_points[k]] = k;
+        }
+    }
+    visit(0, nvis, [&](uint32_t pi, uint32_t pix) {
+        const double n = (double)cnt[pix];
+        if (grad)
+            for (int ch = 0; ch < 3; ++ch) grad[pi * 3 + ch] += dl[pix * 3 + ch] / n;
+        if (fd && pi < listed.size() && listed[pi]) {
+            for (int ch = 0; ch < 3; ++ch) {
+                const double t = target[pix * 3 + ch], v = img[pix * 3 + ch];
+                const double up = v + fd_h / n - t, dn = v - fd_h / n - t;
+                fd[slot[pi] * 3 + ch] += scale * (up * up - dn * dn) / (2.0 * fd_h);
+            }
+        }
+    });
+    return 0;
+}
+
 // NearestPointCPUReference.render (NearestPointCPUReference.swift:16-81).
 void orc_nearest_cpu_reference(const orc_cloud *cloud, int w, int h, const float view[16],
                                const float proj[16], int enable_frustum, uint32_t *depths,

@@ -99,6 +99,17 @@ int orc_render(const orc_cloud *clouds, uint32_t nclouds, const orc_config *cfg,
                uint8_t *rgba, float *depthf, orc_visible *visible, uint32_t visible_stride,
                uint32_t *visible_count, int threads);
 
+/* Differentiable HQS colours in FP64 for one view of one cloud (reference of
+ * the FP32 forward / adjoint): colors and grad hold 3 doubles per pool point,
+ * target and image 3 per pixel (row 0 = top).  loss, grad and fd are added
+ * to; fd[k*3+c] = central difference (step fd_h) of the loss in channel c
+ * of point fd_points[k].  Any output may be NULL. */
+int orc_hqs_grad_f64(const orc_cloud *cloud, const orc_config *cfg, const float view[16],
+                     const float proj[16], int width, int height, const double *colors,
+                     const double *target, double scale, double *image, double *loss,
+                     double *grad, const uint32_t *fd_points, uint32_t n_fd, double fd_h,
+                     double *fd, int threads);
+
 /* holeFillUpdate ping-pong (HoleFill/Shaders.metal:10-48, ComputeRasteriser.swift:298-320). */
 void orc_hole_fill(uint8_t *rgba, int width, int height, int iterations);
 

@@ -31,7 +31,7 @@ __all__ = ["Context", "ComputeRasteriserConfiguration", "ComputeRasteriserCapaci
            "VISIBLE_DTYPE", "computeRasteriserThreadsPerGroup", "MODE_HQS", "MODE_NEAREST",
            "identity_files", "matrix_multiply", "GPUPacker", "PackInput", "DeviceBuffer",
            "HostBuffer", "TerrainParams", "synth_terrain", "synth_lattice", "terrain_height",
-           "PASS_NAMES", "MultiViewRasteriser"]
+           "PASS_NAMES", "MultiViewRasteriser", "l2_loss"]
 
 PASS_NAMES = ("clear", "cull", "depth", "color", "resolve", "hole_fill")
 
@@ -158,7 +158,12 @@ class DeviceBuffer:
                 "version": 3, "strides": None}
 
     def upload(self, host: np.ndarray):
-        h = np.ascontiguousarray(host)
+        """Copy host data in: raw bytes into a byte (uint8) buffer, otherwise
+        converted to the buffer's dtype."""
+        if self.dtype == np.uint8:
+            h = np.ascontiguousarray(host)
+        else:
+            h = np.ascontiguousarray(host, dtype=self.dtype)
         N.check(N.lib().cr_buffer_upload(self.context.handle, C.c_void_p(self.ptr), N.ptr(h),
                                          min(h.nbytes, self.nbytes)))
 
@@ -169,9 +174,11 @@ class DeviceBuffer:
         return out
 
     def close(self):
-        if self.ptr:
+        # A buffer outliving its context (interpreter shutdown frees objects in
+        # no fixed order) was released with it.
+        if self.ptr and self.context.handle:
             N.lib().cr_buffer_destroy(self.context.handle, C.c_void_p(self.ptr))
-            self.ptr = None
+        self.ptr = None
 
     def __del__(self):
         try:
@@ -501,9 +508,9 @@ class ComputeRasteriserPointCloud:
         return out[:count.value].copy()
 
     def close(self):
-        if self._h:
+        if self._h and self.context.handle:
             N.lib().cr_cloud_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -628,9 +635,9 @@ class _Frame:
         return self._h
 
     def close(self):
-        if self._h:
+        if self._h and self.context.handle:
             N.lib().cr_frame_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -825,6 +832,30 @@ class ComputeRasteriser:
         N.check(N.lib().cr_frame_read_nearest_index(f.handle, N.ptr(out)))
         return out
 
+    # --- differentiable colours (FP32 variant of the colour pass) ---
+    def forwardF32(self, cloud: ComputeRasteriserPointCloud, colors: DeviceBuffer,
+                   image: DeviceBuffer):
+        """Image (height x width x 3 float32, device) of `cloud` with learnable
+        colours (pool points x 3 float32, device) at the camera of the last
+        update (cr_hqs_forward_f32)."""
+        f = self._require_frame()
+        cfg = self.configuration.to_c()
+        cam = _camera_c(self._camera)
+        N.check(N.lib().cr_hqs_forward_f32(self.context.handle, f.handle, cloud.handle,
+                                           C.byref(cfg), C.byref(cam), C.c_void_p(colors.ptr),
+                                           C.c_void_p(image.ptr)))
+
+    def backwardColors(self, cloud: ComputeRasteriserPointCloud, dL_dimage: DeviceBuffer,
+                       dL_dcolors: DeviceBuffer):
+        """Adds dL/dcolors of the last forwardF32 to dL_dcolors (cr_hqs_backward_colors)."""
+        f = self._require_frame()
+        cfg = self.configuration.to_c()
+        cam = _camera_c(self._camera)
+        N.check(N.lib().cr_hqs_backward_colors(self.context.handle, f.handle, cloud.handle,
+                                               C.byref(cfg), C.byref(cam),
+                                               C.c_void_p(dL_dimage.ptr),
+                                               C.c_void_p(dL_dcolors.ptr)))
+
     def pickPointIndex(self, atNDC, cloud: ComputeRasteriserPointCloud, camera,
                        searchRadius: int = 10):
         """pickPointIndex(atNDC:in:camera:searchRadius:) (ComputeRasteriser.swift:609-670)."""
@@ -923,3 +954,15 @@ class MultiViewRasteriser:
     def close(self):
         for f in self.frames:
             f.close()
+
+
+def l2_loss(context: Context, image: DeviceBuffer, target: DeviceBuffer, scale: float,
+            dL_dimage: DeviceBuffer, want_loss: bool = True):
+    """dL_dimage = 2 * scale * (image - target); returns scale * sum (image -
+    target)^2 (FP64, synchronises) when want_loss (cr_l2_loss)."""
+    n = image.nbytes // 4
+    loss = C.c_double()
+    N.check(N.lib().cr_l2_loss(context.handle, C.c_void_p(image.ptr), C.c_void_p(target.ptr), n,
+                               float(scale), C.c_void_p(dL_dimage.ptr),
+                               C.byref(loss) if want_loss else None))
+    return loss.value if want_loss else None

@@ -142,6 +142,11 @@ PROTOTYPES = {
     "cr_cull_noalloc": (C.c_int, [P, u32, P, u32, C.POINTER(cr_config), C.POINTER(cr_camera),
                                   C.c_int, C.c_int, P, P, P]),
     "cr_render_multiview": (C.c_int, [P, P, P, u32, P, P, u32, C.POINTER(cr_config)]),
+    "cr_hqs_forward_f32": (C.c_int, [P, P, P, C.POINTER(cr_config), C.POINTER(cr_camera), P,
+                                     P]),
+    "cr_hqs_backward_colors": (C.c_int, [P, P, P, C.POINTER(cr_config), C.POINTER(cr_camera),
+                                         P, P]),
+    "cr_l2_loss": (C.c_int, [P, P, P, u64, C.c_float, P, C.POINTER(C.c_double)]),
     "cr_autotune_multiview": (C.c_int, [P, P, P, u32, P, P, u32, C.POINTER(cr_config),
                                         C.c_char_p, C.c_int, C.POINTER(cr_tuning),
                                         C.POINTER(C.c_float)]),

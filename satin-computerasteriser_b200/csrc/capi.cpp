@@ -406,6 +406,7 @@ CR_API cr_status cr_context_destroy(cr_context *ctx) {
         delete ctx->pack;
     }
     if (ctx->views) views_destroy(ctx->views);
+    if (ctx->d_loss) cudaFree(ctx->d_loss);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CR_OK;
@@ -746,6 +747,8 @@ CR_API cr_status cr_frame_destroy(cr_frame *f) {
     dfree(f->d_rgba[0]);
     dfree(f->d_rgba[1]);
     dfree(f->d_depthf);
+    dfree(f->d_fsum);
+    dfree(f->d_fcount);
     delete f;
     return CR_OK;
 }
@@ -939,6 +942,91 @@ CR_API cr_status cr_frame_read_nearest_index_rows(cr_frame *f, int row0, int nro
 }
 
 // pickPointIndex (ComputeRasteriser.swift:609-670).
+// ---------------------------------------------------------------- differentiable colours
+// The HQS colour pass with learnable FP32 colours (an FP32 variant beside the
+// integer path; no counterpart in the reference) and its adjoint.
+
+static cr_status validate_f32(cr_context *ctx, cr_frame *f, cr_cloud *cloud, const cr_config *cfg,
+                              const cr_camera *cam, const void *in, const void *out) {
+    cr_status st = validate_render(ctx, f, cfg, cam);
+    if (st) return st;
+    if (!cloud || cloud->ctx != ctx)
+        return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null or from another context");
+    if (!in || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null device pointer");
+    if (cfg->mode != CR_MODE_HIGH_QUALITY_AVERAGE)
+        return fail(CR_ERR_UNSUPPORTED, "differentiable colours need the HQS mode");
+    if (cfg->colorizeChunks || cfg->colorizeOverdraw)
+        return fail(CR_ERR_UNSUPPORTED, "colorize options replace the learnable colours");
+    return CR_OK;
+}
+
+CR_API cr_status cr_hqs_forward_f32(cr_context *ctx, cr_frame *f, cr_cloud *cloud,
+                                    const cr_config *cfg, const cr_camera *cam,
+                                    const float *colors, float *image) {
+    cr_status st = validate_f32(ctx, f, cloud, cfg, cam, colors, image);
+    if (st) return st;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const size_t npix = (size_t)f->width * f->height;
+    if (!f->d_fsum) {
+        if ((st = dalloc(&f->d_fsum, npix * sizeof(float4))) ||
+            (st = dalloc(&f->d_fcount, npix * 4)))
+            return st;
+    }
+    CR_CUDA(cudaMemsetAsync(f->d_depth, 0, npix * 4, s));
+    CR_CUDA(cudaMemsetAsync(f->d_fsum, 0, npix * sizeof(float4), s));
+    CR_CUDA(cudaMemsetAsync(f->d_fcount, 0, npix * 4, s));
+    if (cloud->resident > 0) {
+        const RasterUniforms rau = make_raster_uniforms(cfg, cam, f->width, f->height);
+        RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
+        t.fsum = f->d_fsum;
+        t.fcount = f->d_fcount;
+        if ((st = launch_cull(cloud, make_cull_uniforms(cfg, cam, f->width, f->height), s)) ||
+            (st = launch_raster(cloud, PASS_DEPTH, rau, t, s)) ||
+            (st = launch_raster_f32(cloud, PASS_COLOR_F32, rau, t, colors, nullptr, nullptr, s)))
+            return st;
+    }
+    const float bg[3] = {cfg->backgroundColor[0], cfg->backgroundColor[1],
+                         cfg->backgroundColor[2]};
+    return launch_resolve_f32(f, bg, image, s);
+}
+
+CR_API cr_status cr_hqs_backward_colors(cr_context *ctx, cr_frame *f, cr_cloud *cloud,
+                                        const cr_config *cfg, const cr_camera *cam,
+                                        const float *dL_dimage, float *dL_dcolors) {
+    cr_status st = validate_f32(ctx, f, cloud, cfg, cam, dL_dimage, dL_dcolors);
+    if (st) return st;
+    if (!f->d_fsum)
+        return fail(CR_ERR_INVALID_ARGUMENT, "cr_hqs_forward_f32 has not run on this frame");
+    if (cloud->resident == 0) return CR_OK;
+    DeviceGuard g(ctx->device);
+    const RasterUniforms rau = make_raster_uniforms(cfg, cam, f->width, f->height);
+    RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
+    t.fsum = f->d_fsum;
+    t.fcount = f->d_fcount;
+    return launch_raster_f32(cloud, PASS_GRAD, rau, t, nullptr, dL_dimage, dL_dcolors,
+                             ctx->stream);
+}
+
+CR_API cr_status cr_l2_loss(cr_context *ctx, const float *image, const float *target, uint64_t n,
+                            float scale, float *dL_dimage, double *loss) {
+    if (!ctx || (n && (!image || !target || !dL_dimage)))
+        return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    cr_status st;
+    if (loss && !ctx->d_loss && (st = dalloc(&ctx->d_loss, sizeof(double)))) return st;
+    if (loss) CR_CUDA(cudaMemsetAsync(ctx->d_loss, 0, sizeof(double), s));
+    if ((st = launch_l2_loss(image, target, n, scale, dL_dimage, loss ? ctx->d_loss : nullptr,
+                             ctx->sm_count, s)))
+        return st;
+    if (loss) {
+        CR_CUDA(cudaMemcpyAsync(loss, ctx->d_loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+    }
+    return CR_OK;
+}
+
 CR_API cr_status cr_pick(cr_context *ctx, cr_frame *f, cr_cloud *cloud, const float ndc[2],
                          const cr_config *cfg, const cr_camera *cam, int search_radius,
                          uint32_t *index_out, int *found_out) {

@@ -76,11 +76,12 @@ constexpr int kMinChunkPoints = 256;
 struct cr_context {
     PackScratch *pack = nullptr;  // grow-only packer scratch
     ViewsState *views = nullptr;  // buffers and graphs of the last batched render
+    double *d_loss = nullptr;     // cr_l2_loss's device accumulator (lazy)
     int device = 0;
     cudaStream_t stream = nullptr;
     int sm_count = 0;
-    int blocks_per_sm[5] = {0, 0, 0, 0, 0};        // occupancy of the persistent point passes
-    int blocks_per_sm_views[5] = {0, 0, 0, 0, 0};  // the same, batched-view kernels
+    int blocks_per_sm[7] = {};        // occupancy of the persistent point passes (per RasterPass)
+    int blocks_per_sm_views[7] = {};  // the same, batched-view kernels
     int chunk_points = 2048;           // points per chunk work record
     int view_group_pixels = 4194304;   // batched views: pixels per depth/colour group
     bool use_tiles = true;             // shared-memory screen tiles
@@ -159,6 +160,8 @@ struct cr_frame {
     unsigned long long *d_nearest = nullptr;  // (depth << 32) | ~pointIndex
     uint32_t *d_rgba[2] = {nullptr, nullptr}; // RGBA8 ping-pong (resolve, hole fill)
     float *d_depthf = nullptr;              // resolve R32F depth
+    float4 *d_fsum = nullptr;               // differentiable colours: FP32 R, G, B sums (lazy)
+    uint32_t *d_fcount = nullptr;           //   and their sample counts
     int final_rgba = 0;                     // which d_rgba holds the final image
     int last_mode = -1;                     // 0 HQS, 1 nearest, -1 none
 };
@@ -209,9 +212,13 @@ enum RasterPass : int {
     PASS_COLOR = 1,
     PASS_NEAREST = 2,
     PASS_DEPTH_FRAG = 3,
-    PASS_COLOR_FRAG = 4
+    PASS_COLOR_FRAG = 4,
+    PASS_COLOR_F32 = 5,  // differentiable colours: FP32 sums of learnable colours + count
+    PASS_GRAD = 6        // their adjoint: per point, dL/dpixel / count over its visible pixels
 };
-constexpr int kRasterPassCount = 5;
+constexpr int kRasterPassCount = 7;
+static_assert(kRasterPassCount == sizeof(cr_context::blocks_per_sm) / sizeof(int),
+              "one occupancy entry per raster pass");
 
 struct RasterUniforms {
     float view[16];
@@ -228,6 +235,8 @@ struct RasterTargets {
     uint32_t *depth;              // HQS depth plane
     uint4 *accum;                 // HQS accumulators
     unsigned long long *nearest;  // nearest key plane
+    float4 *fsum = nullptr;       // differentiable colours: FP32 sums per pixel
+    uint32_t *fcount = nullptr;   //   and sample counts
     // Colour adds as two 64-bit words per pixel (R | G << 32, B | count << 32)
     // instead of four 32-bit ones; exact while a pixel holds at most
     // kPackedMaxCount samples, which the resolve checks.
@@ -243,6 +252,11 @@ constexpr uint32_t kPackedMaxCount = 16843009u;
 
 cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
                         const RasterTargets &t, cudaStream_t s);
+// PASS_COLOR_F32 (colors: 3 floats per pool point) or PASS_GRAD (dldimg: 3
+// floats per pixel, grad: 3 floats per pool point, added to) of one cloud.
+cr_status launch_raster_f32(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
+                            const RasterTargets &t, const float *colors, const float *dldimg,
+                            float *grad, cudaStream_t s);
 
 // Mode, point-size mode and the unsupported colour effects of a configuration.
 cr_status validate_config(const cr_config *cfg);
@@ -319,6 +333,14 @@ cr_status launch_accum_redo_clear_views(const ViewDesc *views, uint32_t nviews,
 cr_status launch_resolve_views(const ViewDesc *views, uint32_t nviews, uint32_t pix0,
                                uint32_t npix, const ResolveUniforms &u, uint32_t *redo_flag,
                                bool check, const uint32_t *redo, int sm_count, cudaStream_t s);
+// Differentiable colours: image[3p + c] = fsum[p].c / fcount[p], or the
+// background where the count is 0.
+cr_status launch_resolve_f32(cr_frame *f, const float background[3], float *image,
+                             cudaStream_t s);
+// dldimg = 2 * scale * (image - target) over n floats; the loss
+// scale * sum (image - target)^2 is added to *loss (device double) if loss.
+cr_status launch_l2_loss(const float *image, const float *target, uint64_t n, float scale,
+                         float *dldimg, double *loss, int sm_count, cudaStream_t s);
 // One hole-fill iteration of every view: rgba[src] -> rgba[1 - src].
 cr_status launch_hole_fill_views(const ViewDesc *views, uint32_t nviews, uint32_t total_pix,
                                  int src, int sm_count, cudaStream_t s);

@@ -69,6 +69,13 @@ template <>
 struct TileCfg<PASS_DEPTH_FRAG> : TileCfg<PASS_DEPTH> {};
 template <>
 struct TileCfg<PASS_COLOR_FRAG> : TileCfg<PASS_COLOR> {};
+template <>
+struct TileCfg<PASS_COLOR_F32> {  // no screen tiles
+    static constexpr int kPx = 0;
+    static constexpr int kBytes = 0;
+};
+template <>
+struct TileCfg<PASS_GRAD> : TileCfg<PASS_COLOR_F32> {};
 
 __host__ __device__ constexpr bool is_depth(int p) { return p == PASS_DEPTH || p == PASS_DEPTH_FRAG; }
 __host__ __device__ constexpr bool is_color(int p) { return p == PASS_COLOR || p == PASS_COLOR_FRAG; }
@@ -88,6 +95,10 @@ struct RasterArgs {
     float *frag_z;
     uint32_t *frag_col;
     uint32_t *frag_count;
+    // Differentiable colours: learnable colours, dL/dpixel, gradient (3 floats each).
+    const float *fcolors;
+    const float *dldimg;
+    float *fgrad;
     // Batched views (MV kernels): per-view frames, culls and file tables.
     const ViewDesc *views;
     uint32_t nviews;
@@ -286,6 +297,37 @@ __device__ __forceinline__ void red_max_u64(unsigned long long *p, unsigned long
                  : "memory");
 }
 
+__device__ __forceinline__ void red_add_f32x3(float4 *p, float r, float g, float b) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(
+                     __cvta_generic_to_global(p)),
+                 "f"(r), "f"(g), "f"(b), "f"(0.0f)
+                 : "memory");
+}
+
+// Differentiable colours, one visible (point, pixel): the forward adds the
+// point's FP32 colour and one sample; the adjoint adds dL/dpixel / count to
+// the point's gradient (g, in registers, written once per point).
+__device__ __forceinline__ void color_f32_sample(const RasterArgs &a, uint32_t pix,
+                                                 uint32_t pointIndex) {
+    const float *c = a.fcolors + 3 * (size_t)pointIndex;
+    red_add_f32x3(a.t.fsum + pix, c[0], c[1], c[2]);
+    red_add_u32(a.t.fcount + pix, 1u);
+}
+__device__ __forceinline__ void grad_sample(const RasterArgs &a, uint32_t pix, float g[3]) {
+    const float n = (float)a.t.fcount[pix];
+    const float *d = a.dldimg + 3 * (size_t)pix;
+    g[0] = g[0] + d[0] / n;
+    g[1] = g[1] + d[1] / n;
+    g[2] = g[2] + d[2] / n;
+}
+__device__ __forceinline__ void grad_store(const RasterArgs &a, uint32_t pointIndex,
+                                           const float g[3]) {
+    float *o = a.fgrad + 3 * (size_t)pointIndex;
+    o[0] = o[0] + g[0];
+    o[1] = o[1] + g[1];
+    o[2] = o[2] + g[2];
+}
+
 // Adds one sample group to a pixel's R, G, B and count.  Packed: the uint4
 // as two 64-bit words, R | G << 32 and B | count << 32 — half the global
 // atomics.  A lower field that passes 2^32 would carry into its neighbour;
@@ -321,6 +363,15 @@ __device__ __forceinline__ void emit_direct(const RasterArgs &a, const ViewRegsT
         if (vis)
             color_global<MV>(a, vr, pix, o.color & 0xffu, (o.color >> 8) & 0xffu, (o.color >> 16) & 0xffu,
                          1u);
+    } else if (PASS == PASS_COLOR_F32 || PASS == PASS_GRAD) {
+        const uint32_t closest = o.ok ? vdepth<MV>(vr)[pix] : 0u;
+        const bool vis = closest != 0u && o.nz >= crd::uint_to_depth(closest) * a.keep_scale;
+        if (PASS == PASS_COLOR_F32 && vis) color_f32_sample(a, pix, o.pointIndex);
+        if (PASS == PASS_GRAD && vis) {
+            float g[3] = {0.0f, 0.0f, 0.0f};
+            grad_sample(a, pix, g);
+            grad_store(a, o.pointIndex, g);
+        }
     } else {
         if (o.ok) red_max_u64(&vnearest<MV>(vr)[pix], nearest_key(o.depth, o.pointIndex));
     }
@@ -373,6 +424,7 @@ __device__ __forceinline__ void emit_footprint(const RasterArgs &a, const ViewRe
     const int rad =
         crd::footprint_radius(o.px, o.py, o.pz, sb.world, view_view<MV>(a), view_proj<MV>(a), vh<MV>(vr), ps);
     const int W = vw<MV>(vr), H = vh<MV>(vr);
+    float g[3] = {0.0f, 0.0f, 0.0f};  // PASS_GRAD
     for (int oy = -rad; oy <= rad; ++oy) {
         for (int ox = -rad; ox <= rad; ++ox) {
             if (!crd::inside_footprint(ox, oy, rad)) continue;
@@ -381,17 +433,23 @@ __device__ __forceinline__ void emit_footprint(const RasterArgs &a, const ViewRe
             const uint32_t pix = (uint32_t)(ty * W + tx);
             if (is_depth(PASS)) {
                 red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
-            } else if (is_color(PASS)) {
+            } else if (is_color(PASS) || PASS == PASS_COLOR_F32 || PASS == PASS_GRAD) {
                 const uint32_t closest = vdepth<MV>(vr)[pix];
                 if (closest == 0u) continue;
                 if (!(o.nz >= crd::uint_to_depth(closest) * a.keep_scale)) continue;
-                color_global<MV>(a, vr, pix, o.color & 0xffu, (o.color >> 8) & 0xffu,
-                             (o.color >> 16) & 0xffu, 1u);
+                if (PASS == PASS_COLOR_F32)
+                    color_f32_sample(a, pix, o.pointIndex);
+                else if (PASS == PASS_GRAD)
+                    grad_sample(a, pix, g);
+                else
+                    color_global<MV>(a, vr, pix, o.color & 0xffu, (o.color >> 8) & 0xffu,
+                                     (o.color >> 16) & 0xffu, 1u);
             } else {
                 red_max_u64(&vnearest<MV>(vr)[pix], nearest_key(o.depth, o.pointIndex));
             }
         }
     }
+    if (PASS == PASS_GRAD) grad_store(a, o.pointIndex, g);
 }
 
 // Shared count of the fragments the current chunk has kept.
@@ -895,6 +953,9 @@ RasterArgs make_args(cr_cloud *cloud, const RasterUniforms &u, const RasterTarge
     a.chunk_poff = nullptr;
     a.frag_cap = 0;
     a.frag_overflow = nullptr;
+    a.fcolors = nullptr;
+    a.dldimg = nullptr;
+    a.fgrad = nullptr;
     return a;
 }
 
@@ -918,6 +979,29 @@ cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &
     case PASS_COLOR_FRAG: launch_pass<PASS_COLOR_FRAG, false>(a, grid, s); break;
     default: launch_pass<PASS_NEAREST, false>(a, grid, s); break;
     }
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+cr_status launch_raster_f32(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
+                            const RasterTargets &t, const float *colors, const float *dldimg,
+                            float *grad, cudaStream_t s) {
+    if (pass != PASS_COLOR_F32 && pass != PASS_GRAD)
+        return cri::fail(CR_ERR_INTERNAL, "launch_raster_f32: pass");
+    RasterArgs a = make_args(cloud, u, t);
+    a.fcolors = colors;
+    a.dldimg = dldimg;
+    a.fgrad = grad;
+    cr_context *ctx = cloud->ctx;
+    if (ctx->blocks_per_sm[pass] == 0)
+        ctx->blocks_per_sm[pass] = pass == PASS_COLOR_F32
+                                       ? blocks_per_sm_for<PASS_COLOR_F32, false>()
+                                       : blocks_per_sm_for<PASS_GRAD, false>();
+    const int grid = ctx->sm_count * ctx->blocks_per_sm[pass];
+    if (pass == PASS_COLOR_F32)
+        launch_pass<PASS_COLOR_F32, false>(a, grid, s);
+    else
+        launch_pass<PASS_GRAD, false>(a, grid, s);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

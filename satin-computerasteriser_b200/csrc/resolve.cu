@@ -198,6 +198,52 @@ __global__ void __launch_bounds__(kThreads)
     if (index) index[p] = ~(uint32_t)k;
 }
 
+// Differentiable colours: the pixel's mean FP32 colour (background where no
+// sample), row 0 = top, 3 floats per pixel.
+__global__ void __launch_bounds__(kThreads)
+    resolve_f32(const float4 *__restrict__ fsum, const uint32_t *__restrict__ fcount,
+                float *__restrict__ image, uint32_t npix, float bg0, float bg1, float bg2) {
+    for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < npix; p += gridDim.x * kThreads) {
+        const uint32_t n = fcount[p];
+        float *o = image + 3 * (size_t)p;
+        if (n == 0u) {
+            o[0] = bg0;
+            o[1] = bg1;
+            o[2] = bg2;
+            continue;
+        }
+        const float4 s = fsum[p];
+        const float fn = (float)n;
+        o[0] = s.x / fn;
+        o[1] = s.y / fn;
+        o[2] = s.z / fn;
+    }
+}
+
+// L2 loss: dldimg = 2 * scale * (image - target); the loss, accumulated in
+// FP64 per block, is added to *loss.
+__global__ void __launch_bounds__(kThreads)
+    l2_loss(const float *__restrict__ image, const float *__restrict__ target, uint64_t n,
+            float scale, float *__restrict__ dldimg, double *loss) {
+    __shared__ double part[kThreads / 32];
+    double acc = 0.0;
+    for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * kThreads) {
+        const float d = image[i] - target[i];
+        dldimg[i] = 2.0f * scale * d;
+        acc += (double)d * (double)d;
+    }
+    if (!loss) return;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) t += part[w];
+        atomicAdd(loss, t * (double)scale);
+    }
+}
+
 __global__ void __launch_bounds__(kThreads)
     accum_redo_clear(uint4 *__restrict__ accum, const uint32_t *redo, uint32_t npix) {
     if (*redo == 0u) return;
@@ -297,6 +343,25 @@ cr_status launch_hole_fill_views(const ViewDesc *views, uint32_t nviews, uint32_
                                  int src, int sm_count, cudaStream_t s) {
     hole_fill_views<<<views_grid(total_pix, sm_count), kThreads, 0, s>>>(views, nviews, total_pix,
                                                                          src);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+cr_status launch_resolve_f32(cr_frame *f, const float background[3], float *image,
+                             cudaStream_t s) {
+    const uint32_t npix = (uint32_t)f->width * (uint32_t)f->height;
+    resolve_f32<<<views_grid(npix, f->ctx->sm_count), kThreads, 0, s>>>(
+        f->d_fsum, f->d_fcount, image, npix, background[0], background[1], background[2]);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+cr_status launch_l2_loss(const float *image, const float *target, uint64_t n, float scale,
+                         float *dldimg, double *loss, int sm_count, cudaStream_t s) {
+    if (n == 0) return CR_OK;
+    const uint64_t need = (n + kThreads - 1) / kThreads;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(need, (uint64_t)sm_count * 8);
+    l2_loss<<<grid, kThreads, 0, s>>>(image, target, n, scale, dldimg, loss);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }
