@@ -71,6 +71,13 @@ def parse_args():
                     help="views of the batched multi-view comparison (0 = skip it)")
     ap.add_argument("--mv-points", type=int, default=50_000_000)
     ap.add_argument("--mv-reps", type=int, default=5)
+    ap.add_argument("--diff-points", type=int, default=20_000_000,
+                    help="points of the differentiable-colour leg (0 = skip it)")
+    ap.add_argument("--diff-views", type=int, default=32)
+    ap.add_argument("--diff-check", type=int, default=1000,
+                    help="points whose gradient is checked against the FP64 oracle (0 = none)")
+    ap.add_argument("--pack-points", type=int, default=400_000_000,
+                    help="points of the 63-bit packer leg (0 = skip it)")
     return ap.parse_args()
 
 
@@ -437,7 +444,217 @@ def run_ours(args, dist):
     pinned.close()
     if args.mv_views > 0:
         out["multiview"] = run_multiview(args, cr, ctx, torch, dist)
+    if args.diff_points > 0:
+        out["differentiable"] = run_differentiable(args, cr, ctx, torch, dist)
+    if args.pack_points > 0:
+        cloud.close()
+        out["packer"] = run_packer(args, cr, ctx, torch, dist)
     return out
+
+
+def decoded_positions(cloud, first=0, n=None):
+    """Full-precision (level 0, 30-bit) positions of pool points [first, first+n):
+    a freshly packed pool holds batch k's points from slot k * pointsPerBatch."""
+    pts = cloud.points(first, n)
+    ppb = cloud.capacity.pointsPerBatch
+    b = cloud.batches()
+    idx = np.arange(first, first + len(pts["xyzLow"]), dtype=np.int64)
+    slot = idx // ppb
+    lo, me, hi = (pts[k].astype(np.uint64) for k in ("xyzLow", "xyzMed", "xyzHigh"))
+    out = np.zeros((len(idx), 3), np.float64)
+    for a, (mn, mx) in enumerate((("minX", "maxX"), ("minY", "maxY"), ("minZ", "maxZ"))):
+        s = 10 * a
+        q = (((lo >> s) & 1023) << 20) | (((me >> s) & 1023) << 10) | ((hi >> s) & 1023)
+        size = np.maximum(b[mx][slot].astype(np.float64) - b[mn][slot], 1e-6)
+        out[:, a] = q.astype(np.float64) * size / 1073741824.0 + b[mn][slot]
+    return out
+
+
+def run_differentiable(args, cr, ctx, torch, dist):
+    """Differentiable HQS colour fitting: a heightfield of --diff-points points
+    (seed 0xC0FFEE05) with learnable FP32 colours initialised to 0.5, --diff-views
+    views at 512 x 512 (seeded poses), targets rendered from the hidden field
+    c(x) = 0.5 + 0.5 sin(k . x / 400 m + phi).  A step is, for every view, the FP32
+    forward, the L2 loss gradient and the adjoint (gradients accumulate over the
+    views); timed with CUDA events.  The gradient of --diff-check seeded points
+    visible in some view is compared with the FP64 oracle's adjoint and central
+    differences (step 1e-3)."""
+    seed = 0xC0FFEE05
+    params = cr.TerrainParams(seed=seed)
+    cloud, _ = build_cloud(cr, ctx, argparse.Namespace(points=args.diff_points), params)
+    n = cloud.capacity.maxResidentPoints
+    W = H = 512
+    cams = make_poses(cr, params, args.diff_views, seed ^ dist.rank, 1.0)
+    xyz = decoded_positions(cloud)
+    k = np.array([[3.1, -2.3, 1.7], [-1.9, 2.7, 2.2], [2.4, 1.3, -3.0]]) / 400.0
+    phi = np.array([0.3, 1.1, -0.7])
+    hidden = (0.5 + 0.5 * np.sin(xyz @ k.T + phi)).astype(np.float32)
+    del xyz
+    learn = np.full((n, 3), 0.5, np.float32)
+    ras = cr.ComputeRasteriser(ctx)
+    ras.addPointCloud(cloud)
+    ras.resize((W, H))
+    d_col = cr.DeviceBuffer(ctx, n * 12, (n, 3), np.float32)
+    d_grad = cr.DeviceBuffer(ctx, n * 12, (n, 3), np.float32)
+    d_img = cr.DeviceBuffer(ctx, H * W * 12, (H, W, 3), np.float32)
+    d_dl = cr.DeviceBuffer(ctx, H * W * 12, (H, W, 3), np.float32)
+    tgts = [cr.DeviceBuffer(ctx, H * W * 12, (H, W, 3), np.float32) for _ in cams]
+    d_col.upload(hidden)
+    for cam, t in zip(cams, tgts):
+        ras.update(cam)
+        ras.forwardF32(cloud, d_col, t)
+    d_col.upload(learn)
+    scale = 1.0 / (3.0 * W * H * len(cams))
+
+    def step():
+        for cam, t in zip(cams, tgts):
+            ras.update(cam)
+            ras.forwardF32(cloud, d_col, d_img)
+            cr.l2_loss(ctx, d_img, t, scale, d_dl, want_loss=False)
+            ras.backwardColors(cloud, d_dl, d_grad)
+
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=f"cuda:{dist.local}")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(2):
+        step()
+    reps = 3
+    ctx.synchronize()
+    ev0.record(stream)
+    for _ in range(reps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    step_ms = ev0.elapsed_time(ev1) / reps
+    out = {"points": args.diff_points, "views": len(cams), "size": f"{W}x{H}",
+           "step_ms": round(step_ms, 3),
+           "views_per_s": round(len(cams) / (step_ms / 1e3), 1),
+           "gpts_per_s": round(args.diff_points * len(cams) / (step_ms / 1e3) / 1e9, 2),
+           "step": "per view: FP32 forward + L2 loss gradient + adjoint (accumulated)"}
+    if args.diff_check > 0 and dist.rank == 0:
+        out["gradient_check"] = diff_gradient_check(args, cr, ctx, ras, cloud, cams, tgts, d_col,
+                                                    d_grad, learn, scale)
+    for b in [d_col, d_grad, d_img, d_dl] + tgts:
+        b.close()
+    cloud.close()
+    return out
+
+
+def diff_gradient_check(args, cr, ctx, ras, cloud, cams, tgts, d_col, d_grad, learn, scale):
+    import oracle as orc
+    orc.build()
+    n = len(learn)
+    d_col.upload(learn)
+    d_grad.upload(np.zeros((n, 3), np.float32))
+    d_img = cr.DeviceBuffer(ctx, tgts[0].nbytes, tgts[0].shape, np.float32)
+    d_dl = cr.DeviceBuffer(ctx, tgts[0].nbytes, tgts[0].shape, np.float32)
+    for cam, t in zip(cams, tgts):
+        ras.update(cam)
+        ras.forwardF32(cloud, d_col, d_img)
+        cr.l2_loss(ctx, d_img, t, scale, d_dl, want_loss=False)
+        ras.backwardColors(cloud, d_dl, d_grad)
+    g = d_grad.download().astype(np.float64)
+    cand = np.flatnonzero(np.abs(g).max(axis=1) > 0)
+    pts = np.sort(np.random.default_rng(0x5EED).choice(cand, min(args.diff_check, len(cand)),
+                                                        replace=False))
+    ocl = oracle_cloud(orc, cloud)
+    ocfg = oracle_config(orc, ras.configuration)
+    threads = os.cpu_count() or 1
+    grad64 = np.zeros((n, 3))
+    fd = np.zeros((len(pts), 3))
+    t0 = time.perf_counter()
+    W, H = ras.viewportSize
+    for cam, t in zip(cams, tgts):
+        ras.update(cam)
+        ocl.files = cloud.files()
+        orc.hqs_grad_f64(ocl, ocfg, cam.viewMatrix, cam.projectionMatrix, W, H,
+                         learn.astype(np.float64), t.download().astype(np.float64), scale,
+                         grad=grad64, fd_points=pts.astype(np.uint32), fd_h=1e-3, fd=fd,
+                         threads=threads)
+    floor = 1e-2 * np.abs(grad64[pts]).max()
+
+    def rel(a, b):
+        return float((np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), floor)).max())
+
+    d_img.close()
+    d_dl.close()
+    return {"points": int(len(pts)), "fd_step": 1e-3,
+            "max_rel_err_vs_fp64_fd": rel(g[pts], fd),
+            "max_rel_err_vs_fp64_adjoint": rel(g[pts], grad64[pts]),
+            "fd_vs_adjoint_fp64": rel(fd, grad64[pts]),
+            "rel_err": "max over points of max_c |g - ref| / max(max_c |ref|, 1e-2 max |ref|)",
+            "oracle_threads": threads, "oracle_s": round(time.perf_counter() - t0, 1)}
+
+
+def run_packer(args, cr, ctx, torch, dist):
+    """The 63-bit packer at --pack-points points (seed 0xC0FFEE03): GPU-synthesised
+    16-byte records packed with 21 bits per axis (64-bit keys, 32-bit index) into
+    10,240-point batches, timed with CUDA events (mean of 3 packs after one).  The
+    result is checked by size-independent invariants: point count, colour
+    checksum, per-batch level counts against the cumulative LOD words, and every
+    decoded point of 64 seeded batches inside its batch AABB.  (Bit-exact parity
+    with the CPU pack at smaller sizes is a GPU test.)"""
+    n = args.pack_points
+    ppb = 10240
+    params = cr.TerrainParams(seed=0xC0FFEE03)
+    recs = cr.synth_terrain(ctx, params, n)
+    cloud = cr.ComputeRasteriserPointCloud(ctx, cr.ComputeRasteriserCapacity((n + ppb - 1) // ppb,
+                                                                             ppb))
+    packer = cr.GPUPacker(ctx, mortonBits=21)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=f"cuda:{dist.local}")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    packer.pack(records=recs, into=cloud)
+    ctx.synchronize()
+    reps = 3
+    ev0.record(stream)
+    for _ in range(reps):
+        packer.pack(records=recs, into=cloud)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / reps
+    # Colour checksums (sum and sum of squares, modulo 2^64) of the input on
+    # the device, and of the packed pool read back in 10M-point chunks.
+    mask = (1 << 64) - 1
+    rc = torch.as_tensor(recs, device=f"cuda:{dist.local}")[:, 3].contiguous()
+    rc = rc.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
+    in_sum, in_sq = int(rc.sum().item()) & mask, int((rc * rc).sum().item()) & mask
+    del rc
+    recs.close()
+    ctx.trim()
+    b = cloud.batches()
+    res = b[b["state"] != 0]
+    checks = {"points": int(res["numPoints"].astype(np.int64).sum()) == n}
+    cap = cloud.capacity.maxResidentPoints
+    out_sum = out_sq = 0
+    for first in range(0, cap, 10_000_000):
+        m = min(10_000_000, cap - first)
+        col = cloud.points(first, m)["colors"].astype(np.uint64)
+        idx = np.arange(first, first + m, dtype=np.int64)
+        slot = idx // ppb
+        valid = (b["state"][slot] != 0) & (idx - b["firstPoint"][slot] < b["numPoints"][slot])
+        c = col[valid]
+        out_sum = (out_sum + int(c.sum())) & mask
+        out_sq = (out_sq + int((c * c).sum())) & mask
+    checks["colour_checksum"] = bool(in_sum == out_sum and in_sq == out_sq)
+    rng = np.random.default_rng(3)
+    lod_ok = aabb_ok = True
+    for i in rng.choice(len(res), min(64, len(res)), replace=False):
+        f, c = int(res["firstPoint"][i]), int(res["numPoints"][i])
+        lv = cloud.points(f, c)["levels"] & 7
+        cum = []
+        for w in ("lodCum01", "lodCum23", "lodCum45", "lodCum67"):
+            cum += [int(res[w][i]) & 0xFFFF, int(res[w][i]) >> 16]
+        lod_ok &= all(cum[L] == int((lv <= L).sum()) for L in range(8))
+        p = decoded_positions(cloud, f, c)
+        for a, (mn, mx) in enumerate((("minX", "maxX"), ("minY", "maxY"), ("minZ", "maxZ"))):
+            aabb_ok &= bool((p[:, a] >= res[mn][i] - 1e-3).all() and
+                            (p[:, a] <= res[mx][i] + 1e-3).all())
+    checks["lod_cumulative_counts"] = bool(lod_ok)
+    checks["points_inside_batch_aabb"] = bool(aabb_ok)
+    cloud.close()
+    ctx.trim()
+    return {"points": n, "morton_bits": 63, "batches": int(len(res)),
+            "pack_ms": round(ms, 2), "gpts_per_s": round(n / (ms / 1e3) / 1e9, 3),
+            "checks": checks, "timing": "CUDA events, mean of 3 packs after one warm-up pack"}
 
 
 MV_SIZES = ((256, 256), (512, 512), (1280, 720), (1920, 1080))
