@@ -542,17 +542,39 @@ __device__ __forceinline__ void color_quad(const RasterArgs &a, const ViewRegsT<
         closest[i] = 0u;
         if ((uint32_t)i < nvalid) closest[i] = in[i] ? sdep[l[i]] : __ldg(vdepth<MV>(vr) + pix[i]);
     }
+    // Consecutive visible fragments of the quad on the same pixel (neighbour
+    // points of a Morton-ordered batch often share one) are summed in
+    // registers and added once: fewer adds to a contended address.
+    uint32_t rr = 0, gg = 0, bb = 0, nn = 0, cur = 0xffffffffu;
+    bool cin = false;
+    int cl = 0;
+    auto flush = [&]() {
+        if (nn == 0u) return;
+        if (cin) {
+            atomicAdd(acc + cl, rr | (nn << 20));
+            atomicAdd(acc + kPx + cl, gg);
+            atomicAdd(acc + 2 * kPx + cl, bb);
+        } else {
+            color_global<MV>(a, vr, cur, rr, gg, bb, nn);
+        }
+    };
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const bool vis = closest[i] != 0u && nz[i] >= crd::uint_to_depth(closest[i]) * a.keep_scale;
-        const uint32_t r = col[i] & 0xffu, g = (col[i] >> 8) & 0xffu, b = (col[i] >> 16) & 0xffu;
-        if (vis && in[i]) {
-            atomicAdd(acc + l[i], r | (1u << 20));
-            atomicAdd(acc + kPx + l[i], g);
-            atomicAdd(acc + 2 * kPx + l[i], b);
+        if (!vis) continue;
+        if (pix[i] != cur) {
+            flush();
+            cur = pix[i];
+            cin = in[i];
+            cl = l[i];
+            rr = gg = bb = nn = 0u;
         }
-        if (vis && !in[i]) color_global<MV>(a, vr, pix[i], r, g, b, 1u);
+        rr += col[i] & 0xffu;
+        gg += (col[i] >> 8) & 0xffu;
+        bb += (col[i] >> 16) & 0xffu;
+        nn += 1u;
     }
+    flush();
 }
 
 template <int PASS, bool MV>
@@ -857,6 +879,59 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
     cp_async_wait_all();
 }
 
+
+// Colour pass over the depth pass's fragments for one view: one warp per work
+// item of up to kSegFrags fragments of one chunk (chunk k, segment s).
+// Warps run independently — no block barrier, no shared memory — and a lane
+// loads its four quads (128 fragments apart) before reading their pixels'
+// depths, so each SM keeps many loads in flight; runs of same-pixel
+// fragments within a quad are merged (color_quad).
+constexpr uint32_t kSegFrags = 512;
+
+__global__ void __launch_bounds__(kThreads) color_frags_kernel(RasterArgs a, uint32_t segs) {
+    if (a.t.redo && *a.t.redo == 0u) return;
+    constexpr uint32_t kWarps = kThreads / 32;
+    const uint32_t nitems = a.counters[CNT_CHUNKS] * segs;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = gridDim.x * kWarps;
+    const ViewRegsT<false> vr(a);
+    const ChunkRec no_tile{};  // color_quad without a screen tile
+    for (uint32_t it = blockIdx.x * kWarps + (threadIdx.x >> 5); it < nitems; it += nwarps) {
+        const uint32_t k = it / segs, s = it - k * segs;
+        const uint32_t n = __ldg(a.frag_count + k);
+        const uint32_t lo = s * kSegFrags;
+        if (lo >= n) continue;  // warp-uniform
+        const uint32_t cnt = min(n - lo, kSegFrags);
+        const uint32_t base = __ldg(&a.chunks[k].first) + lo;
+        if ((base & 3u) == 0u) {
+            uint4 xy[4], co[4];
+            float4 z[4];
+            uint32_t nv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t f = 128u * j + 4u * lane;
+                nv[j] = f < cnt ? min(4u, cnt - f) : 0u;
+                xy[j] = co[j] = make_uint4(0, 0, 0, 0);
+                z[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (nv[j]) {
+                    xy[j] = __ldcs(reinterpret_cast<const uint4 *>(a.frag_xy + base + f));
+                    z[j] = __ldcs(reinterpret_cast<const float4 *>(a.frag_z + base + f));
+                    co[j] = __ldcs(reinterpret_cast<const uint4 *>(a.frag_col + base + f));
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                color_quad<false>(a, vr, nullptr, no_tile, false, nv[j], xy[j], z[j], co[j]);
+        } else {
+            // Unaligned start (pointsPerBatch not a multiple of 4): one
+            // fragment per lane.
+            for (uint32_t f = lane; f < cnt; f += 32u)
+                do_fragment<false>(a, vr, nullptr, no_tile, false, true, a.frag_xy[base + f],
+                                   a.frag_z[base + f], a.frag_col[base + f]);
+        }
+    }
+}
+
 template <int PASS, bool MV>
 __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
     raster_body<PASS, MV>(a);
@@ -916,7 +991,14 @@ int raster_blocks_per_sm(int pass) {
     case PASS_COLOR: return blocks_per_sm_for<PASS_COLOR, MV>();
     case PASS_DEPTH_FRAG: return blocks_per_sm_for<PASS_DEPTH_FRAG, MV>();
     case PASS_COLOR_FRAG:
-        return MV ? color_views_blocks_per_sm() : blocks_per_sm_for<PASS_COLOR_FRAG, false>();
+        if (MV) return color_views_blocks_per_sm();
+        {
+            int n = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, color_frags_kernel, kThreads, 0) !=
+                cudaSuccess)
+                n = 1;
+            return n < 1 ? 1 : n;
+        }
     default:
         if constexpr (MV)
             return 1;  // batched views draw HQS only
@@ -976,7 +1058,15 @@ cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &
     case PASS_DEPTH: launch_pass<PASS_DEPTH, false>(a, grid, s); break;
     case PASS_COLOR: launch_pass<PASS_COLOR, false>(a, grid, s); break;
     case PASS_DEPTH_FRAG: launch_pass<PASS_DEPTH_FRAG, false>(a, grid, s); break;
-    case PASS_COLOR_FRAG: launch_pass<PASS_COLOR_FRAG, false>(a, grid, s); break;
+    case PASS_COLOR_FRAG: {
+        // Work items of kSegFrags fragments; a chunk holds at most chunkPoints
+        // points, and at most one batch's.
+        const uint32_t cp = (uint32_t)std::max(ctx->chunk_points, kMinChunkPoints);
+        const uint32_t per = std::min<uint32_t>(cp, cloud->cap.pointsPerBatch);
+        const uint32_t segs = std::max<uint32_t>(1u, (per + kSegFrags - 1) / kSegFrags);
+        color_frags_kernel<<<grid, kThreads, 0, s>>>(a, segs);
+        break;
+    }
     default: launch_pass<PASS_NEAREST, false>(a, grid, s); break;
     }
     CR_CUDA(cudaGetLastError());
