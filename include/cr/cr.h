@@ -292,6 +292,17 @@ CR_API cr_status cr_frame_read_depth_f32(cr_frame *frame, float *out /* w*h */);
 CR_API cr_status cr_frame_read_pixels(cr_frame *frame, cr_raster_pixel *out /* w*h */);
 CR_API cr_status cr_frame_read_nearest_depth(cr_frame *frame, uint32_t *out /* w*h */);
 CR_API cr_status cr_frame_read_nearest_index(cr_frame *frame, uint32_t *out /* w*h */);
+/* Asynchronous read-back of the final RGBA8 image: enqueues its copy into
+ * `out` (w*h*4 bytes; page-locked host memory keeps the copy asynchronous) on
+ * the context's copy stream, after the work enqueued so far, and returns at
+ * once.  The next render into the frame waits on the device for the copy
+ * before it rewrites the image (at its resolve), so the copy overlaps that
+ * render's cull, depth and colour passes.  `out` holds the image once
+ * cr_frame_read_wait (or cr_context_synchronize) returns.  No counterpart in
+ * the reference, whose output is a Metal texture the caller blits itself. */
+CR_API cr_status cr_frame_read_rgba8_async(cr_frame *frame, uint8_t *out /* w*h*4 */);
+/* Waits for the frame's enqueued asynchronous read-backs. */
+CR_API cr_status cr_frame_read_wait(cr_frame *frame);
 /* Rows [row0, row0+nrows) of the nearest index plane (pick band read-back). */
 CR_API cr_status cr_frame_read_nearest_index_rows(cr_frame *frame, int row0, int nrows,
                                                   uint32_t *out);

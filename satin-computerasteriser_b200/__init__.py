@@ -628,6 +628,7 @@ class _Frame:
         self.context = context
         self.width, self.height = width, height
         self._h = C.c_void_p()
+        self._pending = []  # host arrays of enqueued asynchronous read-backs
         N.check(N.lib().cr_frame_create(context.handle, width, height, C.byref(self._h)))
 
     @property
@@ -653,6 +654,19 @@ class _Frame:
             raise CRError(1, "out is too small or not contiguous")
         N.check(N.lib().cr_frame_read_rgba8(self._h, N.ptr(out)))
         return out
+
+    def rgba8_async(self, out: np.ndarray) -> np.ndarray:
+        """Enqueues the RGBA8 read-back into `out` and returns at once; the
+        array is held until wait()."""
+        if out.nbytes < self.width * self.height * 4 or not out.flags.c_contiguous:
+            raise CRError(1, "out is too small or not contiguous")
+        N.check(N.lib().cr_frame_read_rgba8_async(self._h, N.ptr(out)))
+        self._pending.append(out)
+        return out
+
+    def wait(self):
+        N.check(N.lib().cr_frame_read_wait(self._h))
+        self._pending.clear()
 
     def depth_f32(self) -> np.ndarray:
         out = np.zeros((self.height, self.width), np.float32)
@@ -807,6 +821,19 @@ class ComputeRasteriser:
             raise CRError(1, "out is too small or not contiguous")
         N.check(N.lib().cr_frame_read_rgba8(f.handle, N.ptr(out)))
         return out
+
+    def outputRGBA8Async(self, out: np.ndarray) -> np.ndarray:
+        """Enqueues the read-back of the final RGBA8 image into `out` (page-locked
+        host memory, e.g. HostBuffer((h, w, 4), np.uint8).array, for the copy
+        to be asynchronous) and returns at once; `out` holds the image after
+        waitOutput().  The next encode() into this frame waits on the device
+        for the copy before its resolve rewrites the image, so a render loop
+        that reads every frame keeps the GPU busy while the images travel."""
+        return self._require_frame().rgba8_async(out)
+
+    def waitOutput(self):
+        """Waits for every read-back enqueued by outputRGBA8Async."""
+        self._require_frame().wait()
 
     def depthTexture(self) -> np.ndarray:
         f = self._require_frame()

@@ -117,6 +117,8 @@ PROTOTYPES = {
     "cr_frame_destroy": (C.c_int, [P]),
     "cr_render": (C.c_int, [P, P, P, u32, C.POINTER(cr_config), C.POINTER(cr_camera)]),
     "cr_frame_read_rgba8": (C.c_int, [P, P]),
+    "cr_frame_read_rgba8_async": (C.c_int, [P, P]),
+    "cr_frame_read_wait": (C.c_int, [P]),
     "cr_frame_read_depth_f32": (C.c_int, [P, P]),
     "cr_frame_read_pixels": (C.c_int, [P, P]),
     "cr_frame_read_nearest_depth": (C.c_int, [P, P]),

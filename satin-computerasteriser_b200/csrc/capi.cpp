@@ -315,6 +315,13 @@ cr_status validate_config(const cr_config *cfg) {
 // ===========================================================================
 // Exported API
 // ===========================================================================
+cr_status frame_copy_fence(cr_frame *f, cudaStream_t s) {
+    if (!f->copy_pending) return CR_OK;
+    CR_CUDA(cudaStreamWaitEvent(s, f->ev_copied, 0));
+    f->copy_pending = false;  // later work on `s` is ordered after the wait
+    return CR_OK;
+}
+
 extern "C" {
 
 CR_API const char *cr_status_string(cr_status s) {
@@ -407,6 +414,10 @@ CR_API cr_status cr_context_destroy(cr_context *ctx) {
     }
     if (ctx->views) views_destroy(ctx->views);
     if (ctx->d_loss) cudaFree(ctx->d_loss);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CR_OK;
@@ -416,6 +427,7 @@ CR_API cr_status cr_context_synchronize(cr_context *ctx) {
     if (!ctx) return fail(CR_ERR_INVALID_ARGUMENT, "ctx is null");
     DeviceGuard g(ctx->device);
     CR_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->copy_stream) CR_CUDA(cudaStreamSynchronize(ctx->copy_stream));
     return CR_OK;
 }
 
@@ -741,6 +753,11 @@ CR_API cr_status cr_frame_destroy(cr_frame *f) {
     if (!f) return CR_OK;
     DeviceGuard g(f->ctx->device);
     cudaStreamSynchronize(f->ctx->stream);
+    if (f->ev_copied) {
+        cudaEventSynchronize(f->ev_copied);
+        cudaEventDestroy(f->ev_copied);
+    }
+    if (f->ev_rendered) cudaEventDestroy(f->ev_rendered);
     dfree(f->d_depth);
     dfree(f->d_accum);
     dfree(f->d_nearest);
@@ -818,6 +835,7 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
         }
         {
             PassTimer pt(ctx, CR_PASS_RESOLVE);
+            if ((st = frame_copy_fence(f, s))) return st;
             if ((st = launch_resolve_hqs(f, ru, s, packed, nullptr))) return st;
             if (packed) {
                 // Exact re-run, which returns at once unless the resolve set
@@ -857,6 +875,7 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
             }
             {
                 PassTimer pt(ctx, CR_PASS_RESOLVE);
+                if ((st = frame_copy_fence(f, s))) return st;
                 if ((st = launch_resolve_nearest(f, first->d_colors, ru, s))) return st;
             }
             f->last_mode = 1;
@@ -867,6 +886,7 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
     f->final_rgba = 0;
     if (cfg->holeFillIterations > 0) {
         PassTimer pt(ctx, CR_PASS_HOLE_FILL);
+        if ((st = frame_copy_fence(f, s))) return st;
         return launch_hole_fill(f, cfg->holeFillIterations, s);
     }
     return CR_OK;
@@ -883,6 +903,31 @@ static cr_status read_plane(cr_frame *f, void *out, const void *src, size_t byte
 CR_API cr_status cr_frame_read_rgba8(cr_frame *f, uint8_t *out) {
     if (!f) return fail(CR_ERR_INVALID_ARGUMENT, "frame is null");
     return read_plane(f, out, f->d_rgba[f->final_rgba], (size_t)f->width * f->height * 4);
+}
+
+CR_API cr_status cr_frame_read_rgba8_async(cr_frame *f, uint8_t *out) {
+    if (!f || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    cr_context *ctx = f->ctx;
+    DeviceGuard g(ctx->device);
+    if (!ctx->copy_stream)
+        CR_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    if (!f->ev_rendered) CR_CUDA(cudaEventCreateWithFlags(&f->ev_rendered, cudaEventDisableTiming));
+    if (!f->ev_copied) CR_CUDA(cudaEventCreateWithFlags(&f->ev_copied, cudaEventDisableTiming));
+    CR_CUDA(cudaEventRecord(f->ev_rendered, ctx->stream));
+    CR_CUDA(cudaStreamWaitEvent(ctx->copy_stream, f->ev_rendered, 0));
+    CR_CUDA(cudaMemcpyAsync(out, f->d_rgba[f->final_rgba], (size_t)f->width * f->height * 4,
+                            cudaMemcpyDeviceToHost, ctx->copy_stream));
+    CR_CUDA(cudaEventRecord(f->ev_copied, ctx->copy_stream));
+    f->copy_pending = true;
+    return CR_OK;
+}
+
+CR_API cr_status cr_frame_read_wait(cr_frame *f) {
+    if (!f) return fail(CR_ERR_INVALID_ARGUMENT, "frame is null");
+    if (!f->ev_copied) return CR_OK;
+    DeviceGuard g(f->ctx->device);
+    CR_CUDA(cudaEventSynchronize(f->ev_copied));
+    return CR_OK;
 }
 
 CR_API cr_status cr_frame_read_depth_f32(cr_frame *f, float *out) {

@@ -79,6 +79,7 @@ struct cr_context {
     double *d_loss = nullptr;     // cr_l2_loss's device accumulator (lazy)
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // asynchronous RGBA8 read-backs (lazy)
     int sm_count = 0;
     int blocks_per_sm[7] = {};        // occupancy of the persistent point passes (per RasterPass)
     int blocks_per_sm_views[7] = {};  // the same, batched-view kernels
@@ -164,7 +165,16 @@ struct cr_frame {
     uint32_t *d_fcount = nullptr;           //   and their sample counts
     int final_rgba = 0;                     // which d_rgba holds the final image
     int last_mode = -1;                     // 0 HQS, 1 nearest, -1 none
+    // Asynchronous read-back: `rendered` is recorded on the context stream
+    // and waited on by the copy stream; `copied` is recorded after the copy
+    // and waited on by the next write of the RGBA8 planes.
+    cudaEvent_t ev_rendered = nullptr, ev_copied = nullptr;
+    bool copy_pending = false;
 };
+
+// Makes later work on `s` wait (on the device) for the frame's enqueued
+// asynchronous read-backs; call before the first write of the RGBA8 planes.
+cr_status frame_copy_fence(cr_frame *f, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Kernel launch interfaces

@@ -561,6 +561,10 @@ CR_API cr_status cr_render_multiview(cr_context *ctx, cr_frame *const *frames,
     if (s->launched[b]) CR_CUDA(cudaEventSynchronize(s->done[b]));
     views_fill(s, b, frames, cams, resident.data(), rmodels.data(), nres, cfg,
                (uint32_t)std::max(ctx->chunk_points, kMinChunkPoints));
+    for (uint32_t v = 0; v < nviews; ++v) {
+        cr_status fe = frame_copy_fence(frames[v], ctx->stream);
+        if (fe) return fe;
+    }
     CR_CUDA(cudaGraphLaunch(s->exec[b], ctx->stream));
     CR_CUDA(cudaEventRecord(s->done[b], ctx->stream));
     s->launched[b] = true;
