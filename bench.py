@@ -79,26 +79,52 @@ def parse_args():
                     help="points whose gradient is checked against the FP64 oracle (0 = none)")
     ap.add_argument("--pack-points", type=int, default=400_000_000,
                     help="points of the 63-bit packer leg (0 = skip it)")
+    ap.add_argument("--shard", default="frames", choices=["frames", "points"],
+                    help="N>1: every rank renders its own frames of its own copy of the cloud "
+                         "(frames, weak scaling), or every frame is split by batches over the "
+                         "ranks with a depth max and a colour sum all-reduce (points, strong "
+                         "scaling)")
     return ap.parse_args()
 
 
 # ---------------------------------------------------------------------------
 # Multi-process plumbing
 # ---------------------------------------------------------------------------
+def pose_order(rank: int, world: int, n: int, poses: int) -> list:
+    """The poses rank `rank` renders, in order: ranks interleave over the pose
+    list, so each renders its own frames (weak scaling)."""
+    return [(rank + world * k) % poses for k in range(n)]
+
+
 class Dist:
-    def __init__(self):
+    """Ranks from the torchrun environment; NCCL on GPUs (one per rank), gloo
+    for the CPU tests of the multi-rank helpers."""
+
+    def __init__(self, backend: str = "nccl", group_of_one: bool = False):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = None
-        if self.world > 1:
+        if self.world > 1 or group_of_one:
+            if self.world == 1:  # a process group of one rank (frames split by points)
+                os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+                if "MASTER_PORT" not in os.environ:
+                    import socket
+                    with socket.socket() as sk:
+                        sk.bind(("127.0.0.1", 0))
+                        os.environ["MASTER_PORT"] = str(sk.getsockname()[1])
+                os.environ.setdefault("RANK", "0")
+                os.environ.setdefault("WORLD_SIZE", "1")
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local))
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                kw["device_id"] = torch.device("cuda", self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
             self.pg = dist
 
     def barrier(self):
@@ -109,7 +135,8 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -326,7 +353,7 @@ def config_dict(args):
                         "_heightfield",
             "points": args.points, "width": args.width, "height": args.height,
             "poses": args.poses, "points_per_batch": 10240, "morton_bits": 30,
-            "mode": args.mode,
+            "mode": args.mode, "shard": args.shard,
             "l2": "inputs larger than L2 (1.7 GB resident slot pool per 100M points)"}
 
 
@@ -348,7 +375,23 @@ def run_ours(args, dist):
     ras.addPointCloud(cloud)
     ras.resize((W, H))
     cams = make_poses(cr, params, args.poses, args.seed, W / H)
-    order = [(dist.rank + dist.world * k) % args.poses for k in range(args.warmup + args.steps)]
+    frame_encoder = ras
+    if args.shard == "points":
+        if args.mode != "hqs":
+            raise SystemExit("--shard points needs --mode hqs")
+        # Every rank keeps its contiguous part of the batches (slot layout and
+        # point indices as in the whole cloud) and renders every frame; the
+        # planes are combined over NCCL between the stages.
+        sharded = importlib.import_module("satin-computerasteriser_b200.sharded")
+        nb = cloud.residentBatchCount
+        lo, hi = sharded.shard_range(nb, dist.rank, dist.world)
+        drop = [b for b in range(nb) if not lo <= b < hi]
+        if drop:
+            cloud.removeBatches(drop)
+        frame_encoder = sharded.PointShardedRasteriser(ras)
+        order = pose_order(0, 1, args.warmup + args.steps, args.poses)
+    else:
+        order = pose_order(dist.rank, dist.world, args.warmup + args.steps, args.poses)
 
     # Survivor lists of every pose (untimed) for the algorithmic byte counts.
     pose_bytes = {}
@@ -358,7 +401,7 @@ def run_ours(args, dist):
         pose_bytes[p] = pass_bytes(cloud.visibleBatches())
     for k in range(args.warmup):
         ras.update(cams[order[k]])
-        ras.encode()
+        frame_encoder.encode()
     ctx.synchronize()
 
     stream = torch.cuda.ExternalStream(ctx.stream(), device=f"cuda:{dist.local}")
@@ -374,7 +417,7 @@ def run_ours(args, dist):
     ev0.record(stream)
     for p in timed:
         ras.update(cams[p])
-        ras.encode()
+        frame_encoder.encode()
     ev1.record(stream)
     ev1.synchronize()
     sampler.end()
@@ -385,7 +428,10 @@ def run_ours(args, dist):
     times = ctx.pass_times(len(timed))
     ctx.set_profiling(False)
     ms_max = dist.max(ms)
-    value = dist.world * args.points * args.steps / (ms_max / 1e3) / 1e9
+    # Points drawn per frame by all ranks: their own frames' clouds (frames),
+    # or one cloud split over them (points).
+    units = args.points * (dist.world if args.shard == "frames" else 1)
+    value = units * args.steps / (ms_max / 1e3) / 1e9
 
     # Dominant pass and its roofline.
     avg = times.mean(axis=0)
@@ -419,7 +465,7 @@ def run_ours(args, dist):
     t0 = time.perf_counter()
     for k, p in enumerate(timed):
         ras.update(cams[p])
-        ras.encode()
+        frame_encoder.encode()
         ras.waitOutput()
         ras.outputRGBA8Async(pinned[k & 1].array)
     ras.waitOutput()
@@ -432,29 +478,32 @@ def run_ours(args, dist):
     t0 = time.perf_counter()
     for p in timed:
         ras.update(cams[p])
-        ras.encode()
+        frame_encoder.encode()
         ras.outputRGBA8(out=pinned[0].array)
     blocking_max = dist.max(time.perf_counter() - t0)
-    e2e = {"value": round(dist.world * args.points * args.steps / e2e_max / 1e9, 4),
+    e2e = {"value": round(units * args.steps / e2e_max / 1e9, 4),
            "unit": "Gpts/s", "h2d_bytes_per_step": 256, "d2h_bytes_per_step": W * H * 4,
            "ms_per_step": round(e2e_max * 1e3 / args.steps, 4),
            "readback": "asynchronous, overlapped with the next frame (2 pinned buffers)",
            "last_image_matches_blocking_read": last_ok,
            "blocking_readback": {
-               "value": round(dist.world * args.points * args.steps / blocking_max / 1e9, 4),
+               "value": round(units * args.steps / blocking_max / 1e9, 4),
                "ms_per_step": round(blocking_max * 1e3 / args.steps, 4)}}
 
     out = {"metric": METRIC, "value": round(value, 4), "unit": "Gpts/s", "n_gpus": dist.world,
            "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f32+u32",
+           "scaling": "weak" if args.shard == "frames" else "strong",
+           "vs_baseline": None, "dtype": "f32+u32",
            "data": "synthetic (seeded fractal heightfield, generated and packed on the GPU)",
            "config": config_dict(args), "e2e": e2e, "roofline": roofline, "clocks": clocks,
            # HQS: cull (classify, compact), depth, colour, resolve, and the
            # exact re-run's clear, colour and resolve, which return at once
            # unless a pixel passed 16,843,009 samples; nearest: cull (2),
            # nearest pass, resolve.
-           "gpu_launches": int(args.steps * (8 if args.mode == "hqs" else 4)),
+           # (+ 2 depth-order flips per frame split by points)
+           "gpu_launches": int(args.steps * ((8 if args.mode == "hqs" else 4) +
+                                             (2 if args.shard == "points" else 0))),
            "pass_ms": {n: round(float(v), 4) for n, v in zip(PASS_NAMES, avg)},
            "survivor_points_per_frame": int(active.mean()),
            "tuning": ctx.tuning(),
@@ -869,7 +918,7 @@ def run_reference(args, dist):
 
 def main():
     args = parse_args()
-    dist = Dist()
+    dist = Dist(group_of_one=args.shard == "points" and args.impl == "ours")
     try:
         out = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
         if out is not None and dist.rank == 0:

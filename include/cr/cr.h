@@ -286,6 +286,51 @@ CR_API cr_status cr_frame_destroy(cr_frame *frame);
 CR_API cr_status cr_render(cr_context *ctx, cr_frame *frame, cr_cloud *const *clouds,
                            uint32_t nclouds, const cr_config *config, const cr_camera *camera);
 
+/* The HQS passes as stages, for a frame whose points are split over several
+ * frames (one per GPU, each holding a part of the batches): every part runs
+ * CR_STAGE_DEPTH; the depth planes are combined by an element-wise maximum
+ * (an all-reduce); every part runs CR_STAGE_COLOR against the combined
+ * depth; the R, G, B, count planes are summed; CR_STAGE_RESOLVE produces the
+ * image.  Integer max and sum are order-independent, so the image is
+ * bit-identical to one cr_render of all the batches.
+ *   CR_STAGE_DEPTH    clear depth and accumulators, cull, depth pass
+ *   CR_STAGE_COLOR    colour pass against the frame's depth plane
+ *   CR_STAGE_RESOLVE  resolve and hole fill
+ * The clouds, their file tables and the configuration must not change
+ * between the stage calls of one frame (the depth stage leaves the cull
+ * results and fragments in the clouds).  A colour stage whose resolve runs in
+ * another call adds each field with a 32-bit add (exact up to 2^32 - 1 per
+ * field), so that accumulators of several frames can be summed; one call
+ * with both stages uses the packed adds of cr_render.  HQS only: separate
+ * stages of the nearest mode return CR_ERR_UNSUPPORTED.  cr_render is
+ * cr_render_stages(..., CR_STAGE_ALL).  No counterpart in the reference. */
+typedef enum cr_stage {
+    CR_STAGE_DEPTH = 1,
+    CR_STAGE_COLOR = 2,
+    CR_STAGE_RESOLVE = 4,
+    CR_STAGE_ALL = 7
+} cr_stage;
+CR_API cr_status cr_render_stages(cr_context *ctx, cr_frame *frame, cr_cloud *const *clouds,
+                                  uint32_t nclouds, const cr_config *config,
+                                  const cr_camera *camera, uint32_t stages);
+
+/* Device planes of a frame, for combining frames between stages with a
+ * collective library: depth is `pixels` uint32 (reverse-Z, larger is
+ * nearer), accum is `pixels` x {R, G, B, count} uint32.  `stream` is the
+ * context's cudaStream_t; work on the planes must be ordered with it. */
+typedef struct cr_frame_planes {
+    void *depth;
+    void *accum;
+    uint64_t pixels;
+    void *stream;
+} cr_frame_planes;
+CR_API cr_status cr_frame_device_planes(cr_frame *frame, cr_frame_planes *out);
+
+/* XORs the top bit of every depth word (enqueued on the context stream):
+ * maps the unsigned order of the depth plane onto the signed order of int32
+ * and back, for collectives that reduce signed 32-bit integers only. */
+CR_API cr_status cr_frame_flip_depth_order(cr_frame *frame);
+
 /* Read-backs (synchronise the context stream). */
 CR_API cr_status cr_frame_read_rgba8(cr_frame *frame, uint8_t *out /* w*h*4 */);
 CR_API cr_status cr_frame_read_depth_f32(cr_frame *frame, float *out /* w*h */);

@@ -102,6 +102,9 @@ def _load():
     lib.orc_render.argtypes = [C.POINTER(orc_cloud), C.c_uint32, C.POINTER(orc_config), P, P,
                                C.c_int, C.c_int, P, P, P, P, P, P, P, C.c_uint32, P, C.c_int]
     lib.orc_hole_fill.argtypes = [P, C.c_int, C.c_int, C.c_int]
+    lib.orc_hqs_stage.restype = C.c_int
+    lib.orc_hqs_stage.argtypes = [C.POINTER(orc_cloud), C.c_uint32, C.POINTER(orc_config), P, P,
+                                  C.c_int, C.c_int, C.c_uint32, P, P, P, P, C.c_int]
     lib.orc_hqs_grad_f64.restype = C.c_int
     lib.orc_hqs_grad_f64.argtypes = [C.POINTER(orc_cloud), C.POINTER(orc_config), P, P,
                                      C.c_int, C.c_int, P, P, C.c_double, P, P, P, P,
@@ -350,6 +353,32 @@ def render(clouds, cfg: Config, view, proj, width: int, height: int, threads: in
     return Frame(rgba.reshape(height, width, 4), depthf.reshape(height, width),
                  depth.reshape(height, width), accum.reshape(height, width, 4),
                  nd.reshape(height, width), ni.reshape(height, width), visible, rc)
+
+
+def hqs_stage(clouds, cfg: Config, view, proj, width: int, height: int, stage: int,
+              depth: np.ndarray, accum: np.ndarray, rgba: np.ndarray | None = None,
+              depthf: np.ndarray | None = None, threads: int = 1) -> None:
+    """One HQS stage of a frame split by points (cr_render_stages): 1 = clear,
+    cull and depth pass into depth (uint32[h*w]); 2 = cull and colour pass
+    against depth, added into accum (uint32[h*w*4]); 4 = resolve and hole fill
+    into rgba (uint8[h*w*4]) and depthf (float32[h*w]).  The arrays must be
+    C-contiguous and are written in place."""
+    if isinstance(clouds, Cloud):
+        clouds = [clouds]
+    for a, dt, n in ((depth, np.uint32, width * height), (accum, np.uint32, width * height * 4)):
+        if a.dtype != dt or a.size != n or not a.flags.c_contiguous:
+            raise ValueError("depth / accum: wrong dtype, size or layout")
+    ccs = (orc_cloud * max(len(clouds), 1))()
+    for i, cl in enumerate(clouds):
+        ccs[i] = cl.to_c()
+    c = cfg.to_c()
+    v, p = _mat(view), _mat(proj)
+    rc = _load().orc_hqs_stage(ccs, len(clouds), C.byref(c), _ptr(v), _ptr(p), width, height,
+                               stage, _ptr(depth), _ptr(accum),
+                               None if rgba is None else _ptr(rgba),
+                               None if depthf is None else _ptr(depthf), threads)
+    if rc != 0:
+        raise ValueError(f"orc_hqs_stage failed ({rc})")
 
 
 def hqs_grad_f64(cloud: Cloud, cfg: Config, view, proj, width: int, height: int, colors,

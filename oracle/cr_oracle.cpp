@@ -454,6 +454,29 @@ inline uint8_t unorm8(float f) {
     return (uint8_t)std::nearbyint(x);
 }
 
+// resolveUpdate (Resolve/Shaders.metal:13-57), count path.
+void resolve_hqs(const uint32_t *depth, const uint32_t *accum, size_t npix, const float *bg,
+                 uint8_t *img, float *dimg) {
+    for (size_t p = 0; p < npix; ++p) {
+        const uint32_t cnt = accum[p * 4 + 3];
+        uint8_t *o = &img[p * 4];
+        if (cnt == 0u) {
+            o[0] = unorm8(bg[0]);
+            o[1] = unorm8(bg[1]);
+            o[2] = unorm8(bg[2]);
+            o[3] = unorm8(0.0f);
+            dimg[p] = 0.0f;
+            continue;
+        }
+        const float inv = 1.0f / u2f(cnt);
+        o[0] = unorm8((u2f(accum[p * 4 + 0]) * inv) / 255.0f);
+        o[1] = unorm8((u2f(accum[p * 4 + 1]) * inv) / 255.0f);
+        o[2] = unorm8((u2f(accum[p * 4 + 2]) * inv) / 255.0f);
+        o[3] = unorm8(1.0f);
+        dimg[p] = uint_to_depth(depth[p]);
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -582,25 +605,7 @@ int orc_render(const orc_cloud *clouds, uint32_t nclouds, const orc_config *cfg,
                         depth.data(), accum.data(), nullptr};
             run_pass(a, PASS_COLOR, threads);
         }
-        // resolveUpdate (Resolve/Shaders.metal:13-57), count path.
-        for (size_t p = 0; p < npix; ++p) {
-            const uint32_t cnt = accum[p * 4 + 3];
-            uint8_t *o = &img[p * 4];
-            if (cnt == 0u) {
-                o[0] = unorm8(bg[0]);
-                o[1] = unorm8(bg[1]);
-                o[2] = unorm8(bg[2]);
-                o[3] = unorm8(0.0f);
-                dimg[p] = 0.0f;
-                continue;
-            }
-            const float inv = 1.0f / u2f(cnt);
-            o[0] = unorm8((u2f(accum[p * 4 + 0]) * inv) / 255.0f);
-            o[1] = unorm8((u2f(accum[p * 4 + 1]) * inv) / 255.0f);
-            o[2] = unorm8((u2f(accum[p * 4 + 2]) * inv) / 255.0f);
-            o[3] = unorm8(1.0f);
-            dimg[p] = uint_to_depth(depth[p]);
-        }
+        resolve_hqs(depth.data(), accum.data(), npix, bg, img.data(), dimg.data());
         if (depth_out) std::memcpy(depth_out, depth.data(), npix * 4);
         if (accum_out) std::memcpy(accum_out, accum.data(), npix * 16);
     } else {
@@ -655,6 +660,46 @@ int orc_render(const orc_cloud *clouds, uint32_t nclouds, const orc_config *cfg,
         for (uint32_t ci = 0; ci < nclouds; ++ci)
             for (uint32_t k = 0; k < vcount[ci] && k < visible_stride; ++k)
                 visible[(size_t)ci * visible_stride + k] = vis[ci][k];
+    return 0;
+}
+
+// One HQS stage of a frame split by points (cr_render_stages), in the order
+// of encodeHighQualityAverage (ComputeRasteriser.swift:322-456): stage 1
+// clears both planes, culls and runs the depth pass of every resident cloud;
+// stage 2 culls and adds the colour pass of every resident cloud, tested
+// against the given depth plane; stage 4 resolves the planes and hole-fills.
+int orc_hqs_stage(const orc_cloud *clouds, uint32_t nclouds, const orc_config *cfg,
+                  const float view[16], const float proj[16], int w, int h, uint32_t stage,
+                  uint32_t *depth, uint32_t *accum, uint8_t *rgba, float *depthf, int threads) {
+    if (w <= 0 || h <= 0 || cfg->mode != 0) return 1;
+    const size_t npix = (size_t)w * h;
+    auto resident = [&](const orc_cloud &c) {
+        for (uint32_t i = 0; i < c.batchCount; ++i)
+            if (c.batches[i].state != 0) return true;
+        return false;
+    };
+    if (stage == 1 || stage == 2) {
+        if (stage == 1) {
+            std::fill(depth, depth + npix, 0u);
+            std::fill(accum, accum + npix * 4, 0u);
+        }
+        for (uint32_t ci = 0; ci < nclouds; ++ci) {
+            const orc_cloud &c = clouds[ci];
+            if (!resident(c)) continue;
+            std::vector<orc_visible> vis(c.batchCount);
+            const uint32_t n = orc_cull(&c, cfg, view, proj, w, h, vis.data(), c.batchCount);
+            pass_args a{&c, vis.data(), n, cfg, view, proj, w, h, depth, accum, nullptr};
+            run_pass(a, stage == 1 ? PASS_DEPTH : PASS_COLOR, threads);
+        }
+        return 0;
+    }
+    if (stage != 4) return 1;
+    std::vector<uint8_t> img(npix * 4);
+    std::vector<float> dimg(npix, 0.0f);
+    resolve_hqs(depth, accum, npix, cfg->backgroundColor, img.data(), dimg.data());
+    orc_hole_fill(img.data(), w, h, cfg->holeFillIterations);
+    if (rgba) std::memcpy(rgba, img.data(), npix * 4);
+    if (depthf) std::memcpy(depthf, dimg.data(), npix * 4);
     return 0;
 }
 

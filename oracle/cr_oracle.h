@@ -99,6 +99,16 @@ int orc_render(const orc_cloud *clouds, uint32_t nclouds, const orc_config *cfg,
                uint8_t *rgba, float *depthf, orc_visible *visible, uint32_t visible_stride,
                uint32_t *visible_count, int threads);
 
+/* One HQS stage of a frame whose points are split over several frames:
+ * stage 1 = clear depth[w*h] and accum[w*h*4], cull, depth pass; 2 = cull and
+ * colour pass against depth[], added into accum[]; 4 = resolve depth[] and
+ * accum[] and hole fill into rgba / depthf (either may be NULL).  The
+ * clouds' resident batches are the part drawn.  Returns 0 on success. */
+int orc_hqs_stage(const orc_cloud *clouds, uint32_t nclouds, const orc_config *cfg,
+                  const float view[16], const float proj[16], int width, int height,
+                  uint32_t stage, uint32_t *depth, uint32_t *accum, uint8_t *rgba,
+                  float *depthf, int threads);
+
 /* Differentiable HQS colours in FP64 for one view of one cloud (reference of
  * the FP32 forward / adjoint): colors and grad hold 3 doubles per pool point,
  * target and image 3 per pixel (row 0 = top).  loss, grad and fd are added

@@ -31,9 +31,11 @@ __all__ = ["Context", "ComputeRasteriserConfiguration", "ComputeRasteriserCapaci
            "VISIBLE_DTYPE", "computeRasteriserThreadsPerGroup", "MODE_HQS", "MODE_NEAREST",
            "identity_files", "matrix_multiply", "GPUPacker", "PackInput", "DeviceBuffer",
            "HostBuffer", "TerrainParams", "synth_terrain", "synth_lattice", "terrain_height",
-           "PASS_NAMES", "MultiViewRasteriser", "l2_loss"]
+           "PASS_NAMES", "MultiViewRasteriser", "l2_loss", "STAGE_DEPTH", "STAGE_COLOR",
+           "STAGE_RESOLVE", "STAGE_ALL"]
 
 PASS_NAMES = ("clear", "cull", "depth", "color", "resolve", "hole_fill")
+STAGE_DEPTH, STAGE_COLOR, STAGE_RESOLVE, STAGE_ALL = 1, 2, 4, 7  # cr_stage
 
 computeRasteriserThreadsPerGroup = 128
 MODE_HQS = 0      # ComputeRasteriserMode.highQualityAverage
@@ -810,6 +812,36 @@ class ComputeRasteriser:
         cam = _camera_c(self._camera)
         N.check(N.lib().cr_render(self.context.handle, self._frame.handle, arr, len(clouds),
                                   C.byref(cfg), C.byref(cam)))
+
+    def encodeStages(self, stages: int):
+        """Some HQS stages of encode() (cr_render_stages): STAGE_DEPTH (clear,
+        cull, depth pass), STAGE_COLOR (colour pass against the frame's depth
+        plane), STAGE_RESOLVE (resolve, hole fill), or a union of them.  Used
+        to combine several frames' planes between the stages (a frame split
+        by points over GPUs, see sharded.PointShardedRasteriser)."""
+        if not self.visible or self._frame is None or self._camera is None:
+            return
+        clouds = self.visiblePointClouds
+        arr = (C.c_void_p * max(len(clouds), 1))(*[c.handle.value for c in clouds])
+        cfg = self.configuration.to_c()
+        cam = _camera_c(self._camera)
+        N.check(N.lib().cr_render_stages(self.context.handle, self._frame.handle, arr,
+                                         len(clouds), C.byref(cfg), C.byref(cam), int(stages)))
+
+    def devicePlanes(self) -> dict:
+        """Device pointers of the frame's depth plane (uint32 per pixel) and
+        accumulators (uint32 R, G, B, count per pixel), the pixel count and
+        the context's CUDA stream (cr_frame_device_planes)."""
+        f = self._require_frame()
+        pl = N.cr_frame_planes()
+        N.check(N.lib().cr_frame_device_planes(f.handle, C.byref(pl)))
+        return {"depth": pl.depth, "accum": pl.accum, "pixels": int(pl.pixels),
+                "stream": pl.stream or 0, "device": self.context.device}
+
+    def flipDepthOrder(self):
+        """XOR the top bit of every depth word (cr_frame_flip_depth_order):
+        unsigned depth order <-> signed int32 order, around an int32 max."""
+        N.check(N.lib().cr_frame_flip_depth_order(self._require_frame().handle))
 
     # --- outputs (row 0 = top of the viewport) ---
     def outputRGBA8(self, out: np.ndarray | None = None) -> np.ndarray:

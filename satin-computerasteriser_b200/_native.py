@@ -71,6 +71,11 @@ class cr_synth_terrain(C.Structure):
                 ("outlierMargin", C.c_float), ("colorNoiseSigma", C.c_float)]
 
 
+class cr_frame_planes(C.Structure):
+    _fields_ = [("depth", C.c_void_p), ("accum", C.c_void_p), ("pixels", C.c_uint64),
+                ("stream", C.c_void_p)]
+
+
 class cr_tuning(C.Structure):
     _fields_ = [("chunkPoints", C.c_int32), ("useTiles", C.c_int32),
                 ("viewGroupPixels", C.c_int32)]
@@ -116,6 +121,10 @@ PROTOTYPES = {
     "cr_frame_create": (C.c_int, [P, C.c_int, C.c_int, VP]),
     "cr_frame_destroy": (C.c_int, [P]),
     "cr_render": (C.c_int, [P, P, P, u32, C.POINTER(cr_config), C.POINTER(cr_camera)]),
+    "cr_render_stages": (C.c_int, [P, P, P, u32, C.POINTER(cr_config), C.POINTER(cr_camera),
+                                   u32]),
+    "cr_frame_device_planes": (C.c_int, [P, C.POINTER(cr_frame_planes)]),
+    "cr_frame_flip_depth_order": (C.c_int, [P]),
     "cr_frame_read_rgba8": (C.c_int, [P, P]),
     "cr_frame_read_rgba8_async": (C.c_int, [P, P]),
     "cr_frame_read_wait": (C.c_int, [P]),

@@ -770,8 +770,13 @@ CR_API cr_status cr_frame_destroy(cr_frame *f) {
     return CR_OK;
 }
 
-CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds,
-                           uint32_t nclouds, const cr_config *cfg, const cr_camera *cam) {
+// cr_render and cr_render_stages: the HQS passes in three stages that a host
+// may separate to combine frames' planes between them (a frame sharded by
+// points over several GPUs).  Packed colour adds (with the exact re-run) only
+// when the colour and resolve stages run in one call.
+static cr_status render_impl(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds,
+                             uint32_t nclouds, const cr_config *cfg, const cr_camera *cam,
+                             uint32_t stages) {
     cr_status st = validate_render(ctx, f, cfg, cam);
     if (st) return st;
     if (nclouds && !clouds) return fail(CR_ERR_INVALID_ARGUMENT, "clouds is null");
@@ -784,18 +789,13 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
     const size_t npix = (size_t)W * H;
     ResolveUniforms ru{W, H, {cfg->backgroundColor[0], cfg->backgroundColor[1],
                               cfg->backgroundColor[2], cfg->backgroundColor[3]}};
-    if (ctx->profiling) {
+    if (ctx->profiling && (stages & CR_STAGE_DEPTH)) {
         ctx->prof_frame = (ctx->prof_frame + 1) % cr_context::kProfRing;
         ctx->prof_count += 1;
         for (int p = 0; p < CR_PASS_COUNT; ++p) ctx->pass_recorded[ctx->prof_frame][p] = false;
     }
     if (cfg->mode == CR_MODE_HIGH_QUALITY_AVERAGE) {
         // encodeHighQualityAverage (ComputeRasteriser.swift:322-456).
-        {
-            PassTimer pt(ctx, CR_PASS_CLEAR);
-            CR_CUDA(cudaMemsetAsync(f->d_depth, 0, npix * 4, s));
-            CR_CUDA(cudaMemsetAsync(f->d_accum, 0, (npix + 1) * 16, s));  // + redo flag
-        }
         std::vector<cr_cloud *> resident;
         uint64_t max_samples = 0;  // upper bound on the frame's colour samples
         for (uint32_t i = 0; i < nclouds; ++i)
@@ -803,37 +803,45 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
                 resident.push_back(clouds[i]);
                 max_samples += (uint64_t)clouds[i]->resident * clouds[i]->cap.pointsPerBatch;
             }
-        const CullUniforms cu = make_cull_uniforms(cfg, cam, W, H);
         const RasterUniforms rau = make_raster_uniforms(cfg, cam, W, H);
-        // Packed colour adds while the frame holds fewer than 2^31 samples:
-        // then a pixel's count field reads its true count plus at most 127
-        // carries out of the blue sum, so a read count of at most
-        // kPackedMaxCount proves that no field carried.
-        const bool packed = max_samples < (1ull << 31);
-        RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
-        t.packed = packed ? 1 : 0;
-        {
-            PassTimer pt(ctx, CR_PASS_CULL);
-            for (cr_cloud *c : resident)
-                if ((st = launch_cull(c, cu, s))) return st;
-        }
         // With single-pixel footprints the depth pass keeps every point that
         // reaches the screen as a fragment and the colour pass reads those
         // instead of decoding and projecting the points again.
         const bool frags = std::fmax(cfg->minimumPointSize, cfg->maximumPointSize) <= 1.0f;
-        {
-            PassTimer pt(ctx, CR_PASS_DEPTH);
-            for (cr_cloud *c : resident)
-                if ((st = launch_raster(c, frags ? PASS_DEPTH_FRAG : PASS_DEPTH, rau, t, s)))
-                    return st;
+        // Packed colour adds while the frame holds fewer than 2^31 samples:
+        // then a pixel's count field reads its true count plus at most 127
+        // carries out of the blue sum, so a read count of at most
+        // kPackedMaxCount proves that no field carried.
+        const bool packed = (stages & CR_STAGE_COLOR) && (stages & CR_STAGE_RESOLVE) &&
+                            max_samples < (1ull << 31);
+        RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
+        t.packed = packed ? 1 : 0;
+        if (stages & CR_STAGE_DEPTH) {
+            {
+                PassTimer pt(ctx, CR_PASS_CLEAR);
+                CR_CUDA(cudaMemsetAsync(f->d_depth, 0, npix * 4, s));
+                CR_CUDA(cudaMemsetAsync(f->d_accum, 0, (npix + 1) * 16, s));  // + redo flag
+            }
+            const CullUniforms cu = make_cull_uniforms(cfg, cam, W, H);
+            {
+                PassTimer pt(ctx, CR_PASS_CULL);
+                for (cr_cloud *c : resident)
+                    if ((st = launch_cull(c, cu, s))) return st;
+            }
+            {
+                PassTimer pt(ctx, CR_PASS_DEPTH);
+                for (cr_cloud *c : resident)
+                    if ((st = launch_raster(c, frags ? PASS_DEPTH_FRAG : PASS_DEPTH, rau, t, s)))
+                        return st;
+            }
         }
-        {
+        if (stages & CR_STAGE_COLOR) {
             PassTimer pt(ctx, CR_PASS_COLOR);
             for (cr_cloud *c : resident)
                 if ((st = launch_raster(c, frags ? PASS_COLOR_FRAG : PASS_COLOR, rau, t, s)))
                     return st;
         }
-        {
+        if (stages & CR_STAGE_RESOLVE) {
             PassTimer pt(ctx, CR_PASS_RESOLVE);
             if ((st = frame_copy_fence(f, s))) return st;
             if ((st = launch_resolve_hqs(f, ru, s, packed, nullptr))) return st;
@@ -850,8 +858,8 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
                         return st;
                 if ((st = launch_resolve_hqs(f, ru, s, false, f->d_redo))) return st;
             }
+            f->last_mode = 0;
         }
-        f->last_mode = 0;
     } else {
         // encodeNearestPoint (ComputeRasteriser.swift:483-497): first resident cloud only.
         cr_cloud *first = nullptr;
@@ -881,6 +889,7 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
             f->last_mode = 1;
         }
     }
+    if (!(stages & CR_STAGE_RESOLVE)) return CR_OK;
     // encodeHoleFill (ComputeRasteriser.swift:298-320) always starts from the
     // resolve target.
     f->final_rgba = 0;
@@ -890,6 +899,36 @@ CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds
         return launch_hole_fill(f, cfg->holeFillIterations, s);
     }
     return CR_OK;
+}
+
+CR_API cr_status cr_render(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds,
+                           uint32_t nclouds, const cr_config *cfg, const cr_camera *cam) {
+    return render_impl(ctx, f, clouds, nclouds, cfg, cam, CR_STAGE_ALL);
+}
+
+CR_API cr_status cr_render_stages(cr_context *ctx, cr_frame *f, cr_cloud *const *clouds,
+                                  uint32_t nclouds, const cr_config *cfg, const cr_camera *cam,
+                                  uint32_t stages) {
+    if (stages == 0 || (stages & ~(uint32_t)CR_STAGE_ALL))
+        return fail(CR_ERR_INVALID_ARGUMENT, "stages must be a non-empty set of CR_STAGE_* bits");
+    if (cfg && cfg->mode != CR_MODE_HIGH_QUALITY_AVERAGE && stages != CR_STAGE_ALL)
+        return fail(CR_ERR_UNSUPPORTED, "separate stages need the HQS mode");
+    return render_impl(ctx, f, clouds, nclouds, cfg, cam, stages);
+}
+
+CR_API cr_status cr_frame_device_planes(cr_frame *f, cr_frame_planes *out) {
+    if (!f || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    out->depth = f->d_depth;
+    out->accum = f->d_accum;
+    out->pixels = (uint64_t)f->width * f->height;
+    out->stream = (void *)f->ctx->stream;
+    return CR_OK;
+}
+
+CR_API cr_status cr_frame_flip_depth_order(cr_frame *f) {
+    if (!f) return fail(CR_ERR_INVALID_ARGUMENT, "frame is null");
+    DeviceGuard g(f->ctx->device);
+    return launch_flip_depth_order(f, f->ctx->stream);
 }
 
 static cr_status read_plane(cr_frame *f, void *out, const void *src, size_t bytes) {

@@ -357,6 +357,8 @@ cr_status launch_hole_fill_views(const ViewDesc *views, uint32_t nviews, uint32_
 cr_status launch_resolve_nearest(cr_frame *f, const uint32_t *colors, const ResolveUniforms &u,
                                  cudaStream_t s);
 cr_status launch_hole_fill(cr_frame *f, int iterations, cudaStream_t s);
+// XOR 0x80000000 into every word of the frame's depth plane.
+cr_status launch_flip_depth_order(cr_frame *f, cudaStream_t s);
 cr_status launch_split_nearest(const unsigned long long *keys, uint32_t *depth_out,
                                uint32_t *index_out, size_t n, cudaStream_t s);
 

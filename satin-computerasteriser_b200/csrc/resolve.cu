@@ -251,6 +251,21 @@ __global__ void __launch_bounds__(kThreads)
         accum[p] = make_uint4(0u, 0u, 0u, 0u);
 }
 
+// Top bit of every depth word flipped: unsigned order <-> signed order.
+__global__ void __launch_bounds__(kThreads)
+    flip_depth_order(uint4 *d4, size_t n4, uint32_t *tail, uint32_t ntail) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+        uint4 v = d4[i];
+        v.x ^= 0x80000000u;
+        v.y ^= 0x80000000u;
+        v.z ^= 0x80000000u;
+        v.w ^= 0x80000000u;
+        d4[i] = v;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < ntail) tail[threadIdx.x] ^= 0x80000000u;
+}
+
 }  // namespace
 
 cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t s, bool check,
@@ -362,6 +377,20 @@ cr_status launch_l2_loss(const float *image, const float *target, uint64_t n, fl
     const uint64_t need = (n + kThreads - 1) / kThreads;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(need, (uint64_t)sm_count * 8);
     l2_loss<<<grid, kThreads, 0, s>>>(image, target, n, scale, dldimg, loss);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+cr_status launch_flip_depth_order(cr_frame *f, cudaStream_t s) {
+    // The plane comes from cudaMalloc (256-byte aligned): 16-byte words, then
+    // the last npix % 4 words.
+    const size_t npix = (size_t)f->width * f->height;
+    const size_t n4 = npix / 4;
+    const uint32_t ntail = (uint32_t)(npix - 4 * n4);
+    const uint32_t grid = (uint32_t)std::max<size_t>(
+        1, std::min<size_t>((n4 + kThreads - 1) / kThreads, (size_t)f->ctx->sm_count * 8));
+    flip_depth_order<<<grid, kThreads, 0, s>>>(reinterpret_cast<uint4 *>(f->d_depth), n4,
+                                               f->d_depth + 4 * n4, ntail);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

@@ -57,3 +57,21 @@ def oracle_cloud_from_device(orc, cloud):
     return orc.Cloud(batches=cloud.batches(), files=cloud.files(), xyzLow=pts["xyzLow"],
                      xyzMed=pts["xyzMed"], xyzHigh=pts["xyzHigh"], colors=pts["colors"],
                      levels=pts["levels"])
+
+
+def look_at_reverse_z(pos, target=(0.0, 0.0, 0.0), aspect=1.0, near=0.01, far=100.0, fov=60.0):
+    """Right-handed view looking from `pos` at `target` (up +Y) and a reverse-Z
+    perspective projection, both column-major float32[16]."""
+    p, t = np.asarray(pos, np.float64), np.asarray(target, np.float64)
+    f = (t - p) / np.linalg.norm(t - p)
+    s = np.cross(f, [0.0, 1.0, 0.0])
+    s /= np.linalg.norm(s)
+    u = np.cross(s, f)
+    v = np.eye(4)
+    v[0, :3], v[1, :3], v[2, :3] = s, u, -f
+    v[0, 3], v[1, 3], v[2, 3] = -s @ p, -u @ p, f @ p
+    k = 1.0 / np.tan(np.radians(fov) / 2)
+    pr = np.zeros((4, 4))
+    pr[0, 0], pr[1, 1] = k / aspect, k
+    pr[2, 2], pr[2, 3], pr[3, 2] = near / (far - near), far * near / (far - near), -1.0
+    return v.T.astype(np.float32).reshape(16), pr.T.astype(np.float32).reshape(16)
