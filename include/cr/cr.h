@@ -245,6 +245,33 @@ CR_API cr_status cr_cloud_add_batches(cr_cloud *cloud,
 /* removeBatches(slots:commit:) — ComputeRasteriserPointCloud.swift:460-473. */
 CR_API cr_status cr_cloud_remove_batches(cr_cloud *cloud, const int32_t *slots, uint32_t n,
                                          int commit);
+
+/* Asynchronous addBatches for streaming residency: takes the slots at once
+ * (slots_out) and copies the points into them while frames render.  The
+ * arrays are copied into the cloud's page-locked staging ring before the
+ * call returns (host pointers borrowed for the call only); the device copies
+ * run on the context's upload stream after the render work enqueued before
+ * the call.  The slots stay non-resident (state 0, skipped by the cull) until
+ * cr_cloud_poll_uploads or cr_cloud_wait_uploads sees their copy landed and
+ * publishes them (state 1; `commit` then uploads the batch table, as
+ * cr_cloud_commit).  Removing a slot whose copy is in flight cancels it: the
+ * slot returns to the free list when the copy lands.  When the ring has no
+ * room the call waits for the oldest copy; a call larger than the ring grows
+ * it.  No counterpart in the reference, whose addBatches
+ * (ComputeRasteriserPointCloud.swift:410-452) copies synchronously. */
+CR_API cr_status cr_cloud_add_batches_async(cr_cloud *cloud, const uint32_t *xyz_low,
+                                            const uint32_t *xyz_med, const uint32_t *xyz_high,
+                                            const uint32_t *colors, const uint8_t *levels,
+                                            uint64_t points_len, const cr_raster_batch *batches,
+                                            uint32_t n, int32_t *slots_out);
+/* Publishes the uploads whose copies have landed (non-blocking): batches
+ * published by this call and batches still in flight (either may be NULL). */
+CR_API cr_status cr_cloud_poll_uploads(cr_cloud *cloud, int commit, uint32_t *landed_batches,
+                                       uint32_t *in_flight_batches);
+/* Waits for every upload in flight and publishes it. */
+CR_API cr_status cr_cloud_wait_uploads(cr_cloud *cloud, int commit);
+/* Staging ring size in bytes (default 64 MiB; waits for copies in flight). */
+CR_API cr_status cr_cloud_set_upload_staging(cr_cloud *cloud, uint64_t bytes);
 /* commitBatchUpdates() — ComputeRasteriserPointCloud.swift:481-483 (uploads
  * the dirty slot range of the host batch mirror). */
 CR_API cr_status cr_cloud_commit(cr_cloud *cloud);

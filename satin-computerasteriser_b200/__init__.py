@@ -427,6 +427,40 @@ class ComputeRasteriserPointCloud:
                                              int(commit), N.ptr(slots)))
         return slots[:len(b)].tolist()
 
+    def addBatchesAsync(self, positionsXYZLow, positionsXYZMed, positionsXYZHigh, colors,
+                        levels, batches) -> list[int]:
+        """addBatches with an asynchronous copy (cr_cloud_add_batches_async): the
+        slots are taken now and become resident when pollUploads / waitUploads
+        sees their copy landed; the arrays may be reused when this returns."""
+        low = np.ascontiguousarray(positionsXYZLow, np.uint32)
+        med = np.ascontiguousarray(positionsXYZMed, np.uint32)
+        high = np.ascontiguousarray(positionsXYZHigh, np.uint32)
+        col = np.ascontiguousarray(colors, np.uint32)
+        lv = np.ascontiguousarray(levels, np.uint8)
+        b = np.ascontiguousarray(batches, BATCH_DTYPE)
+        n = min(len(low), len(med), len(high), len(col), len(lv))
+        slots = np.zeros(max(len(b), 1), np.int32)
+        N.check(N.lib().cr_cloud_add_batches_async(self._h, N.ptr(low), N.ptr(med), N.ptr(high),
+                                                   N.ptr(col), N.ptr(lv), n, N.ptr(b), len(b),
+                                                   N.ptr(slots)))
+        return slots[:len(b)].tolist()
+
+    def pollUploads(self, commit: bool = True) -> tuple[int, int]:
+        """Publishes the asynchronous uploads that have landed (non-blocking);
+        returns (batches published now, batches still in flight)."""
+        landed, flying = C.c_uint32(0), C.c_uint32(0)
+        N.check(N.lib().cr_cloud_poll_uploads(self._h, int(commit), C.byref(landed),
+                                              C.byref(flying)))
+        return landed.value, flying.value
+
+    def waitUploads(self, commit: bool = True):
+        """Waits for every asynchronous upload in flight and publishes it."""
+        N.check(N.lib().cr_cloud_wait_uploads(self._h, int(commit)))
+
+    def setUploadStaging(self, nbytes: int):
+        """Size of the page-locked staging ring of the asynchronous uploads."""
+        N.check(N.lib().cr_cloud_set_upload_staging(self._h, int(nbytes)))
+
     def removeBatches(self, slots, commit: bool = True):
         """removeBatches (ComputeRasteriserPointCloud.swift:460-473)."""
         s = np.ascontiguousarray(slots, np.int32)

@@ -82,18 +82,6 @@ void dfree(T *&p) {
     p = nullptr;
 }
 
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
 
 void free_cloud_buffers(cr_cloud *c) {
     dfree(c->d_low);
@@ -115,6 +103,8 @@ void free_cloud_buffers(cr_cloud *c) {
     dfree(c->d_counters);
 }
 
+}  // namespace
+
 void mark_dirty(cr_cloud *c, int64_t lo, int64_t hi) {
     if (lo < c->dirty_lo) c->dirty_lo = lo;
     if (hi > c->dirty_hi) c->dirty_hi = hi;
@@ -133,6 +123,8 @@ cr_status flush_mirror(cr_cloud *c) {
                             cudaMemcpyHostToDevice, c->ctx->stream));
     return CR_OK;
 }
+
+namespace {
 
 cr_status upload_files(cr_cloud *c, const std::vector<cr_raster_file> &files) {
     if (files.empty()) return CR_OK;
@@ -181,6 +173,7 @@ cr_status alloc_ring(cr_cloud *c) {
 // allocateBuffers + rebuildFilesBuffer + rebuildCullBuffers
 // (ComputeRasteriserPointCloud.swift:532-589).
 cr_status allocate_cloud(cr_cloud *c, cr_capacity cap, const cr_raster_file *files, uint32_t nf) {
+    uploads_free(c);  // waits for copies in flight; the slot table is rebuilt
     free_cloud_buffers(c);
     c->cap = cap;
     c->files.clear();
@@ -473,6 +466,7 @@ CR_API cr_status cr_cloud_create(cr_context *ctx, cr_capacity cap, const cr_rast
 CR_API cr_status cr_cloud_destroy(cr_cloud *c) {
     if (!c) return CR_OK;
     DeviceGuard g(c->ctx->device);
+    uploads_free(c);  // waits for copies in flight
     cudaStreamSynchronize(c->ctx->stream);
     free_cloud_buffers(c);
     if (c->h_files_ring) cudaFreeHost(c->h_files_ring);
@@ -490,6 +484,7 @@ CR_API cr_status cr_cloud_reallocate(cr_cloud *c, cr_capacity cap, const cr_rast
     if ((uint64_t)cap.maxResidentBatches * cap.pointsPerBatch >= 0xffffffffull)
         return fail(CR_ERR_CAPACITY, "pool exceeds 2^32-1 points");
     DeviceGuard g(c->ctx->device);
+    uploads_free(c);  // the slot table and pool change size
     CR_CUDA(cudaStreamSynchronize(c->ctx->stream));
     std::vector<cr_raster_file> keep;
     if (files && nfiles) keep.assign(files, files + nfiles);
@@ -593,6 +588,7 @@ CR_API cr_status cr_cloud_remove_batches(cr_cloud *c, const int32_t *slots, uint
             return fail(CR_ERR_INVALID_ARGUMENT,
                         "removeBatches: slot " + std::to_string(slots[i]) + " out of range");
     for (uint32_t i = 0; i < n; ++i) {
+        if (uploads_cancel(c, slots[i])) continue;  // freed when its copy lands
         cr_raster_batch &b = c->mirror[slots[i]];
         if (b.state == 0) continue;
         c->points -= b.numPoints;
@@ -617,6 +613,8 @@ CR_API cr_status cr_cloud_commit(cr_cloud *c) {
 
 CR_API cr_status cr_cloud_clear(cr_cloud *c) {
     if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
+    cr_status st = uploads_drain(c);
+    if (st) return st;
     for (auto &b : c->mirror) {
         b.state = 0;
         b.numPoints = 0;
@@ -1310,6 +1308,7 @@ CR_API cr_status cr_pack(cr_context *ctx, cr_cloud *c, const cr_pack_input *in, 
     cr_status st = validate_pack(ctx, c, prm);
     if (st) return st;
     DeviceGuard g(ctx->device);
+    if ((st = uploads_drain(c))) return st;  // every slot is rewritten
     // GPUPacker.pack: an empty input clears the cloud (GPUPacker.swift:147-150).
     if (count == 0) return cr_cloud_clear(c);
     if ((st = validate_input(in))) return st;
@@ -1358,7 +1357,7 @@ static int64_t reserve_contiguous(cr_cloud *c, uint32_t n) {
     uint32_t s = 0;
     while ((uint64_t)s + n <= cap) {
         uint32_t k = 0;
-        while (k < n && c->mirror[s + k].state == 0) ++k;
+        while (k < n && c->mirror[s + k].state == 0 && !upload_slot_busy(c, s + k)) ++k;
         if (k == n) {
             std::vector<int32_t> keep;
             keep.reserve(c->free_slots.size());

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <deque>
 #include <vector>
 
 #include "cr/cr.h"
@@ -79,7 +80,8 @@ struct cr_context {
     double *d_loss = nullptr;     // cr_l2_loss's device accumulator (lazy)
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaStream_t copy_stream = nullptr;  // asynchronous RGBA8 read-backs (lazy)
+    cudaStream_t copy_stream = nullptr;    // asynchronous RGBA8 read-backs (lazy)
+    cudaStream_t upload_stream = nullptr;  // asynchronous slot-pool uploads (lazy)
     int sm_count = 0;
     int blocks_per_sm[7] = {};        // occupancy of the persistent point passes (per RasterPass)
     int blocks_per_sm_views[7] = {};  // the same, batched-view kernels
@@ -111,8 +113,45 @@ struct PassTimer {
     }
 };
 
+// Makes `dev` current for a scope (the previous device is restored).
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Asynchronous slot-pool uploads of a cloud (csrc/upload.cpp).
+constexpr uint8_t kSlotIdle = 0, kSlotPending = 1, kSlotCancelled = 2;
+struct UploadBatch {
+    int32_t slot;
+    cr_raster_batch rec;  // the record published when the copy lands
+};
+struct PendingUpload {
+    cudaEvent_t ev = nullptr;  // recorded on the upload stream after the copies
+    uint64_t stage_off = 0;    // staging ring bytes held until the copy lands
+    std::vector<UploadBatch> batches;
+};
+struct UploadState {
+    unsigned char *h_stage = nullptr;  // page-locked staging ring
+    uint64_t cap = 0, want_cap = 0;    // ring bytes; size asked for (0 = default)
+    uint64_t head = 0, tail = 0;       // next free byte; start of the oldest region
+    std::deque<PendingUpload> q;       // in flight, oldest first
+    std::vector<uint8_t> slot;         // per slot: kSlotIdle / Pending / Cancelled
+    std::vector<cudaEvent_t> spare;    // events of landed uploads, reused
+    cudaEvent_t ready = nullptr;       // context-stream point the copies wait for
+    uint32_t in_flight_batches = 0;
+};
+
 struct cr_cloud {
     cr_context *ctx = nullptr;
+    UploadState *up = nullptr;  // asynchronous uploads (lazy)
     cr_capacity cap{0, 0};
     std::vector<cr_raster_file> files;        // file table (world matrices)
     std::vector<cr_raster_file> frame_files;  // last updateFiles snapshot
@@ -171,6 +210,16 @@ struct cr_frame {
     cudaEvent_t ev_rendered = nullptr, ev_copied = nullptr;
     bool copy_pending = false;
 };
+
+// Asynchronous uploads: wait for and publish every upload in flight; free
+// the upload state; cancel a slot's upload in flight (true if it had one);
+// whether a slot has an upload in flight.
+cr_status uploads_drain(cr_cloud *c);
+void uploads_free(cr_cloud *c);
+bool uploads_cancel(cr_cloud *c, int32_t slot);
+bool upload_slot_busy(const cr_cloud *c, uint32_t slot);
+void mark_dirty(cr_cloud *c, int64_t lo, int64_t hi);
+cr_status flush_mirror(cr_cloud *c);
 
 // Makes later work on `s` wait (on the device) for the frame's enqueued
 // asynchronous read-backs; call before the first write of the RGBA8 planes.
