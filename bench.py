@@ -79,6 +79,9 @@ def parse_args():
                     help="points whose gradient is checked against the FP64 oracle (0 = none)")
     ap.add_argument("--pack-points", type=int, default=400_000_000,
                     help="points of the 63-bit packer leg (0 = skip it)")
+    ap.add_argument("--stream-points", type=int, default=20_000_000,
+                    help="points of the streaming-residency leg (0 = skip it)")
+    ap.add_argument("--stream-frames", type=int, default=96)
     ap.add_argument("--shard", default="frames", choices=["frames", "points"],
                     help="N>1: every rank renders its own frames of its own copy of the cloud "
                          "(frames, weak scaling), or every frame is split by batches over the "
@@ -517,10 +520,121 @@ def run_ours(args, dist):
         out["multiview"] = run_multiview(args, cr, ctx, torch, dist)
     if args.diff_points > 0:
         out["differentiable"] = run_differentiable(args, cr, ctx, torch, dist)
+    if args.stream_points > 0:
+        out["streaming"] = run_streaming(args, cr, ctx, dist)
     if args.pack_points > 0:
         cloud.close()
         out["packer"] = run_packer(args, cr, ctx, torch, dist)
     return out
+
+
+class _SyncUploads:
+    """A cloud whose adapter uploads copy synchronously (the reference's
+    addBatches, ComputeRasteriserPointCloud.swift:410-452): the comparison arm
+    of the streaming leg."""
+
+    def __init__(self, cloud):
+        self.cloud = cloud
+
+    def __getattr__(self, name):
+        return getattr(self.cloud, name)
+
+    def addBatchesAsync(self, low, med, high, colors, levels, batches, borrow=False):
+        return self.cloud.addBatches(low, med, high, colors, levels, batches, commit=False)
+
+    def pollUploads(self, commit=True):
+        return 0, 0
+
+
+def run_streaming(args, cr, ctx, dist):
+    """Streaming residency: a camera flight at 300 m over a --stream-points
+    terrain whose chunks (8 batches of 10,240 points, Morton-contiguous) stream
+    from host memory into a pool of 40 % of the batches; the in-memory source
+    wants the nearest chunks within a budget of 50 % of the cloud (the pool is
+    over-subscribed).  The chunks sit in page-locked host memory.  Per frame:
+    StreamingAdapter.update (up to 8 chunk uploads), render, wait for the
+    frame.  Timed twice on the same path, with asynchronous uploads that
+    borrow the chunks' arrays (addBatchesAsync) and with synchronous ones
+    (the reference's addBatches); the
+    adapter's invariant (source's resident chunks = resident + queued) is
+    checked every frame."""
+    streaming = importlib.import_module("satin-computerasteriser_b200.streaming")
+    params = cr.TerrainParams(seed=args.seed ^ 0x57)
+    sargs = argparse.Namespace(**vars(args))
+    sargs.points = args.stream_points
+    src_cloud, _ = build_cloud(cr, ctx, sargs, params)
+    packed = argparse.Namespace(batches=src_cloud.batches(), **src_cloud.points())
+    src_cloud.close()
+    ctx.trim()
+    chunks = streaming.chunks_from_packed(packed, 8)
+    del packed
+    nb = sum(len(c.batches) for c in chunks)
+    total_bytes = sum(c.totalPointCount for c in chunks) * streaming.BYTES_PER_POINT
+    W, H = 1280, 720
+    e = params.extent
+    path = []
+    for k in range(args.stream_frames):
+        t = k / max(args.stream_frames - 1, 1)
+        x, y = e * (0.1 + 0.8 * t), e * (0.3 + 0.4 * t)
+        z = cr.terrain_height(params, x, y) + 300.0
+        cam = cr.PerspectiveCamera(position=(x, y, z), near=1.0, far=10000.0, fov=60.0,
+                                   aspect=W / H)
+        cam.lookAt((x + 600.0, y + 300.0, z - 400.0), up=(0.0, 0.0, 1.0))
+        path.append(cam)
+
+    # Chunks in page-locked host memory: the asynchronous uploads read them
+    # directly; the synchronous arm copies the same arrays.
+    arena = streaming.pin_chunks(chunks)
+
+    def fly(sync: bool):
+        cloud = cr.ComputeRasteriserPointCloud(
+            ctx, cr.ComputeRasteriserCapacity(int(0.4 * nb), 10240))
+        src = streaming.InMemoryStreamingSource(chunks, budget_bytes=int(0.5 * total_bytes))
+        ad = streaming.StreamingAdapter(src, _SyncUploads(cloud) if sync else cloud)
+        ad.maxChunkUploadsPerTick = 8
+        ras = cr.ComputeRasteriser(ctx)
+        ras.addPointCloud(cloud)
+        ras.resize((W, H))
+        ok, full, uploads, t_ad, per_frame = True, False, 0, 0.0, []
+        ctx.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        for cam in path:
+            tf = time.perf_counter()
+            had = set(ad.slotsByChunk)
+            ta = time.perf_counter()
+            ad.update(cam, (W, H))
+            t_ad += time.perf_counter() - ta
+            uploads += len(set(ad.slotsByChunk) - had)
+            ras.update(cam)
+            ras.encode()
+            ctx.synchronize()
+            ok &= len(src.believed) - ad.residentChunks - ad.pendingUploadCount == 0
+            ok &= ad.residentPoints == cloud.pointCount
+            full |= ad.lastError is not None
+            per_frame.append(time.perf_counter() - tf)
+        s = time.perf_counter() - t0
+        cloud.waitUploads()
+        res = {"ms_per_frame": round(dist.max(s) * 1e3 / len(path), 4),
+               "p95_frame_ms": round(float(np.percentile(per_frame, 95)) * 1e3, 4),
+               "max_frame_ms": round(max(per_frame) * 1e3, 4),
+               "adapter_update_ms_per_frame": round(t_ad * 1e3 / len(path), 4),
+               "chunks_uploaded": uploads,
+               "resident_chunks_end": ad.residentChunks, "invariants_hold": bool(ok),
+               "pool_pressure": bool(full)}
+        ras.removePointCloud(cloud)
+        cloud.close()
+        return res
+
+    fly(False)  # warm-up (streams)
+    a = fly(False)
+    b = fly(True)
+    arena.close()
+    return {"points": args.stream_points, "chunks": len(chunks), "batches_per_chunk": 8,
+            "pool_slots": int(0.4 * nb), "frames": len(path), "size": f"{W}x{H}",
+            "max_chunk_uploads_per_tick": 8, "async": a, "sync": b,
+            "speedup": round(b["ms_per_frame"] / max(a["ms_per_frame"], 1e-9), 3),
+            "timing": "wall clock per frame: adapter update + render + wait for the frame"}
 
 
 def decoded_positions(cloud, first=0, n=None):

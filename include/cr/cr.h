@@ -254,16 +254,22 @@ CR_API cr_status cr_cloud_remove_batches(cr_cloud *cloud, const int32_t *slots, 
  * the call.  The slots stay non-resident (state 0, skipped by the cull) until
  * cr_cloud_poll_uploads or cr_cloud_wait_uploads sees their copy landed and
  * publishes them (state 1; `commit` then uploads the batch table, as
- * cr_cloud_commit).  Removing a slot whose copy is in flight cancels it: the
+ * cr_cloud_commit).  flags = CR_UPLOAD_BORROW skips the staging copy (below).  Removing a slot whose copy is in flight cancels it: the
  * slot returns to the free list when the copy lands.  When the ring has no
  * room the call waits for the oldest copy; a call larger than the ring grows
  * it.  No counterpart in the reference, whose addBatches
  * (ComputeRasteriserPointCloud.swift:410-452) copies synchronously. */
+enum {
+    /* The arrays are page-locked (cr_host_alloc or registered memory) and stay
+     * valid and unchanged until the upload is published: they are the source
+     * of the device copies, with no staging copy. */
+    CR_UPLOAD_BORROW = 1
+};
 CR_API cr_status cr_cloud_add_batches_async(cr_cloud *cloud, const uint32_t *xyz_low,
                                             const uint32_t *xyz_med, const uint32_t *xyz_high,
                                             const uint32_t *colors, const uint8_t *levels,
                                             uint64_t points_len, const cr_raster_batch *batches,
-                                            uint32_t n, int32_t *slots_out);
+                                            uint32_t n, uint32_t flags, int32_t *slots_out);
 /* Publishes the uploads whose copies have landed (non-blocking): batches
  * published by this call and batches still in flight (either may be NULL). */
 CR_API cr_status cr_cloud_poll_uploads(cr_cloud *cloud, int commit, uint32_t *landed_batches,

@@ -428,10 +428,18 @@ class ComputeRasteriserPointCloud:
         return slots[:len(b)].tolist()
 
     def addBatchesAsync(self, positionsXYZLow, positionsXYZMed, positionsXYZHigh, colors,
-                        levels, batches) -> list[int]:
+                        levels, batches, borrow: bool = False) -> list[int]:
         """addBatches with an asynchronous copy (cr_cloud_add_batches_async): the
         slots are taken now and become resident when pollUploads / waitUploads
-        sees their copy landed; the arrays may be reused when this returns."""
+        sees their copy landed.  The arrays may be reused when this returns;
+        with borrow=True they must be page-locked (HostBuffer arrays) and stay
+        unchanged until the upload is published (no staging copy)."""
+        if borrow:
+            for a, dt in ((positionsXYZLow, np.uint32), (positionsXYZMed, np.uint32),
+                          (positionsXYZHigh, np.uint32), (colors, np.uint32),
+                          (levels, np.uint8)):
+                if a.dtype != dt or not a.flags.c_contiguous:
+                    raise CRError(1, "borrowed arrays must be C-contiguous of the pool's types")
         low = np.ascontiguousarray(positionsXYZLow, np.uint32)
         med = np.ascontiguousarray(positionsXYZMed, np.uint32)
         high = np.ascontiguousarray(positionsXYZHigh, np.uint32)
@@ -442,7 +450,7 @@ class ComputeRasteriserPointCloud:
         slots = np.zeros(max(len(b), 1), np.int32)
         N.check(N.lib().cr_cloud_add_batches_async(self._h, N.ptr(low), N.ptr(med), N.ptr(high),
                                                    N.ptr(col), N.ptr(lv), n, N.ptr(b), len(b),
-                                                   N.ptr(slots)))
+                                                   1 if borrow else 0, N.ptr(slots)))
         return slots[:len(b)].tolist()
 
     def pollUploads(self, commit: bool = True) -> tuple[int, int]:

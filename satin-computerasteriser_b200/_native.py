@@ -121,7 +121,7 @@ PROTOTYPES = {
     "cr_frame_create": (C.c_int, [P, C.c_int, C.c_int, VP]),
     "cr_frame_destroy": (C.c_int, [P]),
     "cr_render": (C.c_int, [P, P, P, u32, C.POINTER(cr_config), C.POINTER(cr_camera)]),
-    "cr_cloud_add_batches_async": (C.c_int, [P, P, P, P, P, P, u64, P, u32, P]),
+    "cr_cloud_add_batches_async": (C.c_int, [P, P, P, P, P, P, u64, P, u32, u32, P]),
     "cr_cloud_poll_uploads": (C.c_int, [P, C.c_int, P, P]),
     "cr_cloud_wait_uploads": (C.c_int, [P, C.c_int]),
     "cr_cloud_set_upload_staging": (C.c_int, [P, u64]),

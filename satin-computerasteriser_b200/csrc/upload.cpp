@@ -7,7 +7,10 @@
 // the copy is asynchronous:
 //
 //   * the caller's arrays are copied (host memcpy) into a page-locked staging
-//     ring of the cloud and are free again when the call returns;
+//     ring of the cloud and are free again when the call returns; or, with
+//     CR_UPLOAD_BORROW, the caller's own page-locked arrays are the source of
+//     the device copies and stay borrowed until the upload is published (no
+//     host copy at all: a streaming source that keeps its chunks pinned);
 //   * the staging bytes go to the slots' pool ranges on the context's upload
 //     stream, after the render work enqueued before the call (a slot freed in
 //     the same tick may still be read by an earlier frame);
@@ -141,7 +144,7 @@ CR_API cr_status cr_cloud_add_batches_async(cr_cloud *c, const uint32_t *low, co
                                             const uint32_t *high, const uint32_t *colors,
                                             const uint8_t *levels, uint64_t points_len,
                                             const cr_raster_batch *batches, uint32_t n,
-                                            int32_t *slots_out) {
+                                            uint32_t flags, int32_t *slots_out) {
     if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
     if (n > c->free_slots.size())
         return fail(CR_ERR_CAPACITY, "addBatches: not enough free slots (have " +
@@ -163,11 +166,14 @@ CR_API cr_status cr_cloud_add_batches_async(cr_cloud *c, const uint32_t *low, co
             return fail(CR_ERR_INVALID_ARGUMENT, "batch fileIndex outside the file table");
         total += cnt;
     }
+    if (flags & ~(uint32_t)CR_UPLOAD_BORROW)
+        return fail(CR_ERR_INVALID_ARGUMENT, "unknown upload flags");
+    const bool borrow = (flags & CR_UPLOAD_BORROW) != 0;
     cr_context *ctx = c->ctx;
     DeviceGuard g(ctx->device);
     UploadState &u = state(c);
-    const uint64_t need = staging_bytes(total);
-    if (need > u.cap) {
+    const uint64_t need = borrow ? 0 : staging_bytes(total);
+    if (need > 0 && need > u.cap) {
         // Grow the ring (after every copy out of the old one has landed).
         cr_status st = land(c, true, nullptr);
         if (st) return st;
@@ -181,36 +187,49 @@ CR_API cr_status cr_cloud_add_batches_async(cr_cloud *c, const uint32_t *low, co
     if (!ctx->upload_stream)
         CR_CUDA(cudaStreamCreateWithFlags(&ctx->upload_stream, cudaStreamNonBlocking));
     if (!u.ready) CR_CUDA(cudaEventCreateWithFlags(&u.ready, cudaEventDisableTiming));
-    int64_t off;
-    while ((off = ring_alloc(u, need)) < 0) {
-        // No room: wait for the oldest upload to land.
-        CR_CUDA(cudaEventSynchronize(u.q.front().ev));
-        land_front(c);
-    }
-    u.head = (uint64_t)off + need;
-    if (u.q.empty()) u.tail = (uint64_t)off;
-
-    // Host copy into the staging region: the four word arrays and the level
-    // bytes of all batches, batch after batch.
-    unsigned char *base = u.h_stage + off;
-    const uint64_t w4 = align16(4 * total);
-    uint32_t *s_low = reinterpret_cast<uint32_t *>(base);
-    uint32_t *s_med = reinterpret_cast<uint32_t *>(base + w4);
-    uint32_t *s_high = reinterpret_cast<uint32_t *>(base + 2 * w4);
-    uint32_t *s_col = reinterpret_cast<uint32_t *>(base + 3 * w4);
-    uint8_t *s_lv = base + 4 * w4;
     PendingUpload p;
-    p.stage_off = (uint64_t)off;
     p.batches.reserve(n);
-    uint64_t k = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        const uint64_t src = batches[i].firstPoint, cnt = batches[i].numPoints;
-        std::memcpy(s_low + k, low + src, cnt * 4);
-        std::memcpy(s_med + k, med + src, cnt * 4);
-        std::memcpy(s_high + k, high + src, cnt * 4);
-        std::memcpy(s_col + k, colors + src, cnt * 4);
-        std::memcpy(s_lv + k, levels + src, cnt);
-        k += cnt;
+    // Source of the device copies: the caller's page-locked arrays (borrowed
+    // until the upload is published), indexed by the batches' firstPoint; or
+    // a staging region holding the batches' points back to back.
+    const uint32_t *s_low = low, *s_med = med, *s_high = high, *s_col = colors;
+    const uint8_t *s_lv = levels;
+    if (borrow) {
+        p.stage_off = u.head;  // holds no staging bytes
+    } else {
+        int64_t off;
+        while ((off = ring_alloc(u, need)) < 0) {
+            // No room: wait for the oldest upload to land.
+            CR_CUDA(cudaEventSynchronize(u.q.front().ev));
+            land_front(c);
+        }
+        u.head = (uint64_t)off + need;
+        if (u.q.empty()) u.tail = (uint64_t)off;
+        p.stage_off = (uint64_t)off;
+        // Host copy into the staging region: the four word arrays and the
+        // level bytes of all batches, batch after batch.
+        unsigned char *base = u.h_stage + off;
+        const uint64_t w4 = align16(4 * total);
+        uint32_t *d_low = reinterpret_cast<uint32_t *>(base);
+        uint32_t *d_med = reinterpret_cast<uint32_t *>(base + w4);
+        uint32_t *d_high = reinterpret_cast<uint32_t *>(base + 2 * w4);
+        uint32_t *d_col = reinterpret_cast<uint32_t *>(base + 3 * w4);
+        uint8_t *d_lv = base + 4 * w4;
+        uint64_t k = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint64_t src = batches[i].firstPoint, cnt = batches[i].numPoints;
+            std::memcpy(d_low + k, low + src, cnt * 4);
+            std::memcpy(d_med + k, med + src, cnt * 4);
+            std::memcpy(d_high + k, high + src, cnt * 4);
+            std::memcpy(d_col + k, colors + src, cnt * 4);
+            std::memcpy(d_lv + k, levels + src, cnt);
+            k += cnt;
+        }
+        s_low = d_low;
+        s_med = d_med;
+        s_high = d_high;
+        s_col = d_col;
+        s_lv = d_lv;
     }
 
     // Device copies after the render work enqueued so far.
@@ -233,20 +252,21 @@ CR_API cr_status cr_cloud_add_batches_async(cr_cloud *c, const uint32_t *low, co
         run_n = 0;
         return CR_OK;
     };
-    k = 0;
+    uint64_t k = 0;
     for (uint32_t i = 0; i < n; ++i) {
         const int32_t slot = c->free_slots.back();
         c->free_slots.pop_back();
         if (slots_out) slots_out[i] = slot;
         const uint64_t dst = (uint64_t)slot * c->cap.pointsPerBatch;
         const uint64_t cnt = batches[i].numPoints;
+        const uint64_t src = borrow ? (uint64_t)batches[i].firstPoint : k;
         if (cnt > 0) {
-            if (run_n > 0 && run_src + run_n == k && run_dst + run_n == dst) {
+            if (run_n > 0 && run_src + run_n == src && run_dst + run_n == dst) {
                 run_n += cnt;
             } else {
                 cr_status st = flush_run();
                 if (st) return st;
-                run_src = k;
+                run_src = src;
                 run_dst = dst;
                 run_n = cnt;
             }

@@ -55,6 +55,7 @@ class ResidentChunk:
     xyzHigh: np.ndarray
     colors: np.ndarray
     levels: np.ndarray
+    pinned: bool = False  # arrays in page-locked memory (pin_chunks): uploads borrow them
 
     @property
     def totalPointCount(self) -> int:
@@ -112,6 +113,32 @@ def chunks_from_packed(packed, batches_per_chunk: int) -> list[ResidentChunk]:
     return out
 
 
+def pin_chunks(chunks: list[ResidentChunk]):
+    """Moves the chunks' arrays into one page-locked host arena (HostBuffer) so
+    that uploads read them directly (addBatchesAsync(borrow=True), no staging
+    copy).  Returns the arena, which must outlive every upload from it."""
+    from . import HostBuffer
+
+    def a16(x):
+        return (x + 15) & ~15
+    total = sum(4 * a16(4 * c.totalPointCount) + a16(c.totalPointCount) for c in chunks)
+    arena = HostBuffer((max(total, 16),), np.uint8)
+    buf, off = arena.array, 0
+    for c in chunks:
+        n = c.totalPointCount
+        for name in ("xyzLow", "xyzMed", "xyzHigh", "colors"):
+            view = buf[off:off + 4 * n].view(np.uint32)
+            view[:] = getattr(c, name)
+            setattr(c, name, view)
+            off += a16(4 * n)
+        lv = buf[off:off + n]
+        lv[:] = c.levels
+        c.levels = lv
+        off += a16(n)
+        c.pinned = True
+    return arena
+
+
 class InMemoryStreamingSource:
     """A streaming source over chunks in host memory.
 
@@ -122,9 +149,15 @@ class InMemoryStreamingSource:
     wanted set since the last poll, and then counts the added chunks as
     resident on the GPU (the model the adapter must keep up with)."""
 
-    def __init__(self, chunks: list[ResidentChunk], budget_bytes: int):
+    def __init__(self, chunks: list[ResidentChunk], budget_bytes: int, pin: bool = False):
+        # pin: chunks in one page-locked arena, uploaded without a staging copy
+        # (the source must then outlive the uploads from it).
+        self._arena = pin_chunks(chunks) if pin else None
         self.chunks = {c.id: c for c in chunks}
-        self._centres = {c.id: 0.5 * (c.bounds[0] + c.bounds[1]) for c in chunks}
+        self._ids = list(self.chunks)
+        self._centres = np.array([0.5 * (c.bounds[0] + c.bounds[1]) for c in chunks],
+                                 np.float64).reshape(-1, 3)
+        self._cost = np.array([c.totalPointCount * BYTES_PER_POINT for c in chunks], np.int64)
         self.budget = int(budget_bytes)
         self.believed: set = set()
         self._wanted: list = []
@@ -135,16 +168,11 @@ class InMemoryStreamingSource:
 
     def submit(self, view: StreamingCameraView):
         pos = np.asarray(view.position, np.float64)
-        order = sorted(self.chunks, key=lambda i: (float(np.linalg.norm(self._centres[i] - pos)),
-                                                   i))
-        wanted, used = [], 0
-        for i in order:
-            cost = self.chunks[i].totalPointCount * BYTES_PER_POINT
-            if used + cost > self.budget:
-                break
-            wanted.append(i)
-            used += cost
-        self._wanted = wanted
+        d = np.linalg.norm(self._centres - pos, axis=1)
+        order = np.argsort(d, kind="stable")  # ties: chunk order
+        fits = np.cumsum(self._cost[order]) <= self.budget
+        n = len(order) if fits.all() else int(np.argmin(fits))  # nearest prefix in budget
+        self._wanted = [self._ids[i] for i in order[:n]]
 
     def pollLatest(self) -> StreamingUpdate | None:
         if self.closed:
@@ -244,7 +272,8 @@ class StreamingAdapter:
                 break
             self.pendingCursor += 1
             slots = self.cloud.addBatchesAsync(chunk.xyzLow, chunk.xyzMed, chunk.xyzHigh,
-                                               chunk.colors, chunk.levels, chunk.batches)
+                                               chunk.colors, chunk.levels, chunk.batches,
+                                               borrow=chunk.pinned)
             self.slotsByChunk[chunk.id] = slots
             dirty = True
             uploaded += 1

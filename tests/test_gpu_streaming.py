@@ -72,6 +72,21 @@ def test_async_upload_matches_sync_add(cr, orc, ctx, streaming):
     ia, ib = render(cr, ctx, a), render(cr, ctx, b)
     assert np.array_equal(ia[0], ib[0]) and np.array_equal(ia[1], ib[1])
     assert ia[1]["count"].any()
+    # Borrowed page-locked arrays (no staging copy): the same pool.
+    arena = streaming.pin_chunks(chunks)
+    c2 = new_cloud(cr, ctx, packed, 400)
+    sc = []
+    for c in chunks:
+        sc += c2.addBatchesAsync(c.xyzLow, c.xyzMed, c.xyzHigh, c.colors, c.levels, c.batches,
+                                 borrow=True)
+    c2.waitUploads()
+    assert sc == sa
+    pc = c2.points()
+    for f in ("xyzLow", "xyzMed", "xyzHigh", "colors", "levels"):
+        assert np.array_equal(pc[f], pb[f]), f
+    assert np.array_equal(c2.batches(), b.batches())
+    c2.close()
+    arena.close()
 
 
 def test_unpublished_slots_are_not_drawn_and_removal_cancels(cr, orc, ctx, streaming):

@@ -47,7 +47,7 @@ class PoolModel:
     def pointCount(self):
         return sum(self.resident.values())
 
-    def addBatchesAsync(self, low, med, high, colors, levels, batches):
+    def addBatchesAsync(self, low, med, high, colors, levels, batches, borrow=False):
         assert len(batches) <= len(self.free)
         slots = [self.free.pop() for _ in range(len(batches))]
         self.assigned_history.extend(slots)
