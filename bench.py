@@ -82,6 +82,8 @@ def parse_args():
     ap.add_argument("--stream-points", type=int, default=20_000_000,
                     help="points of the streaming-residency leg (0 = skip it)")
     ap.add_argument("--stream-frames", type=int, default=96)
+    ap.add_argument("--ply-points", type=int, default=20_000_000,
+                    help="points of the PLY leg's binary file (ASCII: a tenth; 0 = skip it)")
     ap.add_argument("--shard", default="frames", choices=["frames", "points"],
                     help="N>1: every rank renders its own frames of its own copy of the cloud "
                          "(frames, weak scaling), or every frame is split by batches over the "
@@ -522,9 +524,63 @@ def run_ours(args, dist):
         out["differentiable"] = run_differentiable(args, cr, ctx, torch, dist)
     if args.stream_points > 0:
         out["streaming"] = run_streaming(args, cr, ctx, dist)
+    if args.ply_points > 0 and dist.rank == 0:
+        out["ply"] = run_ply(args, cr, ctx)
     if args.pack_points > 0:
         cloud.close()
         out["packer"] = run_packer(args, cr, ctx, torch, dist)
+    return out
+
+
+def run_ply(args, cr, ctx):
+    """PLY input: a binary little-endian file of --ply-points vertices (float
+    x, y, z; uchar red, green, blue, alpha: 16 B each) and an ASCII file of a
+    tenth as many, written to a temporary directory; parsed with every host
+    thread and with one (the reference's loader is single-threaded), and the
+    binary file loaded end to end (parse + GPU pack into a slot pool)."""
+    import os
+    import tempfile
+    rng = np.random.default_rng(args.seed ^ 0x91)
+    n = args.ply_points
+    rec = np.zeros(n, np.dtype([("p", "<f4", 3), ("c", "u1", 4)]))
+    rec["p"] = rng.normal(0.0, 100.0, (n, 3))
+    rec["c"] = rng.integers(0, 256, (n, 4))
+    head = ("ply\nformat {fmt} 1.0\nelement vertex {n}\nproperty float x\nproperty float y\n"
+            "property float z\nproperty uchar red\nproperty uchar green\nproperty uchar blue\n"
+            "property uchar alpha\nend_header\n")
+    threads = os.cpu_count() or 1
+    out = {"threads": threads}
+    with tempfile.TemporaryDirectory() as d:
+        bpath, apath = os.path.join(d, "b.ply"), os.path.join(d, "a.ply")
+        with open(bpath, "wb") as f:
+            f.write(head.format(fmt="binary_little_endian", n=n).encode())
+            rec.tofile(f)
+        m = max(1, n // 10)
+        with open(apath, "wb") as f:
+            f.write(head.format(fmt="ascii", n=m).encode())
+            np.savetxt(f, np.column_stack([rec["p"][:m].astype(np.float64),
+                                           rec["c"][:m].astype(np.float64)]),
+                       fmt=["%.7g"] * 3 + ["%d"] * 4)
+        for name, path, cnt in (("binary", bpath, n), ("ascii", apath, m)):
+            size = os.path.getsize(path)
+            cr.PLYPointCloudLoader.read(path, threads=threads)  # page cache warm
+            res = {"points": cnt, "mb": round(size / 1e6, 1)}
+            for key, th in (("all_threads", threads), ("one_thread", 1)):
+                t0 = time.perf_counter()
+                pos, col = cr.PLYPointCloudLoader.read(path, threads=th)
+                dt = time.perf_counter() - t0
+                res[key] = {"s": round(dt, 4), "mb_per_s": round(size / 1e6 / dt, 1),
+                            "mpts_per_s": round(cnt / 1e6 / dt, 2)}
+            res["speedup"] = round(res["one_thread"]["s"] / res["all_threads"]["s"], 2)
+            out[name] = res
+        pos = col = None
+        t0 = time.perf_counter()
+        cloud = cr.PLYPointCloudLoader.load(ctx, bpath, pointsPerBatch=10240, threads=threads)
+        ctx.synchronize()
+        out["binary_load_s"] = round(time.perf_counter() - t0, 4)
+        out["binary_load_points"] = cloud.pointCount
+        cloud.close()
+    out["timing"] = "wall clock; files in the page cache; load = parse + GPU pack"
     return out
 
 

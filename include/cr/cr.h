@@ -69,7 +69,8 @@ typedef enum cr_status {
     CR_ERR_CAPACITY = 5,         /* slot pool or fixed buffer too small      */
     CR_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up       */
     CR_ERR_NO_DEVICE = 7,        /* no CUDA device / library not usable      */
-    CR_ERR_INTERNAL = 8
+    CR_ERR_INTERNAL = 8,
+    CR_ERR_FORMAT = 9            /* malformed input file (detail: the case)  */
 } cr_status;
 
 /* ------------------------------------------------------------------------ */
@@ -634,6 +635,45 @@ CR_API cr_status cr_cull_noalloc(const cr_raster_batch *batches, uint32_t nbatch
                                  const cr_config *config, const cr_camera *camera, int width,
                                  int height, cr_visible_batch *visible, uint32_t *count,
                                  void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* PLY input (PLYPointCloudLoader, PLYPointCloudLoader.swift:33-369)          */
+/* ------------------------------------------------------------------------ */
+/* Header of a PLY file: vertexCount vertices from bodyOffset, format 0 =
+ * ascii, 1 = binary_little_endian, propertyCount vertex properties (stride
+ * bytes per binary vertex), colorProperties of them red / green / blue. */
+typedef struct cr_ply_header {
+    uint64_t vertexCount;
+    uint64_t bodyOffset;
+    uint32_t format;
+    uint32_t propertyCount;
+    uint32_t stride;
+    uint32_t colorProperties;
+} cr_ply_header;
+
+/* PLYPointCloudLoader.parse's header step (parseHeader, :171-240, and
+ * PLYVertexLayout, :140-158).  Errors are CR_ERR_FORMAT with the reference's
+ * PLYPointCloudLoaderError case as the detail (cr_last_error_detail):
+ * invalidHeader, unsupportedFormat(f), missingVertexElement,
+ * missingProperty(x, y, z), unsupportedProperty(p), truncatedBody (also when
+ * the body cannot hold vertexCount vertices). */
+CR_API cr_status cr_ply_read_header(const uint8_t *data, uint64_t size, cr_ply_header *out);
+
+/* The vertices of a PLY file in memory as float4 positions (x, y, z, 1) and
+ * float4 colours (r, g, b, 1 in [0, 1]; white without colour properties),
+ * vertexCount of each: the inputs of cr_pack (16-byte position stride,
+ * CR_COLOR_F32X4), as the reference's parseASCII / parseBinaryLittleEndian
+ * (:242-305) hand them to PackedPointCloudFixtures.pack.  threads <= 0 uses
+ * every host core; the result does not depend on it.  ASCII errors:
+ * truncatedBody, invalidASCIIValue(line: n, property: p) for the first
+ * failing vertex line. */
+CR_API cr_status cr_ply_parse(const uint8_t *data, uint64_t size, int threads, float *positions,
+                              float *colors);
+
+/* A file mapped read-only into memory (the reference's Data(contentsOf:
+ * options: .mappedIfSafe)); an empty file maps to (NULL, 0). */
+CR_API cr_status cr_file_map(const char *path, const uint8_t **data, uint64_t *size);
+CR_API cr_status cr_file_unmap(const uint8_t *data, uint64_t size);
 
 #ifdef __cplusplus
 } /* extern "C" */

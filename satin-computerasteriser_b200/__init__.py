@@ -32,7 +32,7 @@ __all__ = ["Context", "ComputeRasteriserConfiguration", "ComputeRasteriserCapaci
            "identity_files", "matrix_multiply", "GPUPacker", "PackInput", "DeviceBuffer",
            "HostBuffer", "TerrainParams", "synth_terrain", "synth_lattice", "terrain_height",
            "PASS_NAMES", "MultiViewRasteriser", "l2_loss", "STAGE_DEPTH", "STAGE_COLOR",
-           "STAGE_RESOLVE", "STAGE_ALL"]
+           "STAGE_RESOLVE", "STAGE_ALL", "PLYPointCloudLoader", "PLYPointCloudLoaderError"]
 
 PASS_NAMES = ("clear", "cull", "depth", "color", "resolve", "hole_fill")
 STAGE_DEPTH, STAGE_COLOR, STAGE_RESOLVE, STAGE_ALL = 1, 2, 4, 7  # cr_stage
@@ -1067,3 +1067,6 @@ def l2_loss(context: Context, image: DeviceBuffer, target: DeviceBuffer, scale: 
                                float(scale), C.c_void_p(dL_dimage.ptr),
                                C.byref(loss) if want_loss else None))
     return loss.value if want_loss else None
+
+
+from .ply import PLYPointCloudLoader, PLYPointCloudLoaderError  # noqa: E402

@@ -76,6 +76,12 @@ class cr_frame_planes(C.Structure):
                 ("stream", C.c_void_p)]
 
 
+class cr_ply_header(C.Structure):
+    _fields_ = [("vertexCount", C.c_uint64), ("bodyOffset", C.c_uint64), ("format", C.c_uint32),
+                ("propertyCount", C.c_uint32), ("stride", C.c_uint32),
+                ("colorProperties", C.c_uint32)]
+
+
 class cr_tuning(C.Structure):
     _fields_ = [("chunkPoints", C.c_int32), ("useTiles", C.c_int32),
                 ("viewGroupPixels", C.c_int32)]
@@ -125,6 +131,10 @@ PROTOTYPES = {
     "cr_cloud_poll_uploads": (C.c_int, [P, C.c_int, P, P]),
     "cr_cloud_wait_uploads": (C.c_int, [P, C.c_int]),
     "cr_cloud_set_upload_staging": (C.c_int, [P, u64]),
+    "cr_ply_read_header": (C.c_int, [P, u64, C.POINTER(cr_ply_header)]),
+    "cr_ply_parse": (C.c_int, [P, u64, C.c_int, P, P]),
+    "cr_file_map": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
+    "cr_file_unmap": (C.c_int, [P, u64]),
     "cr_render_stages": (C.c_int, [P, P, P, u32, C.POINTER(cr_config), C.POINTER(cr_camera),
                                    u32]),
     "cr_frame_device_planes": (C.c_int, [P, C.POINTER(cr_frame_planes)]),
@@ -198,6 +208,10 @@ def lib():
         fn.argtypes = args
     _lib = L
     return L
+
+
+def last_error_detail() -> str:
+    return lib().cr_last_error_detail().decode(errors="replace")
 
 
 def check(status: int) -> None:
