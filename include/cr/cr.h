@@ -155,11 +155,11 @@ typedef struct cr_config {
     float minimumPointSize;    /* default 1                         */
     float maximumPointSize;    /* default 1                         */
     float pointSizeScale;      /* default 1                         */
-    int32_t applyDisplacement; /* default 0 (unsupported if set)    */
-    int32_t applyTint;         /* default 0 (unsupported if set)    */
-    int32_t tintAlphaIsCoverage; /* default 0 (unsupported if set)  */
+    int32_t applyDisplacement; /* default 0 (cr_cloud_attribute)    */
+    int32_t applyTint;         /* default 0 (cr_cloud_attribute)    */
+    int32_t tintAlphaIsCoverage; /* default 0: tint a = coverage    */
     int32_t writesSceneDepth;  /* default 1 (composite only)        */
-    float motionBlur;          /* default 0 (unsupported if > 0)    */
+    float motionBlur;          /* default 0 (velocity scale)        */
     int32_t motionBlurSamples; /* default 8                         */
     float motionBlurMaxSpread; /* default 64                        */
 } cr_config;
@@ -246,6 +246,52 @@ CR_API cr_status cr_cloud_add_batches(cr_cloud *cloud,
 /* removeBatches(slots:commit:) — ComputeRasteriserPointCloud.swift:460-473. */
 CR_API cr_status cr_cloud_remove_batches(cr_cloud *cloud, const int32_t *slots, uint32_t n,
                                          int commit);
+
+/* Per-point float4 attributes of the colour variants (ColorPass/Shaders.metal
+ * :38-42, DepthPass/Shaders.metal:30-34): the buffers a user kernel writes
+ * before cr_render, as the reference's DisplacementPass / TintPass sketches
+ * write the cloud's displacement and tint buffers.  One float4 per pool
+ * point (index = the point's pool index, RasterBatch.firstPoint + i), *count
+ * of them; allocated zeroed on first request and valid until the cloud is
+ * reallocated, released or destroyed; write them on the context's stream
+ * (cr_context_stream) or synchronise first.
+ *   CR_ATTR_DISPLACEMENT       xyz added to the decoded position when
+ *                              config.applyDisplacement; a NaN component
+ *                              drops the point from both passes
+ *   CR_ATTR_PREV_DISPLACEMENT  the previous frame's displacement (motion
+ *                              blur); cr_render copies the displacement here
+ *                              after each frame's colour pass while
+ *                              config.motionBlur > 0
+ *   CR_ATTR_TINT               rgba with config.applyTint: colour = mix(colour,
+ *                              saturate(rgb), saturate(a)); a < 0 drops the
+ *                              point's colour; with tintAlphaIsCoverage,
+ *                              coverage = saturate(1 - a) for the
+ *                              weighted-blended accumulation
+ * A cloud without a buffer reads zeros.  The variants run in cr_render
+ * (and cr_render_stages) only; batched views and the differentiable colours
+ * return CR_ERR_UNSUPPORTED while they are on. */
+typedef enum cr_attribute {
+    CR_ATTR_DISPLACEMENT = 0,
+    CR_ATTR_PREV_DISPLACEMENT = 1,
+    CR_ATTR_TINT = 2
+} cr_attribute;
+CR_API cr_status cr_cloud_attribute(cr_cloud *cloud, int32_t which, void **device_ptr,
+                                    uint64_t *count);
+CR_API cr_status cr_cloud_release_attribute(cr_cloud *cloud, int32_t which);
+
+/* The cloud's device arrays, for user kernels that compute the attributes
+ * (the buffers the reference's DisplacementPass / TintPass bind for their
+ * sketches: batches, split-precision words, levels, colours).  Read-only for
+ * the caller; valid until the cloud is reallocated or destroyed. */
+typedef struct cr_cloud_arrays {
+    const cr_raster_batch *batches; /* maxResidentBatches slots */
+    const uint32_t *xyzLow, *xyzMed, *xyzHigh, *colors;
+    const uint8_t *levels;
+    uint64_t points; /* pool points (maxResidentBatches * pointsPerBatch) */
+    uint32_t slots;
+    uint32_t pointsPerBatch;
+} cr_cloud_arrays;
+CR_API cr_status cr_cloud_device_arrays(cr_cloud *cloud, cr_cloud_arrays *out);
 
 /* Asynchronous addBatches for streaming residency: takes the slots at once
  * (slots_out) and copies the points into them while frames render.  The

@@ -56,7 +56,10 @@ class orc_config(C.Structure):
                 ("holeFillIterations", C.c_int32), ("colorizeChunks", C.c_int32),
                 ("colorizeOverdraw", C.c_int32), ("pointSizeMode", C.c_int32),
                 ("minimumPointSize", C.c_float), ("maximumPointSize", C.c_float),
-                ("pointSizeScale", C.c_float)]
+                ("pointSizeScale", C.c_float), ("applyDisplacement", C.c_int32),
+                ("applyTint", C.c_int32), ("tintAlphaIsCoverage", C.c_int32),
+                ("motionBlur", C.c_float), ("motionBlurSamples", C.c_int32),
+                ("motionBlurMaxSpread", C.c_float)]
 
 
 class orc_cloud(C.Structure):
@@ -64,7 +67,8 @@ class orc_cloud(C.Structure):
                 ("files", C.POINTER(orc_file)), ("fileCount", C.c_uint32),
                 ("xyzLow", C.POINTER(C.c_uint32)), ("xyzMed", C.POINTER(C.c_uint32)),
                 ("xyzHigh", C.POINTER(C.c_uint32)), ("colors", C.POINTER(C.c_uint32)),
-                ("levels", C.POINTER(C.c_uint8))]
+                ("levels", C.POINTER(C.c_uint8)), ("displacements", C.c_void_p),
+                ("prevDisplacements", C.c_void_p), ("tints", C.c_void_p)]
 
 
 # numpy dtypes with the same layouts (RasterBatch 64 B, RasterFile 256 B, VisibleBatch 16 B).
@@ -89,6 +93,8 @@ def _load():
     P = C.c_void_p
     lib.orc_log2f.restype = C.c_float
     lib.orc_log2f.argtypes = [C.c_float]
+    lib.orc_exp_neg.restype = C.c_float
+    lib.orc_exp_neg.argtypes = [C.c_float]
     lib.orc_hash_unit.restype = C.c_float
     lib.orc_hash_unit.argtypes = [C.c_uint32]
     lib.orc_depth_to_uint.restype = C.c_uint32
@@ -131,6 +137,11 @@ def _mat(m):
 
 def log2f(x: float) -> float:
     return _load().orc_log2f(x)
+
+
+def exp_neg(x: float) -> float:
+    """The project's e^-x (x >= 0) shared by the coverage resolve and the oracle."""
+    return _load().orc_exp_neg(x)
 
 
 def hash_unit(x: int) -> float:
@@ -186,6 +197,12 @@ class Config:
     minimumPointSize: float = 1.0
     maximumPointSize: float = 1.0
     pointSizeScale: float = 1.0
+    applyDisplacement: bool = False
+    applyTint: bool = False
+    tintAlphaIsCoverage: bool = False
+    motionBlur: float = 0.0
+    motionBlurSamples: int = 8
+    motionBlurMaxSpread: float = 64.0
 
     def to_c(self) -> orc_config:
         c = orc_config()
@@ -208,6 +225,9 @@ class Cloud:
     xyzHigh: np.ndarray
     colors: np.ndarray
     levels: np.ndarray
+    displacements: np.ndarray | None = None      # float32 [points, 4]
+    prevDisplacements: np.ndarray | None = None  # float32 [points, 4]
+    tints: np.ndarray | None = None              # float32 [points, 4]
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> orc_cloud:
@@ -229,6 +249,12 @@ class Cloud:
         c.xyzHigh = arrs[4].ctypes.data_as(C.POINTER(C.c_uint32))
         c.colors = arrs[5].ctypes.data_as(C.POINTER(C.c_uint32))
         c.levels = arrs[6].ctypes.data_as(C.POINTER(C.c_uint8))
+        for name in ("displacements", "prevDisplacements", "tints"):
+            a = getattr(self, name)
+            if a is not None:
+                a = np.ascontiguousarray(a, dtype=np.float32).reshape(-1, 4)
+                self._keep.append(a)
+                setattr(c, name, a.ctypes.data)
         return c
 
 

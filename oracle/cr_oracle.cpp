@@ -105,6 +105,36 @@ float log2_contract(float x) {
 
 // depthToUintReverseZ / uintToDepthReverseZ (Common.metal:10-16).  The constant
 // float(CR_MAX_DEPTH - 1u) rounds to 4294967296.0f.
+// e^-x for x >= 0 (the coverage resolve's alpha), written for this project:
+// Cody-Waite range reduction (Cody and Waite, Software Manual for the
+// Elementary Functions, 1980): n = floor(x log2 e), r = (x - n ln2_hi) -
+// n ln2_lo with ln2_hi exact in 15 bits, so n ln2_hi is exact; e^-r by its
+// Taylor series to degree 9 (Horner, every operation rounded); an exact
+// power-of-two scale 2^-n.  The kernels evaluate the same operations.
+inline float exp_neg(float x) {
+    if (x != x) return x;
+    if (!(x > 0.0f)) return 1.0f;
+    const float t = x * 1.44269504f;
+    if (t >= 126.0f) return 0.0f;
+    const float n = std::floor(t);
+    const float r = (x - n * 0.693145751953125f) - n * 1.42860682e-06f;
+    const float z = 0.0f - r;
+    float p = 2.75573192e-06f;
+    p = p * z + 2.48015873e-05f;
+    p = p * z + 1.98412698e-04f;
+    p = p * z + 1.38888889e-03f;
+    p = p * z + 8.33333333e-03f;
+    p = p * z + 4.16666667e-02f;
+    p = p * z + 1.66666667e-01f;
+    p = p * z + 0.5f;
+    p = p * z + 1.0f;
+    p = p * z + 1.0f;
+    uint32_t bits = (uint32_t)(127 - (int)n) << 23;
+    float scale;
+    std::memcpy(&scale, &bits, 4);
+    return p * scale;
+}
+
 inline uint32_t depth_to_uint(float z) { return f2u(saturate_(z) * 4294967296.0f); }
 inline float uint_to_depth(uint32_t d) { return u2f(d) / 4294967296.0f; }
 
@@ -369,9 +399,160 @@ struct pass_args {
     uint32_t *depth;  // HQS depth plane or nearest depth plane
     uint32_t *accum;  // HQS r,g,b,count
     uint32_t *index;  // nearest index plane
+    bool variant = false;  // HQS colour variants on (run_batch_variant)
 };
 
+inline float saturate_nan0(float x) { return fmin_(fmax_(x, 0.0f), 1.0f); }  // NaN -> 0
+
+inline f4 attr(const float *a, uint32_t i) {
+    if (!a) return f4{0.0f, 0.0f, 0.0f, 0.0f};
+    return f4{a[4 * (size_t)i], a[4 * (size_t)i + 1], a[4 * (size_t)i + 2], a[4 * (size_t)i + 3]};
+}
+
+// The depth and colour passes with the colour variants on: displacement
+// (DepthPass/Shaders.metal:63-71, ColorPass/Shaders.metal:70-77), tint mix and
+// discard (ColorPass :116-140, DepthPass :56-60), coverage / motion-blur
+// weighted-blended accumulation without a depth test, fixed point S = 4096
+// (ColorPass :109-199).  One point at a time in the reference's order.
+void run_batch_variant(const pass_args &a, pass_kind kind, uint32_t v, bool mt) {
+    const orc_cloud &c = *a.cloud;
+    const orc_visible &vb = a.vis[v];
+    const orc_batch &b = c.batches[vb.batchIndex];
+    const orc_file &file = c.files[b.fileIndex];
+    const orc_config &cfg = *a.cfg;
+    const int sw = a.sw, sh = a.sh;
+    const bool coverage_mode = cfg.applyTint != 0 && cfg.tintAlphaIsCoverage != 0;
+    const bool mb_on = cfg.motionBlur > 0.0f;
+    const bool oit = coverage_mode || mb_on;
+    for (uint32_t local = 0; local < vb.activePoints; ++local) {
+        const uint32_t pi = b.firstPoint + local;
+        const float pointLevel = u2f((uint32_t)c.levels[pi] & 7u);
+        const float dither = (cfg.enableLODDither != 0) ? hash_unit(pi) : 0.5f;
+        if (dither >= (vb.lodThreshold - pointLevel) + 0.5f) continue;
+        if (kind == PASS_DEPTH && coverage_mode && attr(c.tints, pi).w < 0.0f) continue;
+        const f3 base = decode_point(pi, b, c, vb.level);
+        f3 p = base;
+        if (cfg.applyDisplacement != 0) {
+            const f4 d = attr(c.displacements, pi);
+            p = f3{p.x + d.x, p.y + d.y, p.z + d.z};
+            if (p.x != p.x || p.y != p.y || p.z != p.z) continue;
+        }
+        const f4 clip = mulv(file.transform, f4{p.x, p.y, p.z, 1.0f});
+        if (clip.w <= 0.0f) continue;
+        const float nx = clip.x / clip.w, ny = clip.y / clip.w, nz = clip.z / clip.w;
+        if (nx < -1.0f || ny < -1.0f || nx > 1.0f || ny > 1.0f || nz < 0.0f || nz > 1.0f) continue;
+        int px = f2i((nx * 0.5f + 0.5f) * (float)sw);
+        int py = f2i((ny * 0.5f + 0.5f) * (float)sh);
+        if (px < 0 || px >= sw || py < 0 || py >= sh) continue;
+        py = sh - 1 - py;
+        if (kind == PASS_DEPTH) {
+            const uint32_t depth = depth_to_uint(nz);
+            const int rad = footprint_radius(p, file, a.view, a.proj, sw, sh, cfg);
+            for (int oy = -rad; oy <= rad; ++oy)
+                for (int ox = -rad; ox <= rad; ++ox) {
+                    if (!inside_footprint(ox, oy, rad)) continue;
+                    const int tx = px + ox, ty = py + oy;
+                    if (tx < 0 || tx >= sw || ty < 0 || ty >= sh) continue;
+                    atomic_max_u32(&a.depth[(uint32_t)(ty * sw + tx)], depth, mt);
+                }
+            continue;
+        }
+        uint32_t color = c.colors[pi];
+        if (cfg.colorizeChunks != 0)
+            color = vb.batchIndex * 1234567u;
+        else if (cfg.colorizeOverdraw != 0)
+            color = 0x00010101u;
+        uint32_t r = color & 0xffu, g = (color >> 8) & 0xffu, bl = (color >> 16) & 0xffu;
+        float cov = 1.0f;
+        if (cfg.applyTint != 0) {
+            const f4 t = attr(c.tints, pi);
+            if (t.w < 0.0f) continue;
+            if (coverage_mode) {
+                cov = saturate_nan0(1.0f - t.w);
+            } else {
+                const float w = saturate_nan0(t.w);
+                const float k = 1.0f / 255.0f;
+                const float ox = u2f(r) * k, oy = u2f(g) * k, oz = u2f(bl) * k;
+                const float mx = ox + (saturate_nan0(t.x) - ox) * w;  // mix(orig, tint, w)
+                const float my = oy + (saturate_nan0(t.y) - oy) * w;
+                const float mz = oz + (saturate_nan0(t.z) - oz) * w;
+                r = f2u(saturate_nan0(mx) * 255.0f + 0.5f);
+                g = f2u(saturate_nan0(my) * 255.0f + 0.5f);
+                bl = f2u(saturate_nan0(mz) * 255.0f + 0.5f);
+            }
+        }
+        if (oit && cov <= 0.0f) continue;
+        const int rad = footprint_radius(p, file, a.view, a.proj, sw, sh, cfg);
+        int samples = 1;
+        float stepx = 0.0f, stepy = 0.0f;
+        if (mb_on) {
+            f3 pp = base;
+            if (cfg.applyDisplacement != 0) {
+                const f4 d = attr(c.prevDisplacements ? c.prevDisplacements : c.displacements, pi);
+                pp = f3{pp.x + d.x, pp.y + d.y, pp.z + d.z};
+            }
+            const f4 pc = mulv(file.prevTransform, f4{pp.x, pp.y, pp.z, 1.0f});
+            if (pc.w > 0.0f) {
+                const float pnx = pc.x / pc.w, pny = pc.y / pc.w;
+                const int ppx = f2i((pnx * 0.5f + 0.5f) * (float)sw);
+                const int ppy = sh - 1 - f2i((pny * 0.5f + 0.5f) * (float)sh);
+                float vx = (float)((int64_t)px - (int64_t)ppx) * cfg.motionBlur;
+                float vy = (float)((int64_t)py - (int64_t)ppy) * cfg.motionBlur;
+                float len = std::sqrt(vx * vx + vy * vy);
+                if (len > cfg.motionBlurMaxSpread) {
+                    const float k = cfg.motionBlurMaxSpread / len;
+                    vx = vx * k;
+                    vy = vy * k;
+                    len = cfg.motionBlurMaxSpread;
+                }
+                if (len > 0.75f) {
+                    samples = std::min(std::max(f2i(std::ceil(len)), 1), cfg.motionBlurSamples);
+                    samples = std::max(samples, 1);
+                    const float den = (float)std::max(samples - 1, 1);
+                    stepx = vx / den;
+                    stepy = vy / den;
+                }
+            }
+        }
+        const float aN = cov / (float)samples;
+        const float kS = 4096.0f, k255 = 1.0f / 255.0f;
+        const uint32_t caR = f2u(((u2f(r) * k255) * aN) * kS + 0.5f);
+        const uint32_t caG = f2u(((u2f(g) * k255) * aN) * kS + 0.5f);
+        const uint32_t caB = f2u(((u2f(bl) * k255) * aN) * kS + 0.5f);
+        const uint32_t caA = f2u(aN * kS + 0.5f);
+        for (int s = 0; s < samples; ++s) {
+            const int cx = px - f2i(std::round(stepx * (float)s));
+            const int cy = py - f2i(std::round(stepy * (float)s));
+            for (int oy = -rad; oy <= rad; ++oy)
+                for (int ox = -rad; ox <= rad; ++ox) {
+                    if (!inside_footprint(ox, oy, rad)) continue;
+                    const int tx = cx + ox, ty = cy + oy;
+                    if (tx < 0 || tx >= sw || ty < 0 || ty >= sh) continue;
+                    const uint32_t pix = (uint32_t)(ty * sw + tx);
+                    if (oit) {
+                        atomic_add_u32(&a.accum[pix * 4 + 0], caR, mt);
+                        atomic_add_u32(&a.accum[pix * 4 + 1], caG, mt);
+                        atomic_add_u32(&a.accum[pix * 4 + 2], caB, mt);
+                        atomic_add_u32(&a.accum[pix * 4 + 3], caA, mt);
+                        continue;
+                    }
+                    const uint32_t closest = a.depth[pix];
+                    if (closest == 0u) continue;
+                    if (!(nz >= uint_to_depth(closest) * (1.0f - cfg.depthTolerance))) continue;
+                    atomic_add_u32(&a.accum[pix * 4 + 0], r, mt);
+                    atomic_add_u32(&a.accum[pix * 4 + 1], g, mt);
+                    atomic_add_u32(&a.accum[pix * 4 + 2], bl, mt);
+                    atomic_add_u32(&a.accum[pix * 4 + 3], 1u, mt);
+                }
+        }
+    }
+}
+
 void run_batch(const pass_args &a, pass_kind kind, uint32_t v, bool mt) {
+    if (a.variant) {
+        run_batch_variant(a, kind, v, mt);
+        return;
+    }
     const orc_cloud &c = *a.cloud;
     const orc_visible &vb = a.vis[v];
     const orc_batch &b = c.batches[vb.batchIndex];
@@ -477,6 +658,31 @@ void resolve_hqs(const uint32_t *depth, const uint32_t *accum, size_t npix, cons
     }
 }
 
+// resolveUpdate with coverageEnabled (Resolve/Shaders.metal:24-41): the
+// weighted-blended average and alpha 1 - e^-(sum of alpha).
+void resolve_coverage(const uint32_t *depth, const uint32_t *accum, size_t npix, const float *bg,
+                      uint8_t *img, float *dimg) {
+    for (size_t p = 0; p < npix; ++p) {
+        const uint32_t a = accum[p * 4 + 3];
+        uint8_t *o = &img[p * 4];
+        if (a == 0u) {
+            o[0] = unorm8(bg[0]);
+            o[1] = unorm8(bg[1]);
+            o[2] = unorm8(bg[2]);
+            o[3] = unorm8(0.0f);
+            dimg[p] = 0.0f;
+            continue;
+        }
+        const float fa = u2f(a);
+        o[0] = unorm8(u2f(accum[p * 4 + 0]) / fa);
+        o[1] = unorm8(u2f(accum[p * 4 + 1]) / fa);
+        o[2] = unorm8(u2f(accum[p * 4 + 2]) / fa);
+        const float sum_a = fa * (1.0f / 4096.0f);
+        o[3] = unorm8(saturate_nan0(1.0f - exp_neg(sum_a)));
+        dimg[p] = uint_to_depth(depth[p]);
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -485,6 +691,7 @@ void resolve_hqs(const uint32_t *depth, const uint32_t *accum, size_t npix, cons
 extern "C" {
 
 float orc_log2f(float x) { return log2_contract(x); }
+float orc_exp_neg(float x) { return exp_neg(x); }
 float orc_hash_unit(uint32_t x) { return hash_unit(x); }
 uint32_t orc_depth_to_uint(float z) { return depth_to_uint(z); }
 void orc_mat4_mul(const float a[16], const float b[16], float out[16]) { mat4mul(a, b, out); }
@@ -595,17 +802,28 @@ int orc_render(const orc_cloud *clouds, uint32_t nclouds, const orc_config *cfg,
         for (uint32_t ci = 0; ci < nclouds; ++ci)
             if (resident(clouds[ci])) order.push_back(ci);
         for (uint32_t ci : order) cull_cloud(ci);
+        // Colour variants (ComputeRasteriser.swift:229-253): coverage resolve
+        // when translucent defocus or motion blur is on.
+        const bool variant =
+            cfg->applyDisplacement != 0 || cfg->applyTint != 0 || cfg->motionBlur > 0.0f;
+        const bool coverage =
+            (cfg->applyTint != 0 && cfg->tintAlphaIsCoverage != 0) || cfg->motionBlur > 0.0f;
         for (uint32_t ci : order) {
             pass_args a{&clouds[ci], vis[ci].data(), vcount[ci], cfg, view, proj, w, h,
                         depth.data(), accum.data(), nullptr};
+            a.variant = variant;
             run_pass(a, PASS_DEPTH, threads);
         }
         for (uint32_t ci : order) {
             pass_args a{&clouds[ci], vis[ci].data(), vcount[ci], cfg, view, proj, w, h,
                         depth.data(), accum.data(), nullptr};
+            a.variant = variant;
             run_pass(a, PASS_COLOR, threads);
         }
-        resolve_hqs(depth.data(), accum.data(), npix, bg, img.data(), dimg.data());
+        if (coverage)
+            resolve_coverage(depth.data(), accum.data(), npix, bg, img.data(), dimg.data());
+        else
+            resolve_hqs(depth.data(), accum.data(), npix, bg, img.data(), dimg.data());
         if (depth_out) std::memcpy(depth_out, depth.data(), npix * 4);
         if (accum_out) std::memcpy(accum_out, accum.data(), npix * 16);
     } else {

@@ -55,6 +55,12 @@ typedef struct orc_config {
     int32_t enableFrustumCulling, lodBias, enableCLOD, enableLODDither;
     int32_t holeFillIterations, colorizeChunks, colorizeOverdraw, pointSizeMode;
     float minimumPointSize, maximumPointSize, pointSizeScale;
+    /* Colour variants (ColorPass/Shaders.metal:54-199, DepthPass/Shaders.metal:56-71,
+     * Resolve/Shaders.metal:19-41); all off by default. */
+    int32_t applyDisplacement, applyTint, tintAlphaIsCoverage;
+    float motionBlur;
+    int32_t motionBlurSamples;
+    float motionBlurMaxSpread;
 } orc_config;
 
 /* One cloud's slot pool as the device holds it. */
@@ -65,10 +71,15 @@ typedef struct orc_cloud {
     uint32_t fileCount;
     const uint32_t *xyzLow, *xyzMed, *xyzHigh, *colors;
     const uint8_t *levels;
+    /* Per-point float4 attributes of the colour variants (NULL reads zeros):
+     * displacement (xyz), the previous frame's displacement (motion blur;
+     * NULL uses the current one), tint (rgba). */
+    const float *displacements, *prevDisplacements, *tints;
 } orc_cloud;
 
 /* ---- scalar helpers exposed for tests ---- */
 float orc_log2f(float x);
+float orc_exp_neg(float x);
 float orc_hash_unit(uint32_t x);
 uint32_t orc_depth_to_uint(float ndcz);
 void orc_mat4_mul(const float a[16], const float b[16], float out[16]);

@@ -32,7 +32,9 @@ __all__ = ["Context", "ComputeRasteriserConfiguration", "ComputeRasteriserCapaci
            "identity_files", "matrix_multiply", "GPUPacker", "PackInput", "DeviceBuffer",
            "HostBuffer", "TerrainParams", "synth_terrain", "synth_lattice", "terrain_height",
            "PASS_NAMES", "MultiViewRasteriser", "l2_loss", "STAGE_DEPTH", "STAGE_COLOR",
-           "STAGE_RESOLVE", "STAGE_ALL", "PLYPointCloudLoader", "PLYPointCloudLoaderError"]
+           "STAGE_RESOLVE", "STAGE_ALL", "PLYPointCloudLoader", "PLYPointCloudLoaderError",
+           "DeviceView", "DisplacementPass", "TintPass", "ATTR_DISPLACEMENT",
+           "ATTR_PREV_DISPLACEMENT", "ATTR_TINT"]
 
 PASS_NAMES = ("clear", "cull", "depth", "color", "resolve", "hole_fill")
 STAGE_DEPTH, STAGE_COLOR, STAGE_RESOLVE, STAGE_ALL = 1, 2, 4, 7  # cr_stage
@@ -341,6 +343,39 @@ class PackedPointCloud:
         return len(self.batches)
 
 
+class DeviceView:
+    """A device array owned by the library (a cloud's attribute or pool
+    array), with __cuda_array_interface__ for torch / CuPy / numba kernels and
+    host upload / download through the C ABI."""
+
+    def __init__(self, context: Context, ptr: int, shape, dtype, owner=None):
+        self.context = context
+        self.ptr = int(ptr)
+        self.shape = tuple(int(d) for d in shape)
+        self.dtype = np.dtype(dtype)
+        self.nbytes = int(np.prod(self.shape)) * self.dtype.itemsize
+        self._owner = owner  # keeps the cloud alive
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": self.shape, "typestr": self.dtype.str, "data": (self.ptr, False),
+                "version": 3, "strides": None}
+
+    def upload(self, host: np.ndarray):
+        h = np.ascontiguousarray(host, dtype=self.dtype)
+        N.check(N.lib().cr_buffer_upload(self.context.handle, C.c_void_p(self.ptr), N.ptr(h),
+                                         min(h.nbytes, self.nbytes)))
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.shape, self.dtype)
+        N.check(N.lib().cr_buffer_download(self.context.handle, N.ptr(out),
+                                           C.c_void_p(self.ptr), out.nbytes))
+        return out
+
+
+ATTR_DISPLACEMENT, ATTR_PREV_DISPLACEMENT, ATTR_TINT = 0, 1, 2  # cr_attribute
+
+
 class ComputeRasteriserPointCloud:
     """ComputeRasteriserPointCloud (ComputeRasteriserPointCloud.swift:59-678).
 
@@ -468,6 +503,44 @@ class ComputeRasteriserPointCloud:
     def setUploadStaging(self, nbytes: int):
         """Size of the page-locked staging ring of the asynchronous uploads."""
         N.check(N.lib().cr_cloud_set_upload_staging(self._h, int(nbytes)))
+
+    # --- colour-variant attributes (displacementBuffer / tintBuffer) ---
+    def _attribute(self, which: int) -> DeviceView:
+        p, n = C.c_void_p(), C.c_uint64()
+        N.check(N.lib().cr_cloud_attribute(self._h, which, C.byref(p), C.byref(n)))
+        return DeviceView(self.context, p.value, (n.value, 4), np.float32, owner=self)
+
+    def displacementBuffer(self) -> DeviceView:
+        """The per-point float4 displacement (xyz) buffer, allocated zeroed on
+        first use (makeDisplacementBuffer, ComputeRasteriserPointCloud.swift)."""
+        return self._attribute(ATTR_DISPLACEMENT)
+
+    def prevDisplacementBuffer(self) -> DeviceView:
+        """The previous frame's displacement (motion blur)."""
+        return self._attribute(ATTR_PREV_DISPLACEMENT)
+
+    def tintBuffer(self) -> DeviceView:
+        """The per-point float4 tint (rgba) buffer (makeTintBuffer)."""
+        return self._attribute(ATTR_TINT)
+
+    def releaseAttribute(self, which: int):
+        N.check(N.lib().cr_cloud_release_attribute(self._h, which))
+
+    def deviceArrays(self) -> dict:
+        """The pool's device arrays for user kernels (read-only): batches
+        (BATCH_DTYPE per slot), xyzLow / xyzMed / xyzHigh / colors (uint32 per
+        point), levels (uint8 per point)."""
+        a = N.cr_cloud_arrays()
+        N.check(N.lib().cr_cloud_device_arrays(self._h, C.byref(a)))
+        ctx, n = self.context, int(a.points)
+        return {"batches": DeviceView(ctx, a.batches, (a.slots, BATCH_DTYPE.itemsize), np.uint8,
+                                      self),
+                "xyzLow": DeviceView(ctx, a.xyzLow, (n,), np.uint32, self),
+                "xyzMed": DeviceView(ctx, a.xyzMed, (n,), np.uint32, self),
+                "xyzHigh": DeviceView(ctx, a.xyzHigh, (n,), np.uint32, self),
+                "colors": DeviceView(ctx, a.colors, (n,), np.uint32, self),
+                "levels": DeviceView(ctx, a.levels, (n,), np.uint8, self),
+                "pointsPerBatch": int(a.pointsPerBatch)}
 
     def removeBatches(self, slots, commit: bool = True):
         """removeBatches (ComputeRasteriserPointCloud.swift:460-473)."""
@@ -978,6 +1051,67 @@ class ComputeRasteriser:
         if self._frame is None:
             raise CRError(1, "no viewport: call resize or update first")
         return self._frame
+
+
+class _UserAttributePass:
+    """Shared machinery of DisplacementPass and TintPass (DisplacementPass.swift,
+    TintPass.swift): per frame, make sure the target cloud has the attribute
+    buffer, run the user kernel on the library's stream with the cloud's
+    device arrays and the output buffer, and switch the variant on in the
+    rasteriser's configuration.  The kernel is any Python callable that
+    launches CUDA work (a torch / CuPy / numba kernel, a custom extension):
+        kernel(arrays: dict, out: DeviceView, stream: int, **user)
+    with arrays from ComputeRasteriserPointCloud.deviceArrays() and stream the
+    context's cudaStream_t (the kernel must run on it, or synchronise)."""
+
+    _which = ATTR_DISPLACEMENT
+
+    def __init__(self, rasteriser: ComputeRasteriser, kernel, **user):
+        self.rasteriser = rasteriser
+        self.kernel = kernel
+        self.user = user
+
+    def _flip(self, cfg):
+        raise NotImplementedError
+
+    def encode(self, cloud: ComputeRasteriserPointCloud | None = None):
+        """Runs the kernel for `cloud` (default: the rasteriser's first cloud);
+        call before encode() so the frame sees this frame's values."""
+        target = cloud or (self.rasteriser.pointClouds[0] if self.rasteriser.pointClouds
+                           else None)
+        if target is None:
+            return
+        out = target._attribute(self._which)
+        self.kernel(target.deviceArrays(), out, self.rasteriser.context.stream(), **self.user)
+        self._flip(self.rasteriser.configuration)
+
+
+class DisplacementPass(_UserAttributePass):
+    """Per-point displacement written by a user kernel (xyz added to each
+    decoded position; a NaN component drops the point); sets
+    configuration.applyDisplacement."""
+
+    _which = ATTR_DISPLACEMENT
+
+    def _flip(self, cfg):
+        cfg.applyDisplacement = True
+
+
+class TintPass(_UserAttributePass):
+    """Per-point tint written by a user kernel (rgba: mix weight a, a < 0
+    drops the point's colour); sets configuration.applyTint, and with
+    alphaIsCoverage tintAlphaIsCoverage (translucent defocus: a is the
+    circle of confusion, coverage = 1 - a, weighted-blended accumulation)."""
+
+    _which = ATTR_TINT
+
+    def __init__(self, rasteriser, kernel, alphaIsCoverage: bool = False, **user):
+        super().__init__(rasteriser, kernel, **user)
+        self.alphaIsCoverage = alphaIsCoverage
+
+    def _flip(self, cfg):
+        cfg.applyTint = True
+        cfg.tintAlphaIsCoverage = bool(self.alphaIsCoverage)
 
 
 class MultiViewRasteriser:

@@ -82,6 +82,12 @@ class cr_ply_header(C.Structure):
                 ("colorProperties", C.c_uint32)]
 
 
+class cr_cloud_arrays(C.Structure):
+    _fields_ = [("batches", C.c_void_p), ("xyzLow", C.c_void_p), ("xyzMed", C.c_void_p),
+                ("xyzHigh", C.c_void_p), ("colors", C.c_void_p), ("levels", C.c_void_p),
+                ("points", C.c_uint64), ("slots", C.c_uint32), ("pointsPerBatch", C.c_uint32)]
+
+
 class cr_tuning(C.Structure):
     _fields_ = [("chunkPoints", C.c_int32), ("useTiles", C.c_int32),
                 ("viewGroupPixels", C.c_int32)]
@@ -135,6 +141,9 @@ PROTOTYPES = {
     "cr_ply_parse": (C.c_int, [P, u64, C.c_int, P, P]),
     "cr_file_map": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
     "cr_file_unmap": (C.c_int, [P, u64]),
+    "cr_cloud_attribute": (C.c_int, [P, i32, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
+    "cr_cloud_release_attribute": (C.c_int, [P, i32]),
+    "cr_cloud_device_arrays": (C.c_int, [P, C.POINTER(cr_cloud_arrays)]),
     "cr_render_stages": (C.c_int, [P, P, P, u32, C.POINTER(cr_config), C.POINTER(cr_camera),
                                    u32]),
     "cr_frame_device_planes": (C.c_int, [P, C.POINTER(cr_frame_planes)]),

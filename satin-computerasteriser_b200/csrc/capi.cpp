@@ -101,6 +101,9 @@ void free_cloud_buffers(cr_cloud *c) {
     dfree(c->d_frag_col);
     dfree(c->d_frag_count);
     dfree(c->d_counters);
+    dfree(c->d_disp);
+    dfree(c->d_prev_disp);
+    dfree(c->d_tint);
 }
 
 }  // namespace
@@ -170,6 +173,11 @@ cr_status alloc_ring(cr_cloud *c) {
     return CR_OK;
 }
 
+// Points of a cloud's per-point attribute buffers: one per pool point.
+size_t attribute_points(const cr_cloud *c) {
+    return (size_t)c->cap.maxResidentBatches * c->cap.pointsPerBatch;
+}
+
 // allocateBuffers + rebuildFilesBuffer + rebuildCullBuffers
 // (ComputeRasteriserPointCloud.swift:532-589).
 cr_status allocate_cloud(cr_cloud *c, cr_capacity cap, const cr_raster_file *files, uint32_t nf) {
@@ -228,14 +236,6 @@ cr_status allocate_cloud(cr_cloud *c, cr_capacity cap, const cr_raster_file *fil
     return CR_OK;
 }
 
-bool config_unsupported(const cr_config *cfg, std::string &why) {
-    if (cfg->applyDisplacement) why = "applyDisplacement (user displacement kernels) is not supported";
-    else if (cfg->applyTint) why = "applyTint (user tint kernels) is not supported";
-    else if (cfg->tintAlphaIsCoverage) why = "tintAlphaIsCoverage (OIT coverage) is not supported";
-    else if (cfg->motionBlur > 0.0f) why = "motionBlur is not supported";
-    else return false;
-    return true;
-}
 
 CullUniforms make_cull_uniforms(const cr_config *cfg, const cr_camera *cam, int w, int h) {
     CullUniforms u;
@@ -300,8 +300,21 @@ cr_status validate_config(const cr_config *cfg) {
         return fail(CR_ERR_INVALID_ARGUMENT, "config.mode must be 0 (HQS) or 1 (nearest)");
     if (cfg->pointSizeMode != 0 && cfg->pointSizeMode != 1)
         return fail(CR_ERR_INVALID_ARGUMENT, "config.pointSizeMode must be 0 or 1");
-    std::string why;
-    if (config_unsupported(cfg, why)) return fail(CR_ERR_UNSUPPORTED, why);
+    if (cfg->motionBlur > 0.0f && cfg->motionBlurSamples < 1)
+        return fail(CR_ERR_INVALID_ARGUMENT, "config.motionBlurSamples must be at least 1");
+    return CR_OK;
+}
+
+bool variants_on(const cr_config *cfg) {
+    return cfg->mode == CR_MODE_HIGH_QUALITY_AVERAGE &&
+           (cfg->applyDisplacement || cfg->applyTint || cfg->motionBlur > 0.0f);
+}
+
+cr_status reject_variants(const cr_config *cfg, const char *where) {
+    if (variants_on(cfg))
+        return fail(CR_ERR_UNSUPPORTED, std::string(where) +
+                                            ": the colour variants (displacement, tint, "
+                                            "coverage, motion blur) need cr_render");
     return CR_OK;
 }
 
@@ -646,6 +659,53 @@ CR_API cr_status cr_cloud_update_files(cr_cloud *c, const float vp[16], const fl
     return upload_files(c, snap);
 }
 
+CR_API cr_status cr_cloud_attribute(cr_cloud *c, int32_t which, void **device_ptr,
+                                    uint64_t *count) {
+    if (!c || !device_ptr) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    float4 **slot = which == CR_ATTR_DISPLACEMENT        ? &c->d_disp
+                    : which == CR_ATTR_PREV_DISPLACEMENT ? &c->d_prev_disp
+                    : which == CR_ATTR_TINT               ? &c->d_tint
+                                                          : nullptr;
+    if (!slot) return fail(CR_ERR_INVALID_ARGUMENT, "unknown attribute");
+    DeviceGuard g(c->ctx->device);
+    const size_t n = attribute_points(c);
+    if (!*slot) {
+        cr_status st = dalloc(slot, n * sizeof(float4));
+        if (st) return st;
+        CR_CUDA(cudaMemsetAsync(*slot, 0, n * sizeof(float4), c->ctx->stream));
+    }
+    *device_ptr = *slot;
+    if (count) *count = n;
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_release_attribute(cr_cloud *c, int32_t which) {
+    if (!c) return fail(CR_ERR_INVALID_ARGUMENT, "cloud is null");
+    float4 **slot = which == CR_ATTR_DISPLACEMENT        ? &c->d_disp
+                    : which == CR_ATTR_PREV_DISPLACEMENT ? &c->d_prev_disp
+                    : which == CR_ATTR_TINT               ? &c->d_tint
+                                                          : nullptr;
+    if (!slot) return fail(CR_ERR_INVALID_ARGUMENT, "unknown attribute");
+    DeviceGuard g(c->ctx->device);
+    CR_CUDA(cudaStreamSynchronize(c->ctx->stream));
+    dfree(*slot);
+    return CR_OK;
+}
+
+CR_API cr_status cr_cloud_device_arrays(cr_cloud *c, cr_cloud_arrays *out) {
+    if (!c || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
+    out->batches = c->d_batches;
+    out->xyzLow = c->d_low;
+    out->xyzMed = c->d_med;
+    out->xyzHigh = c->d_high;
+    out->colors = c->d_colors;
+    out->levels = c->d_levels;
+    out->points = (uint64_t)c->cap.maxResidentBatches * c->cap.pointsPerBatch;
+    out->slots = c->cap.maxResidentBatches;
+    out->pointsPerBatch = c->cap.pointsPerBatch;
+    return CR_OK;
+}
+
 CR_API cr_status cr_cloud_info_get(const cr_cloud *c, cr_cloud_info *out) {
     if (!c || !out) return fail(CR_ERR_INVALID_ARGUMENT, "null argument");
     out->capacity = c->cap;
@@ -802,15 +862,22 @@ static cr_status render_impl(cr_context *ctx, cr_frame *f, cr_cloud *const *clou
                 max_samples += (uint64_t)clouds[i]->resident * clouds[i]->cap.pointsPerBatch;
             }
         const RasterUniforms rau = make_raster_uniforms(cfg, cam, W, H);
+        // Colour variants (ComputeRasteriser.swift:229-253): their own depth
+        // and colour passes with 32-bit adds, and the coverage resolve when
+        // translucent defocus or motion blur is on.
+        const bool variants = variants_on(cfg);
+        const bool coverage =
+            variants && ((cfg->applyTint && cfg->tintAlphaIsCoverage) || cfg->motionBlur > 0.0f);
         // With single-pixel footprints the depth pass keeps every point that
         // reaches the screen as a fragment and the colour pass reads those
         // instead of decoding and projecting the points again.
-        const bool frags = std::fmax(cfg->minimumPointSize, cfg->maximumPointSize) <= 1.0f;
+        const bool frags =
+            !variants && std::fmax(cfg->minimumPointSize, cfg->maximumPointSize) <= 1.0f;
         // Packed colour adds while the frame holds fewer than 2^31 samples:
         // then a pixel's count field reads its true count plus at most 127
         // carries out of the blue sum, so a read count of at most
         // kPackedMaxCount proves that no field carried.
-        const bool packed = (stages & CR_STAGE_COLOR) && (stages & CR_STAGE_RESOLVE) &&
+        const bool packed = !variants && (stages & CR_STAGE_COLOR) && (stages & CR_STAGE_RESOLVE) &&
                             max_samples < (1ull << 31);
         RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
         t.packed = packed ? 1 : 0;
@@ -829,20 +896,38 @@ static cr_status render_impl(cr_context *ctx, cr_frame *f, cr_cloud *const *clou
             {
                 PassTimer pt(ctx, CR_PASS_DEPTH);
                 for (cr_cloud *c : resident)
-                    if ((st = launch_raster(c, frags ? PASS_DEPTH_FRAG : PASS_DEPTH, rau, t, s)))
+                    if ((st = variants ? launch_variant_pass(c, false, rau, *cfg, t, s)
+                                       : launch_raster(c, frags ? PASS_DEPTH_FRAG : PASS_DEPTH,
+                                                       rau, t, s)))
                         return st;
             }
         }
         if (stages & CR_STAGE_COLOR) {
             PassTimer pt(ctx, CR_PASS_COLOR);
             for (cr_cloud *c : resident)
-                if ((st = launch_raster(c, frags ? PASS_COLOR_FRAG : PASS_COLOR, rau, t, s)))
+                if ((st = variants ? launch_variant_pass(c, true, rau, *cfg, t, s)
+                                   : launch_raster(c, frags ? PASS_COLOR_FRAG : PASS_COLOR, rau,
+                                                   t, s)))
                     return st;
+            // Motion blur: this frame's displacement is the next frame's
+            // previous one (ComputeRasteriser.swift:453-480).
+            if (variants && cfg->motionBlur > 0.0f)
+                for (cr_cloud *c : resident) {
+                    if (!c->d_disp) continue;
+                    const size_t bytes = attribute_points(c) * sizeof(float4);
+                    if (!c->d_prev_disp && (st = dalloc(&c->d_prev_disp, bytes))) return st;
+                    CR_CUDA(cudaMemcpyAsync(c->d_prev_disp, c->d_disp, bytes,
+                                            cudaMemcpyDeviceToDevice, s));
+                }
         }
         if (stages & CR_STAGE_RESOLVE) {
             PassTimer pt(ctx, CR_PASS_RESOLVE);
             if ((st = frame_copy_fence(f, s))) return st;
-            if ((st = launch_resolve_hqs(f, ru, s, packed, nullptr))) return st;
+            if (coverage) {
+                if ((st = launch_resolve_coverage(f, ru, s))) return st;
+            } else if ((st = launch_resolve_hqs(f, ru, s, packed, nullptr))) {
+                return st;
+            }
             if (packed) {
                 // Exact re-run, which returns at once unless the resolve set
                 // the redo flag: zero the accumulators, colour pass with one
@@ -1039,7 +1124,7 @@ static cr_status validate_f32(cr_context *ctx, cr_frame *f, cr_cloud *cloud, con
         return fail(CR_ERR_UNSUPPORTED, "differentiable colours need the HQS mode");
     if (cfg->colorizeChunks || cfg->colorizeOverdraw)
         return fail(CR_ERR_UNSUPPORTED, "colorize options replace the learnable colours");
-    return CR_OK;
+    return reject_variants(cfg, "differentiable colours");
 }
 
 CR_API cr_status cr_hqs_forward_f32(cr_context *ctx, cr_frame *f, cr_cloud *cloud,

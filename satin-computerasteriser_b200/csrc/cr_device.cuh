@@ -218,6 +218,35 @@ __device__ __forceinline__ int precision_level(float px) {
     return 0;
 }
 
+// e^-x for x >= 0 (the coverage resolve's alpha), written for this project
+// and evaluated by the oracle with the same operations: Cody-Waite range
+// reduction (Cody and Waite, Software Manual for the Elementary Functions,
+// 1980) n = floor(x log2 e), r = (x - n ln2_hi) - n ln2_lo with n ln2_hi
+// exact; e^-r by its Taylor series to degree 9 (Horner, every operation
+// rounded); an exact power-of-two scale 2^-n.
+__device__ __forceinline__ float exp_neg(float x) {
+    if (x != x) return x;
+    if (!(x > 0.0f)) return 1.0f;
+    const float t = __fmul_rn(x, 1.44269504f);
+    if (t >= 126.0f) return 0.0f;
+    const float n = floorf(t);
+    const float r = __fsub_rn(__fsub_rn(x, __fmul_rn(n, 0.693145751953125f)),
+                              __fmul_rn(n, 1.42860682e-06f));
+    const float z = __fsub_rn(0.0f, r);
+    float p = 2.75573192e-06f;
+    p = __fadd_rn(__fmul_rn(p, z), 2.48015873e-05f);
+    p = __fadd_rn(__fmul_rn(p, z), 1.98412698e-04f);
+    p = __fadd_rn(__fmul_rn(p, z), 1.38888889e-03f);
+    p = __fadd_rn(__fmul_rn(p, z), 8.33333333e-03f);
+    p = __fadd_rn(__fmul_rn(p, z), 4.16666667e-02f);
+    p = __fadd_rn(__fmul_rn(p, z), 1.66666667e-01f);
+    p = __fadd_rn(__fmul_rn(p, z), 0.5f);
+    p = __fadd_rn(__fmul_rn(p, z), 1.0f);
+    p = __fadd_rn(__fmul_rn(p, z), 1.0f);
+    const float scale = __uint_as_float((uint32_t)(127 - (int)n) << 23);
+    return __fmul_rn(p, scale);
+}
+
 // unorm8 texture write (rint(clamp(f*255, 0, 255)), round half to even).
 __device__ __forceinline__ uint32_t unorm8(float f) {
     return (uint32_t)rintf(fminf(fmaxf(f * 255.0f, 0.0f), 255.0f));

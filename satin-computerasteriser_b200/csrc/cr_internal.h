@@ -181,6 +181,10 @@ struct cr_cloud {
     float *d_frag_z = nullptr;         // NDC z
     uint32_t *d_frag_col = nullptr;    // RGBA8 (after the colorize options)
     uint32_t *d_frag_count = nullptr;  // kept points per chunk record
+    // Per-point float4 attributes of the colour variants, written by user
+    // kernels (lazy, zeroed on allocation): displacement, the previous
+    // frame's displacement (motion blur), tint.
+    float4 *d_disp = nullptr, *d_prev_disp = nullptr, *d_tint = nullptr;
     uint32_t *d_counters = nullptr;          // CounterSlot words
 
     // Pinned staging ring for the per-frame file table upload.
@@ -319,6 +323,13 @@ cr_status launch_raster_f32(cr_cloud *cloud, RasterPass pass, const RasterUnifor
 
 // Mode, point-size mode and the unsupported colour effects of a configuration.
 cr_status validate_config(const cr_config *cfg);
+// The colour variants (displacement, tint, coverage, motion blur) of an HQS
+// configuration; CR_ERR_UNSUPPORTED naming `where` when they are on.
+bool variants_on(const cr_config *cfg);
+cr_status reject_variants(const cr_config *cfg, const char *where);
+// HQS depth (color = false) or colour pass with the colour variants on.
+cr_status launch_variant_pass(cr_cloud *cloud, bool color, const RasterUniforms &u,
+                              const cr_config &cfg, const RasterTargets &t, cudaStream_t s);
 // Occupancy of the batched-view point passes (call before capturing them).
 void raster_prepare_views(cr_context *ctx);
 
@@ -377,6 +388,8 @@ cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t
                              const uint32_t *redo);
 // Zeroes the accumulators if *f->d_redo != 0.
 cr_status launch_accum_redo_clear(cr_frame *f, cudaStream_t s);
+// Coverage resolve (weighted-blended accumulation) into d_rgba[0].
+cr_status launch_resolve_coverage(cr_frame *f, const ResolveUniforms &u, cudaStream_t s);
 
 // Batched views: every view's pixels form one range, view after view
 // (ViewDesc::pix_begin); views [0, nviews) of `views` cover [pix0, pix0+npix).

@@ -251,6 +251,27 @@ __global__ void __launch_bounds__(kThreads)
         accum[p] = make_uint4(0u, 0u, 0u, 0u);
 }
 
+// resolveUpdate with coverageEnabled (Resolve/Shaders.metal:24-41): the
+// weighted-blended average sum(c a S) / sum(a S) and alpha 1 - e^-(sum a).
+__global__ void __launch_bounds__(kThreads)
+    resolve_coverage(const uint32_t *__restrict__ depth, const uint4 *__restrict__ accum,
+                     uint32_t *__restrict__ rgba, float *__restrict__ depthf, uint32_t npix,
+                     ResolveUniforms u) {
+    const uint32_t p = blockIdx.x * kThreads + threadIdx.x;
+    if (p >= npix) return;
+    const uint4 acc = accum[p];
+    if (acc.w == 0u) {
+        rgba[p] = pack_rgba(u.background[0], u.background[1], u.background[2], 0.0f);
+        depthf[p] = 0.0f;
+        return;
+    }
+    const float fa = (float)acc.w;
+    const float sum_a = fa * (1.0f / 4096.0f);
+    const float alpha = fminf(fmaxf(1.0f - crd::exp_neg(sum_a), 0.0f), 1.0f);
+    rgba[p] = pack_rgba((float)acc.x / fa, (float)acc.y / fa, (float)acc.z / fa, alpha);
+    depthf[p] = crd::uint_to_depth(depth[p]);
+}
+
 // Top bit of every depth word flipped: unsigned order <-> signed order.
 __global__ void __launch_bounds__(kThreads)
     flip_depth_order(uint4 *d4, size_t n4, uint32_t *tail, uint32_t ntail) {
@@ -392,5 +413,14 @@ cr_status launch_flip_depth_order(cr_frame *f, cudaStream_t s) {
     flip_depth_order<<<grid, kThreads, 0, s>>>(reinterpret_cast<uint4 *>(f->d_depth), n4,
                                                f->d_depth + 4 * n4, ntail);
     CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+cr_status launch_resolve_coverage(cr_frame *f, const ResolveUniforms &u, cudaStream_t s) {
+    const uint32_t npix = (uint32_t)f->width * (uint32_t)f->height;
+    resolve_coverage<<<(npix + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+        f->d_depth, f->d_accum, f->d_rgba[0], f->d_depthf, npix, u);
+    CR_CUDA(cudaGetLastError());
+    f->final_rgba = 0;
     return CR_OK;
 }

@@ -493,6 +493,7 @@ CR_API cr_status cr_render_multiview(cr_context *ctx, cr_frame *const *frames,
     if (vst) return vst;
     if (cfg->mode != CR_MODE_HIGH_QUALITY_AVERAGE)
         return fail(CR_ERR_UNSUPPORTED, "batched views render the HQS mode only");
+    if ((vst = reject_variants(cfg, "batched views"))) return vst;
     if (cfg->holeFillIterations > 64)
         return fail(CR_ERR_INVALID_ARGUMENT, "batched views: holeFillIterations must be at most 64");
     for (uint32_t v = 0; v < nviews; ++v) {

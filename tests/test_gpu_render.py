@@ -225,20 +225,24 @@ def test_empty_and_nonresident_clouds(cr, orc, ctx):
     assert np.all(gpu["rgba"][..., 0] == 255) and np.all(gpu["rgba"][..., 3] == 0)
 
 
-def test_unsupported_effects_are_rejected(cr, orc, ctx):
+def test_colour_variant_flags_render_on_an_empty_cloud(cr, orc, ctx):
+    """The colour variants (parity in test_gpu_variants.py) render through
+    cr_render, clouds without attribute buffers reading zeros; a motion blur
+    with no sample allowed is an argument error."""
     cloud = cr.ComputeRasteriserPointCloud(ctx, cr.ComputeRasteriserCapacity(1, 16))
     ras = cr.ComputeRasteriser(ctx)
     ras.addPointCloud(cloud)
     ras.resize((8, 8))
     ras.update(camera(cr, (0, 0, 3), w=8, h=8))
-    for field in ("applyTint", "applyDisplacement", "tintAlphaIsCoverage"):
-        ras.configuration = cr.ComputeRasteriserConfiguration(**{field: True})
-        with pytest.raises(cr.CRError) as e:
-            ras.encode()
-        assert e.value.status == 4
-    ras.configuration = cr.ComputeRasteriserConfiguration(motionBlur=0.5)
-    with pytest.raises(cr.CRError):
+    for kw in ({"applyTint": True}, {"applyDisplacement": True},
+               {"applyTint": True, "tintAlphaIsCoverage": True}, {"motionBlur": 0.5}):
+        ras.configuration = cr.ComputeRasteriserConfiguration(**kw)
         ras.encode()
+        assert not ras.pixels()["count"].any()
+    ras.configuration = cr.ComputeRasteriserConfiguration(motionBlur=0.5, motionBlurSamples=0)
+    with pytest.raises(cr.CRError) as e:
+        ras.encode()
+    assert e.value.status == 1
 
 
 def test_capacity_errors(cr, orc, ctx):

@@ -210,3 +210,15 @@ def test_multithreaded_render_matches_single(orc):
         assert np.array_equal(a.rgba, b.rgba)
         assert np.array_equal(a.accum, b.accum)
         assert np.array_equal(a.nearest_index, b.nearest_index)
+
+
+def test_project_exp_neg_accuracy(orc):
+    """The coverage resolve's e^-x (written for this project, shared by the
+    kernels and the oracle) against float64 exp: within 2 float ulps."""
+    xs = np.concatenate([np.linspace(0, 1, 2001), np.linspace(1, 20, 4001),
+                         np.array([1e-6, 1e-3, 0.5, 10.0, 40.0, 80.0, 87.0])]).astype(np.float32)
+    got = np.array([orc.exp_neg(float(x)) for x in xs], np.float32)
+    want = np.exp(-xs.astype(np.float64))
+    ulp = np.spacing(want.astype(np.float32)).astype(np.float64)
+    assert (np.abs(got - want) <= 2 * ulp + 1e-45).all()
+    assert orc.exp_neg(0.0) == 1.0 and orc.exp_neg(200.0) == 0.0
