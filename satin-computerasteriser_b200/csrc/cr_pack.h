@@ -20,8 +20,7 @@ struct PackScratch {
     uint64_t cap_grid = 0;
     uint64_t cap_hist = 0;
     void *raw = nullptr;                    // staged host input
-    float4 *pos = nullptr;                  // input positions (x, y, z, 0)
-    uint32_t *col = nullptr;                // input colours, packed RGBA8
+    float4 *pos = nullptr;                  // input x, y, z and RGBA8 bits in w
     void *keys[2] = {nullptr, nullptr};     // Morton keys (u32 or u64), ping-pong
     uint32_t *idx[2] = {nullptr, nullptr};  // sort payload, ping-pong
     float4 *sorted = nullptr;               // positions in Morton order

@@ -83,22 +83,26 @@ struct LoadArgs {
 
 // Stage 0: raw input -> float4 positions + packed RGBA8 (GPUPacker/Shaders.metal:219-235
 // colour rule: uint(clamp(c, 0, 1) * 255), truncating).
+// One 16-byte record per point: x, y, z and the packed RGBA8 colour's bits
+// in w (moved, never computed on), so the Morton-order gather brings both
+// with one access.
 __global__ void __launch_bounds__(kThreads)
-    pack_load(LoadArgs a, uint64_t n, float4 *__restrict__ pos, uint32_t *__restrict__ col) {
+    pack_load(LoadArgs a, uint64_t n, float4 *__restrict__ pos) {
     const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
     const float *p = reinterpret_cast<const float *>(a.pos + i * a.pos_stride);
-    pos[i] = make_float4(p[0], p[1], p[2], 0.0f);
+    uint32_t col;
     if (a.col_format == 1) {
-        col[i] = *reinterpret_cast<const uint32_t *>(a.col + i * a.col_stride);
+        col = *reinterpret_cast<const uint32_t *>(a.col + i * a.col_stride);
     } else {
         const float *c = reinterpret_cast<const float *>(a.col + i * a.col_stride);
         const uint32_t r = (uint32_t)(fminf(fmaxf(c[0], 0.0f), 1.0f) * 255.0f);
         const uint32_t g = (uint32_t)(fminf(fmaxf(c[1], 0.0f), 1.0f) * 255.0f);
         const uint32_t b = (uint32_t)(fminf(fmaxf(c[2], 0.0f), 1.0f) * 255.0f);
         const uint32_t al = (uint32_t)(fminf(fmaxf(c[3], 0.0f), 1.0f) * 255.0f);
-        col[i] = r | (g << 8) | (b << 16) | (al << 24);
+        col = r | (g << 8) | (b << 16) | (al << 24);
     }
+    pos[i] = make_float4(p[0], p[1], p[2], __uint_as_float(col));
 }
 
 // Stage 1: global bounds (packBounds, GPUPacker/Shaders.metal:71-105).
@@ -179,12 +183,20 @@ __device__ __forceinline__ uint64_t lod_cell(const float4 &p, const LodArgs &a) 
 }
 
 // Stage 5 (packLODClaim / packLODAssign, GPUPacker/Shaders.metal:337-371).
+// The points are in Morton order, so neighbouring lanes often share a cell;
+// lanes carry increasing indices, so the lowest lane of each group of lanes
+// with the same cell holds the group's minimum and alone does the atomicMin
+// (the grid ends the same: min is order-independent).
 __global__ void __launch_bounds__(kThreads)
     pack_lod_claim(const float4 *__restrict__ sorted, const uint8_t *__restrict__ lv, uint64_t n,
                    LodArgs a, uint32_t *__restrict__ grid) {
     const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
-    if (i >= n || lv[i] != a.max_level) return;
-    atomicMin(&grid[lod_cell(sorted[i], a)], (uint32_t)i);
+    const bool part = i < n && lv[i] == a.max_level;
+    const unsigned act = __ballot_sync(0xffffffffu, part);
+    if (!part) return;
+    const uint64_t cell = lod_cell(sorted[i], a);
+    const unsigned same = __match_any_sync(act, (unsigned long long)cell);
+    if ((int)(__ffs(same) - 1) == (int)(threadIdx.x & 31u)) atomicMin(&grid[cell], (uint32_t)i);
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -299,19 +311,19 @@ __global__ void __launch_bounds__(kThreads)
 // Stage 7: final order, quantisation (packQuantize, GPUPacker/Shaders.metal:288-309).
 __global__ void __launch_bounds__(kThreads)
     pack_emit(uint64_t n, uint32_t ppb, const uint32_t *__restrict__ perm,
-              const uint32_t *__restrict__ idx_sorted, const float4 *__restrict__ pos,
-              const uint32_t *__restrict__ col, const uint8_t *__restrict__ lv_out,
+              const uint32_t *__restrict__ idx_sorted, const float4 *__restrict__ sorted,
+              const uint8_t *__restrict__ lv_out,
               const cr_raster_batch *__restrict__ batches, uint32_t *__restrict__ low,
               uint32_t *__restrict__ med, uint32_t *__restrict__ high,
               uint32_t *__restrict__ colors, uint8_t *__restrict__ levels,
               uint32_t *__restrict__ src_out) {
     const uint64_t j = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
     if (j >= n) return;
+    // perm only reorders points within their batch (level bucketing), so
+    // the Morton-ordered arrays are read nearly in order.
     const uint32_t pj = perm[j];
     if (pj >= n) return;  // unreachable for a complete permutation
-    const uint32_t orig = idx_sorted[pj];
-    if (orig >= n) return;
-    const float4 p = pos[orig];
+    const float4 p = sorted[pj];
     const cr_raster_batch &b = batches[j / ppb];
     const float sx = fmaxf(b.maxX - b.minX, 0.000001f);
     const float sy = fmaxf(b.maxY - b.minY, 0.000001f);
@@ -326,9 +338,9 @@ __global__ void __launch_bounds__(kThreads)
     low[j] = ((qx >> 20) & 1023u) | (((qy >> 20) & 1023u) << 10) | (((qz >> 20) & 1023u) << 20);
     med[j] = ((qx >> 10) & 1023u) | (((qy >> 10) & 1023u) << 10) | (((qz >> 10) & 1023u) << 20);
     high[j] = (qx & 1023u) | ((qy & 1023u) << 10) | ((qz & 1023u) << 20);
-    colors[j] = col[orig];
+    colors[j] = __float_as_uint(p.w);
     levels[j] = lv_out[j];
-    if (src_out) src_out[j] = orig;
+    if (src_out) src_out[j] = idx_sorted[pj];
 }
 
 unsigned grid_for(uint64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
@@ -363,7 +375,6 @@ cr_status ensure_points(PackScratch &s, uint64_t n) {
         }                                                                   \
     } while (0)
     ALLOC(s.pos, m * sizeof(float4));
-    ALLOC(s.col, m * 4);
     ALLOC(s.keys[0], m * 8);
     ALLOC(s.keys[1], m * 8);
     ALLOC(s.idx[0], m * 4);
@@ -383,7 +394,7 @@ cr_status ensure_points(PackScratch &s, uint64_t n) {
 }  // namespace
 
 void pack_scratch_free(PackScratch &s) {
-    void *ptrs[] = {s.raw, s.pos, s.col, s.keys[0], s.keys[1], s.idx[0], s.idx[1], s.sorted,
+    void *ptrs[] = {s.raw, s.pos, s.keys[0], s.keys[1], s.idx[0], s.idx[1], s.sorted,
                     s.lv_morton, s.lv_out, s.perm, s.grid, s.hist, s.digit_total, s.bounds,
                     s.src_idx};
     for (void *p : ptrs)
@@ -437,7 +448,7 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
             la.col = raw + coff;
         }
     }
-    pack_load<<<grid_for(count), kThreads, 0, s>>>(la, count, sc.pos, sc.col);
+    pack_load<<<grid_for(count), kThreads, 0, s>>>(la, count, sc.pos);
     CR_CUDA(cudaGetLastError());
 
     // Stage 1: bounds, read back once.
@@ -530,7 +541,8 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
     CR_CUDA(cudaGetLastError());
     const uint64_t p0 = (uint64_t)first_slot * ppb;
     pack_emit<<<grid_for(count), kThreads, 0, s>>>(
-        count, ppb, sc.perm, idx_sorted, sc.pos, sc.col, sc.lv_out, dst_batches, cloud->d_low + p0,
+        count, ppb, sc.perm, idx_sorted, sc.sorted, sc.lv_out, dst_batches,
+        cloud->d_low + p0,
         cloud->d_med + p0, cloud->d_high + p0, cloud->d_colors + p0, cloud->d_levels + p0,
         sc.src_idx);
     CR_CUDA(cudaGetLastError());

@@ -8,10 +8,12 @@
 //            shared memory), written digit-major;
 //   scan     one CTA per digit turns its row into exclusive partition
 //            offsets and the digit total;
-//   scatter  each partition re-reads its keys in rounds of 256; lanes rank
-//            themselves among equal digits with __match_any_sync, warps are
-//            ordered through shared memory, so equal keys keep their input
-//            order (stable), as the CPU's stable sort does.
+//   scatter  each partition re-reads its keys in tiles of 4096, ranks them
+//            among equal digits in input order (warp multisplit with
+//            __match_any_sync, then scans over warps and digits), sorts the
+//            tile by digit in shared memory and writes one coalesced run per
+//            digit, so equal keys keep their input order (stable), as the
+//            CPU's stable sort does.
 // 32-bit keys (30-bit Morton) take 4 passes, 64-bit keys (63-bit Morton) 8.
 #include <algorithm>
 
@@ -23,7 +25,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kPartition = 16384;
-constexpr int kRounds = kPartition / kThreads;
 
 template <typename K>
 __global__ void __launch_bounds__(kThreads)
@@ -87,68 +88,127 @@ __global__ void __launch_bounds__(1024)
     if (threadIdx.x == 0) digit_total[blockIdx.x] = carry;
 }
 
+// Scatter of one pass, a partition per CTA in tiles of kTileKeys keys:
+//   1. each warp takes 512 consecutive keys, 16 per lane in warp-striped
+//      order (key j*32 + lane), and ranks them among equal digits with
+//      __match_any_sync against running per-warp digit counts, in input
+//      order (j, then lane);
+//   2. per digit, exclusive scans over the warps and then over the digits
+//      give each key its slot in a tile sorted by digit, stable;
+//   3. the keys and values move to that slot in shared memory;
+//   4. threads read the sorted tile in order and write each key to its
+//      digit's running global offset: keys of one digit are consecutive in
+//      shared memory and land at consecutive addresses (coalesced runs).
+constexpr int kKeysPerLane = 16;
+constexpr int kTileKeys = kThreads * kKeysPerLane;
+static_assert(kPartition % kTileKeys == 0, "a partition is whole tiles");
+
+template <typename K>
+size_t scatter_smem_bytes() {
+    return (size_t)kTileKeys * (sizeof(K) + sizeof(uint32_t)) +
+           ((size_t)kWarps * 256 + 256 + 256) * sizeof(uint32_t);
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kThreads)
     radix_scatter(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                   K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, uint64_t n, int shift,
                   const uint32_t *__restrict__ hist, uint32_t nparts,
                   const uint32_t *__restrict__ digit_total) {
-    __shared__ uint32_t offset[256];       // running global offset per digit
-    __shared__ uint32_t wcount[kWarps][256];
-    __shared__ uint32_t scan_tmp[256];
+    extern __shared__ __align__(16) unsigned char smem[];
+    K *skey = reinterpret_cast<K *>(smem);
+    uint32_t *sval = reinterpret_cast<uint32_t *>(skey + kTileKeys);
+    uint32_t *wcnt = sval + kTileKeys;        // [kWarps][256]
+    uint32_t *offset = wcnt + kWarps * 256;   // running global offset per digit
+    uint32_t *tbase = offset + 256;           // tile-local digit base
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // Digit bases: exclusive scan of the 256 digit totals.
+    const uint32_t lt = (1u << lane) - 1u;
+    // Digit bases: exclusive scan of the 256 digit totals, plus this
+    // partition's offset within each digit.
     {
         const uint32_t t = digit_total[threadIdx.x];
-        scan_tmp[threadIdx.x] = t;
+        tbase[threadIdx.x] = t;
         __syncthreads();
         for (int o = 1; o < 256; o <<= 1) {
-            const uint32_t y = threadIdx.x >= (unsigned)o ? scan_tmp[threadIdx.x - o] : 0u;
+            const uint32_t y = threadIdx.x >= (unsigned)o ? tbase[threadIdx.x - o] : 0u;
             __syncthreads();
-            scan_tmp[threadIdx.x] += y;
+            tbase[threadIdx.x] += y;
             __syncthreads();
         }
         offset[threadIdx.x] =
-            scan_tmp[threadIdx.x] - t + hist[(size_t)threadIdx.x * nparts + blockIdx.x];
+            tbase[threadIdx.x] - t + hist[(size_t)threadIdx.x * nparts + blockIdx.x];
     }
-    for (int i = threadIdx.x; i < kWarps * 256; i += kThreads) (&wcount[0][0])[i] = 0;
-    __syncthreads();
-    const uint64_t base = (uint64_t)blockIdx.x * kPartition;
-    const uint32_t lt = (1u << lane) - 1u;
-    for (int r = 0; r < kRounds; ++r) {
-        const uint64_t i = base + (uint64_t)r * kThreads + threadIdx.x;
-        if (base + (uint64_t)r * kThreads >= n) break;  // uniform across the CTA
-        const bool v = i < n;
-        K k = 0;
-        uint32_t val = 0;
-        if (v) {
-            k = keys_in[i];
-            val = vals_in[i];
-        }
-        const uint32_t d = v ? ((uint32_t)(k >> shift) & 0xffu) : 256u;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        const uint32_t rank = __popc(peers & lt);
-        if (v && rank == 0) wcount[warp][d] = __popc(peers);
+    const uint64_t pbase = (uint64_t)blockIdx.x * kPartition;
+    for (uint32_t t0 = 0; t0 < kPartition; t0 += kTileKeys) {
+        const uint64_t tile0 = pbase + t0;
+        if (tile0 >= n) break;  // uniform across the CTA
+        const uint32_t tile_n = (n - tile0 < (uint64_t)kTileKeys) ? (uint32_t)(n - tile0)
+                                                                  : (uint32_t)kTileKeys;
+        for (int i = threadIdx.x; i < kWarps * 256; i += kThreads) wcnt[i] = 0u;
         __syncthreads();
-        uint32_t before = 0;
-        if (v) {
-            for (int w = 0; w < warp; ++w) before += wcount[w][d];
-            const uint64_t dst = (uint64_t)offset[d] + before + rank;
+        // 1. Warp-level ranking in input order; a key's rank within its
+        //    warp (< 512) and digit are kept packed, the key and value are
+        //    read again (from L1 / L2) when they move.
+        uint32_t rd[kKeysPerLane];
+        uint32_t *wc = wcnt + warp * 256;
+#pragma unroll
+        for (int j = 0; j < kKeysPerLane; ++j) {
+            const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
+            const bool v = li < tile_n;
+            const K key = v ? keys_in[tile0 + li] : K(0);
+            const uint32_t d = v ? ((uint32_t)(key >> shift) & 0xffu) : 256u;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            const uint32_t before = v ? wc[d] : 0u;
+            rd[j] = (before + __popc(peers & lt)) | (d << 16);
+            __syncwarp();
+            if (v && (peers & lt) == 0u) wc[d] = before + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        // 2. Per digit: warp bases (exclusive over warps) and tile bases
+        //    (exclusive over digits).
+        const uint32_t dd = threadIdx.x;
+        uint32_t total = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = wcnt[w * 256 + dd];
+            wcnt[w * 256 + dd] = total;
+            total += c;
+        }
+        tbase[dd] = total;
+        __syncthreads();
+        for (int o = 1; o < 256; o <<= 1) {
+            const uint32_t y = dd >= (unsigned)o ? tbase[dd - o] : 0u;
+            __syncthreads();
+            tbase[dd] += y;
+            __syncthreads();
+        }
+        tbase[dd] -= total;  // inclusive -> exclusive
+        __syncthreads();
+        // 3. Keys and values to their sorted slots in the tile.
+#pragma unroll
+        for (int j = 0; j < kKeysPerLane; ++j) {
+            const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
+            if (li < tile_n) {
+                const uint32_t d = rd[j] >> 16;
+                const uint32_t slot = tbase[d] + wcnt[warp * 256 + d] + (rd[j] & 0xffffu);
+                skey[slot] = keys_in[tile0 + li];
+                sval[slot] = vals_in[tile0 + li];
+            }
+        }
+        __syncthreads();
+        // 4. Coalesced runs per digit to the global output.
+        for (uint32_t i = threadIdx.x; i < tile_n; i += kThreads) {
+            const K k = skey[i];
+            const uint32_t d = (uint32_t)(k >> shift) & 0xffu;
+            const uint64_t dst = (uint64_t)offset[d] + (i - tbase[d]);
             if (dst < n) {  // always true when the histograms are consistent
                 keys_out[dst] = k;
-                vals_out[dst] = val;
+                vals_out[dst] = sval[i];
             }
         }
         __syncthreads();
-        {
-            uint32_t s = 0;
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) {
-                s += wcount[w][threadIdx.x];
-                wcount[w][threadIdx.x] = 0;
-            }
-            offset[threadIdx.x] += s;
-        }
+        offset[dd] += total;
         __syncthreads();
     }
 }
@@ -169,8 +229,11 @@ cr_status radix_sort_pairs(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_
         CR_CUDA(cudaGetLastError());
         radix_scan<<<256, 1024, 0, s>>>(hist, nparts, digit_total);
         CR_CUDA(cudaGetLastError());
-        radix_scatter<K><<<nparts, kThreads, 0, s>>>(kin, vin, kout, vout, n, shift, hist, nparts,
-                                                     digit_total);
+        const size_t smem = scatter_smem_bytes<K>();
+        CR_CUDA(cudaFuncSetAttribute(radix_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        radix_scatter<K><<<nparts, kThreads, smem, s>>>(kin, vin, kout, vout, n, shift, hist, nparts,
+                                                        digit_total);
         CR_CUDA(cudaGetLastError());
         std::swap(kin, kout);
         std::swap(vin, vout);
