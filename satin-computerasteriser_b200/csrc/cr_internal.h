@@ -30,7 +30,7 @@ cr_status cuda_fail(cudaError_t e, const char *what);
 // ---------------------------------------------------------------------------
 enum CounterSlot : int {
     CNT_VISIBLE = 0,     // survivors of the last cull (VisibleBatch count)
-    CNT_WORK_DEPTH = 1,  // dynamic work cursor of the depth / nearest pass
+    CNT_WORK_DEPTH = 1,  // dynamic work cursor of the one-view point passes
     CNT_WORK_COLOR = 2,  // dynamic work cursor of the colour pass
     CNT_CHUNKS = 3,      // chunk work records written by the last cull
     CNT_ARGS_X = 4,      // CRDispatchArgs mirror: {count, 1, 1}
@@ -38,6 +38,7 @@ enum CounterSlot : int {
     CNT_ARGS_Z = 6,
     CNT_ERROR = 7,       // first device-side error code (0 = none)
     CNT_POINTS = 8,      // fragment span of the last cull's survivors (chunks rounded to 4)
+    CNT_DONE = 9,        // CTAs finished with the dynamic cursor (the last one resets both)
     CNT_COUNT = 32
 };
 
@@ -85,7 +86,7 @@ struct cr_context {
     int sm_count = 0;
     int blocks_per_sm[7] = {};        // occupancy of the persistent point passes (per RasterPass)
     int blocks_per_sm_views[7] = {};  // the same, batched-view kernels
-    int chunk_points = 2048;           // points per chunk work record
+    int chunk_points = 4096;           // points per chunk work record
     int view_group_pixels = 4194304;   // batched views: pixels per depth/colour group
     bool use_tiles = true;             // shared-memory screen tiles
     // Profiling: a ring of frames, each with a start/stop event per pass.

@@ -261,6 +261,7 @@ __device__ __forceinline__ void compact_body(const CullArgs &a) {
         counters[CNT_ARGS_Z] = 1u;
         counters[CNT_WORK_DEPTH] = 0u;
         counters[CNT_WORK_COLOR] = 0u;
+        counters[CNT_DONE] = 0u;
         counters[CNT_CHUNKS] = off_c + mine_chunks;
         counters[CNT_POINTS] = off_p + mine_points;
     }
@@ -285,6 +286,7 @@ __global__ void cull_empty(uint32_t *counters) {
     counters[CNT_ARGS_Z] = 1u;
     counters[CNT_WORK_DEPTH] = 0u;
     counters[CNT_WORK_COLOR] = 0u;
+    counters[CNT_DONE] = 0u;
     counters[CNT_CHUNKS] = 0u;
     counters[CNT_POINTS] = 0u;
 }

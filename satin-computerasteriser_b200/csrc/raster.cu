@@ -652,9 +652,11 @@ __device__ __forceinline__ uint32_t find_view(const uint32_t *begin, uint32_t nv
     return lo;
 }
 
-// Persistent pass over the chunk records (static grid-stride schedule): the
-// record of the CTA's next chunk is copied into shared memory with cp.async
-// while the current chunk is processed.  Batched views (MV): the chunks of
+// Persistent pass over the chunk records: the record of the CTA's next chunk
+// is copied into shared memory with cp.async while the current chunk is
+// processed.  One view: the CTAs claim chunks from the cloud's work cursor
+// (dynamic schedule; a chunk's work varies with its batch's LOD prefix), and
+// the last CTA to finish resets the cursor for the next launch.  Batched views (MV): the chunks of
 // all views form one index space, view after view; each CTA scans the
 // per-view chunk counts once, finds a chunk's view by binary search and
 // switches frame, camera and file table when the view changes.
@@ -711,8 +713,27 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
     } else {
         nchunks = a.counters[CNT_CHUNKS];
     }
+    constexpr bool kDyn = !MV;
+    __shared__ uint32_t s_k[2];  // claimed chunk of each record buffer
+    auto finish = [&]() {
+        if (kDyn && threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(a.counters + CNT_DONE, 1u) == gridDim.x - 1u) {
+                a.counters[CNT_WORK_DEPTH] = 0u;
+                a.counters[CNT_DONE] = 0u;
+            }
+        }
+    };
     uint32_t k = blockIdx.x;
-    if (k >= nchunks) return;
+    if (kDyn) {
+        if (threadIdx.x == 0) s_k[0] = atomicAdd(a.counters + CNT_WORK_DEPTH, 1u);
+        __syncthreads();
+        k = s_k[0];
+    }
+    if (k >= nchunks) {
+        finish();
+        return;
+    }
     // View of chunk kk and the index of its record (also its fragment-count slot).
     auto locate = [&](uint32_t kk, uint32_t &view) -> uint32_t {
         if (!MV) {
@@ -739,9 +760,14 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
         s_frag_count = 0u;
     }
     int buf = 0;
-    for (; k < nchunks; k += gridDim.x, buf ^= 1, cur_view = next_view, cur_slot = next_slot) {
+    for (;; buf ^= 1, cur_view = next_view, cur_slot = next_slot) {
         cp_async_wait_all();
         __syncthreads();  // rec[buf] complete; the previous chunk is fully done
+        if (kDyn) {
+            k = s_k[buf];
+            cur_slot = k;
+        }
+        if (k >= nchunks) break;
         const ChunkRec c = rec[buf];
         const uint32_t nfrag = PASS == PASS_COLOR_FRAG ? rec_frags[buf][0] : 0u;
         const uint32_t fslot = cur_slot;
@@ -749,10 +775,25 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
         // view's fragment span in the arena (batched views).
         const uint32_t fbase =
             MV ? (kFrag ? (uint32_t)(s_pbegin[cur_view] + rec_frags[buf][1]) : 0u) : c.first;
-        const uint32_t kn = k + gridDim.x;
-        if (kn < nchunks) {
-            next_slot = locate(kn, next_view);
-            fetch(next_slot, buf ^ 1);
+        if (kDyn) {
+            if (threadIdx.x == 0) {
+                const uint32_t kn = atomicAdd(a.counters + CNT_WORK_DEPTH, 1u);
+                s_k[buf ^ 1] = kn;
+                if (kn < nchunks) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        cp_async16(reinterpret_cast<uint4 *>(&rec[buf ^ 1]) + q,
+                                   reinterpret_cast<const uint4 *>(a.chunks + kn) + q);
+                    if (PASS == PASS_COLOR_FRAG) cp_async4(&rec_frags[buf ^ 1][0], a.frag_count + kn);
+                }
+            }
+        } else {
+            const uint32_t kn = k + gridDim.x;
+            k = kn;
+            if (kn < nchunks) {
+                next_slot = locate(kn, next_view);
+                fetch(next_slot, buf ^ 1);
+            }
         }
         cp_async_commit();
         const uint32_t file_id = MV ? cur_view * a.nfiles + c.file : c.file;
@@ -877,6 +918,7 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
         }
     }
     cp_async_wait_all();
+    finish();
 }
 
 
