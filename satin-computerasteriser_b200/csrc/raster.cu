@@ -713,10 +713,15 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
     } else {
         nchunks = a.counters[CNT_CHUNKS];
     }
-    constexpr bool kDyn = !MV;
-    __shared__ uint32_t s_k[2];  // claimed chunk of each record buffer
+    // Chunks are claimed from a work cursor in the launch's counters (the
+    // cull zeroes it; the last CTA to finish resets it for the next launch):
+    // a dynamic schedule, since a chunk's work varies with its batch's LOD
+    // prefix and its view.  Thread 0 claims the next chunk, finds its view
+    // and record and prefetches the record while the CTA draws the current
+    // one.
+    __shared__ uint32_t s_k[2], s_kview[2], s_kslot[2];  // per record buffer
     auto finish = [&]() {
-        if (kDyn && threadIdx.x == 0) {
+        if (threadIdx.x == 0) {
             __threadfence();
             if (atomicAdd(a.counters + CNT_DONE, 1u) == gridDim.x - 1u) {
                 a.counters[CNT_WORK_DEPTH] = 0u;
@@ -724,16 +729,6 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
             }
         }
     };
-    uint32_t k = blockIdx.x;
-    if (kDyn) {
-        if (threadIdx.x == 0) s_k[0] = atomicAdd(a.counters + CNT_WORK_DEPTH, 1u);
-        __syncthreads();
-        k = s_k[0];
-    }
-    if (k >= nchunks) {
-        finish();
-        return;
-    }
     // View of chunk kk and the index of its record (also its fragment-count slot).
     auto locate = [&](uint32_t kk, uint32_t &view) -> uint32_t {
         if (!MV) {
@@ -743,31 +738,34 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
         view = find_view(s_vbegin, a.nviews, kk);
         return view * a.chunk_stride + (kk - s_vbegin[view]);
     };
-    auto fetch = [&](uint32_t slot, int b) {
-        if (threadIdx.x < 4)
-            cp_async16(reinterpret_cast<uint4 *>(&rec[b]) + threadIdx.x,
-                       reinterpret_cast<const uint4 *>(a.chunks + slot) + threadIdx.x);
-        if (PASS == PASS_COLOR_FRAG && threadIdx.x == 4)
-            cp_async4(&rec_frags[b][0], a.frag_count + slot);
-        if (MV && kFrag && threadIdx.x == 5) cp_async4(&rec_frags[b][1], a.chunk_poff + slot);
+    // Thread 0: claim a chunk into record buffer b and start its copy.
+    auto claim = [&](int b) {
+        const uint32_t kk = atomicAdd(a.counters + CNT_WORK_DEPTH, 1u);
+        s_k[b] = kk;
+        if (kk >= nchunks) return;
+        uint32_t view;
+        const uint32_t slot = locate(kk, view);
+        s_kview[b] = view;
+        s_kslot[b] = slot;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            cp_async16(reinterpret_cast<uint4 *>(&rec[b]) + q,
+                       reinterpret_cast<const uint4 *>(a.chunks + slot) + q);
+        if (PASS == PASS_COLOR_FRAG) cp_async4(&rec_frags[b][0], a.frag_count + slot);
+        if (MV && kFrag) cp_async4(&rec_frags[b][1], a.chunk_poff + slot);
     };
-    uint32_t cur_view, next_view = 0u, loaded_view = 0xffffffffu;
-    uint32_t cur_slot = locate(k, cur_view), next_slot = 0u;
-    fetch(cur_slot, 0);
-    cp_async_commit();
     if (threadIdx.x == 0) {
+        claim(0);
         sb.file = 0xffffffffu;
         s_frag_count = 0u;
     }
-    int buf = 0;
-    for (;; buf ^= 1, cur_view = next_view, cur_slot = next_slot) {
+    cp_async_commit();
+    uint32_t loaded_view = 0xffffffffu;
+    for (int buf = 0;; buf ^= 1) {
         cp_async_wait_all();
         __syncthreads();  // rec[buf] complete; the previous chunk is fully done
-        if (kDyn) {
-            k = s_k[buf];
-            cur_slot = k;
-        }
-        if (k >= nchunks) break;
+        if (s_k[buf] >= nchunks) break;
+        const uint32_t cur_view = s_kview[buf], cur_slot = s_kslot[buf];
         const ChunkRec c = rec[buf];
         const uint32_t nfrag = PASS == PASS_COLOR_FRAG ? rec_frags[buf][0] : 0u;
         const uint32_t fslot = cur_slot;
@@ -775,26 +773,7 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
         // view's fragment span in the arena (batched views).
         const uint32_t fbase =
             MV ? (kFrag ? (uint32_t)(s_pbegin[cur_view] + rec_frags[buf][1]) : 0u) : c.first;
-        if (kDyn) {
-            if (threadIdx.x == 0) {
-                const uint32_t kn = atomicAdd(a.counters + CNT_WORK_DEPTH, 1u);
-                s_k[buf ^ 1] = kn;
-                if (kn < nchunks) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        cp_async16(reinterpret_cast<uint4 *>(&rec[buf ^ 1]) + q,
-                                   reinterpret_cast<const uint4 *>(a.chunks + kn) + q);
-                    if (PASS == PASS_COLOR_FRAG) cp_async4(&rec_frags[buf ^ 1][0], a.frag_count + kn);
-                }
-            }
-        } else {
-            const uint32_t kn = k + gridDim.x;
-            k = kn;
-            if (kn < nchunks) {
-                next_slot = locate(kn, next_view);
-                fetch(next_slot, buf ^ 1);
-            }
-        }
+        if (threadIdx.x == 0) claim(buf ^ 1);
         cp_async_commit();
         const uint32_t file_id = MV ? cur_view * a.nfiles + c.file : c.file;
         const bool new_file = file_id != sb.file;
