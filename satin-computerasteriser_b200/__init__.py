@@ -60,15 +60,13 @@ def _mat16(m) -> np.ndarray:
 def matrix_multiply(a, b) -> np.ndarray:
     """a * b for column-major float[16] matrices with the library's fixed
     operation order (rows summed k = 0..3 left to right, no FMA)."""
-    a, b = _mat16(a), _mat16(b)
-    out = np.zeros(16, np.float32)
-    for c in range(4):
-        for r in range(4):
-            s = np.float32(a[r] * b[c * 4 + 0]) + np.float32(a[4 + r] * b[c * 4 + 1])
-            s = np.float32(s) + np.float32(a[8 + r] * b[c * 4 + 2])
-            s = np.float32(s) + np.float32(a[12 + r] * b[c * 4 + 3])
-            out[c * 4 + r] = s
-    return out
+    A, B = _mat16(a).reshape(4, 4), _mat16(b).reshape(4, 4)  # A[k][r] = a[4k + r]
+    # Element (c, r): ((a[r] b[4c] + a[4+r] b[4c+1]) + a[8+r] b[4c+2]) + a[12+r] b[4c+3],
+    # every product and sum rounded to float32, for all 16 elements at once.
+    s = np.multiply.outer(B[:, 0], A[0]) + np.multiply.outer(B[:, 1], A[1])
+    s = s + np.multiply.outer(B[:, 2], A[2])
+    s = s + np.multiply.outer(B[:, 3], A[3])
+    return np.ascontiguousarray(s, dtype=np.float32).reshape(16)
 
 
 def identity_files(n: int = 1) -> np.ndarray:
@@ -811,8 +809,27 @@ class PerspectiveCamera:
         self.target = np.asarray(target, np.float64)
         self.up = np.asarray(up, np.float64)
 
+    # The matrices are recomputed only when the pose or the lens changes (a
+    # render loop reads them several times per frame).
     @property
     def viewMatrix(self) -> np.ndarray:
+        key = (np.asarray(self.position, np.float64).tobytes(),
+               np.asarray(self.target, np.float64).tobytes(),
+               np.asarray(self.up, np.float64).tobytes())
+        if getattr(self, "_view_key", None) != key:
+            self._view = self._compute_view()
+            self._view_key = key
+        return self._view.copy()
+
+    @property
+    def projectionMatrix(self) -> np.ndarray:
+        key = (self.near, self.far, self.fov, self.aspect)
+        if getattr(self, "_proj_key", None) != key:
+            self._proj = self._compute_projection()
+            self._proj_key = key
+        return self._proj.copy()
+
+    def _compute_view(self) -> np.ndarray:
         f = self.target - self.position
         f = f / np.linalg.norm(f)
         s = np.cross(f, self.up)
@@ -823,8 +840,7 @@ class PerspectiveCamera:
         m[0, 3], m[1, 3], m[2, 3] = -s @ self.position, -u @ self.position, f @ self.position
         return _mat16(m)
 
-    @property
-    def projectionMatrix(self) -> np.ndarray:
+    def _compute_projection(self) -> np.ndarray:
         t = 1.0 / math.tan(math.radians(self.fov) * 0.5)
         n, fa = self.near, self.far
         m = np.zeros((4, 4))
@@ -838,8 +854,8 @@ class PerspectiveCamera:
 
 def _camera_c(camera) -> N.cr_camera:
     c = N.cr_camera()
-    c.view[:] = _mat16(camera.viewMatrix).tolist()
-    c.projection[:] = _mat16(camera.projectionMatrix).tolist()
+    C.memmove(c.view, _mat16(camera.viewMatrix).ctypes.data, 64)
+    C.memmove(c.projection, _mat16(camera.projectionMatrix).ctypes.data, 64)
     return c
 
 
