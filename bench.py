@@ -450,7 +450,7 @@ def run_ours(args, dist):
     peak, peak_kind = measured_peaks()
     # Single-pixel footprints: the depth pass emits fragments (PASS_DEPTH_FRAG
     # = 3) and the colour pass reads them (color_hash_kernel).
-    kernel = {"depth": "raster_kernel<3>", "color": "color_hash_kernel"}.get(PASS_NAMES[dom],
+    kernel = {"depth": "depth_kernel<3>", "color": "color_hash_kernel"}.get(PASS_NAMES[dom],
                                                                            PASS_NAMES[dom])
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,

@@ -17,13 +17,14 @@
 // point prefix into chunk records of at most `chunkPoints` points carrying
 // the per-batch decode values and screen rectangle, and publishes their
 // count (the CUDA counterpart of the indirect argument buffer).  A
-// persistent grid sized to fill every SM walks the records with a static
-// grid-stride schedule, copying the next record into shared memory
-// (cp.async) while the current chunk is processed, so batches of very
-// different sizes spread evenly over the SMs.  Each CTA of 256 threads walks
-// a chunk four points per thread with 16-byte loads of the level bytes and
-// position / colour words; warps skip the projection and the atomics when
-// none of their lanes survives the dither or clip tests.
+// persistent grid sized to fill every SM claims the records from a work
+// cursor, copying the next record into shared memory (cp.async) while the
+// current chunk is processed, so batches of very different sizes spread
+// evenly over the SMs.  Each CTA of 256 threads walks a chunk four points
+// per thread with 16-byte loads of the level bytes and position / colour
+// words; warps skip the projection and the atomics when none of their lanes
+// survives the dither or clip tests, and a chunk whose LOD threshold keeps
+// every level skips the dither hash.
 //
 // Screen tiles.  A batch is Morton-compact, so its points land in a small
 // screen rectangle (the projection of its AABB's eight corners, widened by
@@ -235,17 +236,26 @@ template <int PASS, bool MV>
 __device__ __forceinline__ void project_point(const RasterArgs &a, const ViewRegsT<MV> &vr, const BatchShared &sb,
                                               const ChunkRec &c, uint32_t lo, uint32_t me,
                                               uint32_t hi, PointOut &o) {
-    // Branch-free split-precision decode: a word the chunk's level does not
-    // use was never loaded and is zero; the shifts place the coarse (low),
-    // medium and fine (high) 10-bit chunks for level 0 (30 bits), level 1
-    // (20 bits) or level >= 2 (10 bits).
-    const uint32_t sl = c.level == 0 ? 20u : (c.level == 1 ? 10u : 0u);
-    const uint32_t sm = c.level == 0 ? 10u : 0u;
-    const uint32_t x = ((lo & 1023u) << sl) | ((me & 1023u) << sm) | (hi & 1023u);
-    const uint32_t y = (((lo >> 10) & 1023u) << sl) | (((me >> 10) & 1023u) << sm) |
-                       ((hi >> 10) & 1023u);
-    const uint32_t z = (((lo >> 20) & 1023u) << sl) | (((me >> 20) & 1023u) << sm) |
-                       ((hi >> 20) & 1023u);
+    // Split-precision decode: the coarse (low), medium and fine (high) 10-bit
+    // chunks for level >= 2 (10 bits), level 1 (20 bits) or level 0 (30
+    // bits).  A word the chunk's level does not use was never loaded and is
+    // zero; the level is the same for the whole chunk, so the branch is
+    // uniform and each level does only its own shifts.
+    uint32_t x, y, z;
+    if (c.level >= 2) {
+        x = lo & 1023u;
+        y = (lo >> 10) & 1023u;
+        z = (lo >> 20) & 1023u;
+    } else if (c.level == 1) {
+        x = ((lo & 1023u) << 10) | (me & 1023u);
+        y = (((lo >> 10) & 1023u) << 10) | ((me >> 10) & 1023u);
+        z = (((lo >> 20) & 1023u) << 10) | ((me >> 20) & 1023u);
+    } else {
+        const uint32_t sl = c.level == 0 ? 20u : 0u, sm = c.level == 0 ? 10u : 0u;
+        x = ((lo & 1023u) << sl) | ((me & 1023u) << sm) | (hi & 1023u);
+        y = (((lo >> 10) & 1023u) << sl) | (((me >> 10) & 1023u) << sm) | ((hi >> 10) & 1023u);
+        z = (((lo >> 20) & 1023u) << sl) | (((me >> 20) & 1023u) << sm) | ((hi >> 20) & 1023u);
+    }
     o.px = (float)x * c.qx + c.minX;
     o.py = (float)y * c.qy + c.minY;
     o.pz = (float)z * c.qz + c.minZ;
@@ -478,11 +488,12 @@ __device__ __forceinline__ void do_point(const RasterArgs &a, const ViewRegsT<MV
                                          unsigned char *smem, const ChunkRec &c, bool tiled,
                                          bool valid, uint32_t local, uint32_t lvl, uint32_t lo,
                                          uint32_t me, uint32_t hi, uint32_t color, uint32_t fbase,
-                                         bool emit) {
+                                         bool emit, bool all_keep) {
     PointOut o;
     o.pointIndex = c.first + local;
     o.color = color;
-    o.ok = valid && keep_point(a, c, o.pointIndex, lvl);
+    o.ok = valid;
+    if (!all_keep) o.ok = o.ok && keep_point(a, c, o.pointIndex, lvl);
     if (!__any_sync(kFull, o.ok)) return;
     project_point<PASS, MV>(a, vr, sb, c, lo, me, hi, o);
     if (!__any_sync(kFull, o.ok)) return;
@@ -820,6 +831,10 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
         }();
         const bool need_med = c.level <= 1, need_high = c.level == 0;
         constexpr bool kNeedColor = PASS == PASS_COLOR || PASS == PASS_DEPTH_FRAG;
+        // Every point of the chunk passes the dither test when even its
+        // highest level (7) does with the largest dither (hash_unit reaches
+        // 1.0f; 0.5f without dither): (thr - L) + 0.5f only grows as L falls.
+        const bool all_keep = (a.u.lodDither ? 1.0f : 0.5f) < (c.thr - 7.0f) + 0.5f;
         if (PASS == PASS_COLOR_FRAG) {
             // The chunk's fragments, four per thread when 16-byte aligned.
             if ((fbase & 3u) == 0u) {
@@ -865,13 +880,13 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                 }
                 const uint32_t l0 = 4u * q;
                 do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 0 < c.count, l0 + 0,
-                               lv4 & 0xffu, lo4.x, me4.x, hi4.x, co4.x, fbase, emit);
+                               lv4 & 0xffu, lo4.x, me4.x, hi4.x, co4.x, fbase, emit, all_keep);
                 do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 1 < c.count, l0 + 1,
-                               (lv4 >> 8) & 0xffu, lo4.y, me4.y, hi4.y, co4.y, fbase, emit);
+                               (lv4 >> 8) & 0xffu, lo4.y, me4.y, hi4.y, co4.y, fbase, emit, all_keep);
                 do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 2 < c.count, l0 + 2,
-                               (lv4 >> 16) & 0xffu, lo4.z, me4.z, hi4.z, co4.z, fbase, emit);
+                               (lv4 >> 16) & 0xffu, lo4.z, me4.z, hi4.z, co4.z, fbase, emit, all_keep);
                 do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 3 < c.count, l0 + 3,
-                               lv4 >> 24, lo4.w, me4.w, hi4.w, co4.w, fbase, emit);
+                               lv4 >> 24, lo4.w, me4.w, hi4.w, co4.w, fbase, emit, all_keep);
             }
         } else {
             // Unaligned start (pointsPerBatch not a multiple of 4): one point per thread.
@@ -884,7 +899,7 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                 const uint32_t me = (v && need_med) ? a.med[i] : 0u;
                 const uint32_t hi = (v && need_high) ? a.high[i] : 0u;
                 const uint32_t co = (v && kNeedColor) ? a.colors[i] : 0u;
-                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, v, local, lv, lo, me, hi, co, fbase, emit);
+                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, v, local, lv, lo, me, hi, co, fbase, emit, all_keep);
             }
         }
         if (tiled || PASS == PASS_DEPTH_FRAG) {
@@ -1006,6 +1021,13 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
     raster_body<PASS, MV>(a);
 }
 
+// The one-view depth passes fit 64 registers without spilling, so four CTAs
+// (and their 32 KB screen tiles) share an SM.
+template <int PASS>
+__global__ void __launch_bounds__(kThreads, 4) depth_kernel(RasterArgs a) {
+    raster_body<PASS, false>(a);
+}
+
 // The colour pass that decodes the points holds a 64 KB screen tile, so at
 // most three CTAs share an SM whatever their registers; saying so lets the
 // compiler use up to 85 registers per thread instead of spilling.
@@ -1028,6 +1050,8 @@ template <int PASS, bool MV>
 constexpr auto kernel_for() {
     if constexpr (PASS == PASS_COLOR)
         return raster_kernel_color<MV>;
+    else if constexpr (!MV && is_depth(PASS))
+        return depth_kernel<PASS>;
     else
         return raster_kernel<PASS, MV>;
 }
