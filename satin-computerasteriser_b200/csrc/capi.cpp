@@ -230,6 +230,7 @@ cr_status allocate_cloud(cr_cloud *c, cr_capacity cap, const cr_raster_file *fil
     CR_CUDA(cudaMemsetAsync(c->d_batches, 0, nb * sizeof(cr_raster_batch), s));
     CR_CUDA(cudaMemsetAsync(c->d_visible, 0, nb * sizeof(cr_visible_batch), s));
     CR_CUDA(cudaMemsetAsync(c->d_counters, 0, CNT_COUNT * sizeof(uint32_t), s));
+    CR_CUDA(cudaMemsetAsync(c->d_cull_cta, 0, ctas * kCullCtaWords * sizeof(uint32_t), s));
     if ((st = alloc_ring(c))) return st;
     if ((st = upload_files(c, c->files))) return st;
     CR_CUDA(cudaStreamSynchronize(s));
@@ -884,8 +885,7 @@ static cr_status render_impl(cr_context *ctx, cr_frame *f, cr_cloud *const *clou
         if (stages & CR_STAGE_DEPTH) {
             {
                 PassTimer pt(ctx, CR_PASS_CLEAR);
-                CR_CUDA(cudaMemsetAsync(f->d_depth, 0, npix * 4, s));
-                CR_CUDA(cudaMemsetAsync(f->d_accum, 0, (npix + 1) * 16, s));  // + redo flag
+                if ((st = launch_frame_clear(f, s))) return st;  // depth, accumulators, redo flag
             }
             const CullUniforms cu = make_cull_uniforms(cfg, cam, W, H);
             {

@@ -39,6 +39,8 @@ enum CounterSlot : int {
     CNT_ERROR = 7,       // first device-side error code (0 = none)
     CNT_POINTS = 8,      // fragment span of the last cull's survivors (chunks rounded to 4)
     CNT_DONE = 9,        // CTAs finished with the dynamic cursor (the last one resets both)
+    CNT_CULL_EPOCH = 10,  // one-pass cull: launches completed (its CTAs' publish flags are epoch + 1)
+    CNT_CULL_DONE = 11,   // one-pass cull: CTAs finished (the last one advances the epoch)
     CNT_COUNT = 32
 };
 
@@ -242,7 +244,11 @@ struct CullUniforms {
 
 // Words per 256-slot CTA in CullArgs::cta_counts: survivors, chunk records,
 // fragment span.
-constexpr uint32_t kCullCtaWords = 3;
+// Per 256-slot CTA: survivor, chunk and point counts, and the one-pass
+// cull's publish flag.
+constexpr uint32_t kCullCtaWords = 4;
+// CNT_ERROR code: a one-pass cull CTA gave up waiting for a predecessor.
+constexpr uint32_t kErrCullWait = 1u;
 
 // Arguments of the cull of one view of one cloud (inputs, scratch, outputs).
 struct CullArgs {
@@ -389,6 +395,8 @@ cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t
                              const uint32_t *redo);
 // Zeroes the accumulators if *f->d_redo != 0.
 cr_status launch_accum_redo_clear(cr_frame *f, cudaStream_t s);
+// Zeroes the depth plane, the accumulators and the redo word of an HQS frame.
+cr_status launch_frame_clear(cr_frame *f, cudaStream_t s);
 // Coverage resolve (weighted-blended accumulation) into d_rgba[0].
 cr_status launch_resolve_coverage(cr_frame *f, const ResolveUniforms &u, cudaStream_t s);
 

@@ -14,6 +14,9 @@
 //      its survivors to that offset and writes one chunk record per
 //      `chunkPoints` survivor points; the last CTA publishes the totals (the
 //      CUDA counterpart of the indirect argument buffer).
+// The one-view cull does both steps in one launch (cull_one_pass: each CTA
+// publishes its counts and reads its predecessors'); batched views keep the
+// two launches, one grid row per view.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -267,6 +270,151 @@ __device__ __forceinline__ void compact_body(const CullArgs &a) {
     }
 }
 
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Polls of a predecessor's flag before a CTA gives up (about 0.1 s).
+constexpr uint32_t kCullSpinLimit = 1u << 20;
+
+// The one-view cull in one pass: every CTA classifies its 256 slots,
+// publishes its survivor, chunk and point counts (flag = this launch's
+// epoch + 1, after a release), sums the counts of the CTAs before it and
+// writes its survivors and chunk records at those offsets.  The CTAs of a
+// launch start in block order and all fit on the GPU at once (a few hundred
+// at most), so every predecessor publishes; a CTA that has polled a flag
+// kCullSpinLimit times records kErrCullWait and counts that CTA as empty
+// (its writes stay inside the outputs, the frame is wrong).  The last CTA to
+// finish advances the epoch, so the flags never need clearing.
+__global__ void __launch_bounds__(kCullThreads) cull_one_pass(CullArgs a) {
+    __shared__ uint32_t warp_counts[kCullThreads / 32], warp_chunks[kCullThreads / 32],
+        warp_points[kCullThreads / 32];
+    __shared__ uint32_t part_v[kCullThreads / 32], part_c[kCullThreads / 32],
+        part_p[kCullThreads / 32];
+    __shared__ uint32_t scan_c[kCullThreads / 32], scan_p[kCullThreads / 32];
+    const uint32_t epoch = *(volatile const uint32_t *)(a.counters + CNT_CULL_EPOCH) + 1u;
+    const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    CullRec rec;
+    const bool keep = gid < a.nbatches && cull_slot(a, gid, rec);
+    const uint32_t c = keep ? nchunks(rec.vb.activePoints, a.chunk_points) : 0u;
+    const uint32_t n = keep ? fragment_span(rec.vb.activePoints, a.chunk_points) : 0u;
+    const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
+    const uint32_t ch = __reduce_add_sync(0xffffffffu, c);
+    const uint32_t pts = __reduce_add_sync(0xffffffffu, n);
+    if (lane == 0) {
+        warp_counts[warp] = __popc(ballot);
+        warp_chunks[warp] = ch;
+        warp_points[warp] = pts;
+    }
+    __syncthreads();
+    uint32_t before = 0, total = 0, total_chunks = 0, total_points = 0;
+#pragma unroll
+    for (int w = 0; w < kCullThreads / 32; ++w) {
+        if (w < warp) before += warp_counts[w];
+        total += warp_counts[w];
+        total_chunks += warp_chunks[w];
+        total_points += warp_points[w];
+    }
+    if (threadIdx.x == 0) {
+        uint32_t *mine = a.cta_counts + kCullCtaWords * blockIdx.x;
+        mine[0] = total;
+        mine[1] = total_chunks;
+        mine[2] = total_points;
+        st_release(mine + 3, epoch);
+    }
+    // Counts of the CTAs before this one, a thread per predecessor.
+    uint32_t sv = 0, sc = 0, sp = 0;
+    bool gave_up = false;
+    for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kCullThreads) {
+        const uint32_t *w = a.cta_counts + kCullCtaWords * i;
+        bool published = false;
+        for (uint32_t polls = 0; polls < kCullSpinLimit; ++polls) {
+            if (ld_acquire(w + 3) == epoch) {
+                published = true;
+                break;
+            }
+            __nanosleep(100);
+        }
+        if (!published) {
+            gave_up = true;
+            continue;
+        }
+        sv += __ldcg(w);
+        sc += __ldcg(w + 1);
+        sp += __ldcg(w + 2);
+    }
+    if (gave_up) atomicCAS(a.counters + CNT_ERROR, 0u, kErrCullWait);
+    sv = __reduce_add_sync(0xffffffffu, sv);
+    sc = __reduce_add_sync(0xffffffffu, sc);
+    sp = __reduce_add_sync(0xffffffffu, sp);
+    if (lane == 0) {
+        part_v[warp] = sv;
+        part_c[warp] = sc;
+        part_p[warp] = sp;
+    }
+    __syncthreads();
+    uint32_t off_v = 0, off_c = 0, off_p = 0;
+#pragma unroll
+    for (int w = 0; w < kCullThreads / 32; ++w) {
+        off_v += part_v[w];
+        off_c += part_c[w];
+        off_p += part_p[w];
+    }
+    // Survivors in slot order, then their chunk records (exclusive scans of
+    // the chunk and point counts in slot order, which is survivor order).
+    if (keep) a.visible[off_v + before + __popc(ballot & ((1u << lane) - 1u))] = rec.vb;
+    const uint32_t base = off_c + block_exclusive_scan(c, scan_c);
+    const uint32_t pbase = off_p + block_exclusive_scan(n, scan_p);
+    for (uint32_t j = 0; j < c; ++j) {
+        ChunkRec k;
+        k.first = rec.first + j * a.chunk_points;
+        k.count = min(a.chunk_points, rec.vb.activePoints - j * a.chunk_points);
+        k.level = rec.vb.level;
+        k.thr = rec.vb.lodThreshold;
+        k.batchIndex = rec.vb.batchIndex;
+        k.file = rec.file;
+        k.minX = rec.minX;
+        k.minY = rec.minY;
+        k.minZ = rec.minZ;
+        k.qx = rec.qx;
+        k.qy = rec.qy;
+        k.qz = rec.qz;
+        k.x0 = rec.x0;
+        k.y0 = rec.y0;
+        k.tw = rec.tw;
+        k.th = rec.th;
+        a.chunks[base + j] = k;
+        if (a.chunk_poff) a.chunk_poff[base + j] = pbase + j * round4(a.chunk_points);
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+        // cullFinalizeUpdate (CullFinalize/Shaders.metal:3-14): {count, 1, 1}.
+        uint32_t *counters = a.counters;
+        counters[CNT_VISIBLE] = off_v + total;
+        counters[CNT_ARGS_X] = off_v + total;
+        counters[CNT_ARGS_Y] = 1u;
+        counters[CNT_ARGS_Z] = 1u;
+        counters[CNT_WORK_DEPTH] = 0u;
+        counters[CNT_WORK_COLOR] = 0u;
+        counters[CNT_DONE] = 0u;
+        counters[CNT_CHUNKS] = off_c + total_chunks;
+        counters[CNT_POINTS] = off_p + total_points;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(a.counters + CNT_CULL_DONE, 1u) == gridDim.x - 1u) {
+            a.counters[CNT_CULL_DONE] = 0u;
+            a.counters[CNT_CULL_EPOCH] = epoch;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kCullThreads) cull_classify(CullArgs a) { classify_body(a); }
 __global__ void __launch_bounds__(kCullThreads) cull_compact(CullArgs a) { compact_body(a); }
 
@@ -310,9 +458,7 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s) {
     CullArgs a{cloud->d_batches, n,  cloud->d_files,   (uint32_t)cloud->files.size(),
                cloud->d_cull_tmp, cloud->d_cull_cta, cp, u, cloud->d_visible, cloud->d_chunks,
                cloud->d_counters, nullptr};
-    cull_classify<<<ctas, kCullThreads, 0, s>>>(a);
-    CR_CUDA(cudaGetLastError());
-    cull_compact<<<ctas, kCullThreads, 0, s>>>(a);
+    cull_one_pass<<<ctas, kCullThreads, 0, s>>>(a);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

@@ -926,7 +926,7 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
 // atomics were slower), and the table is flushed with one global add pair
 // (or four 32-bit adds) per distinct pixel.  A fragment whose pixel finds no
 // slot within kHashProbes probes is added to the frame directly.
-constexpr int kHashBits = 11;
+constexpr int kHashBits = 10;
 constexpr uint32_t kHashSlots = 1u << kHashBits;
 constexpr int kHashProbes = 16;
 constexpr uint32_t kHashEmpty = 0xffffffffu;
@@ -950,7 +950,9 @@ __device__ __forceinline__ void hash_add(uint32_t *hkey, uint32_t *hsum, const R
     color_global<false>(a, vr, pix, r, g, b, 1u);
 }
 
-__global__ void __launch_bounds__(kThreads) color_hash_kernel(RasterArgs a) {
+// 1024 slots (about three times a chunk's typical distinct visible pixels)
+// and at most 40 registers: six CTAs share an SM.
+__global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(RasterArgs a) {
     if (a.t.redo && *a.t.redo == 0u) return;
     __shared__ uint32_t hkey[kHashSlots];
     __shared__ uint32_t hsum[4 * kHashSlots];

@@ -272,6 +272,20 @@ __global__ void __launch_bounds__(kThreads)
     depthf[p] = crd::uint_to_depth(depth[p]);
 }
 
+// Zeroes the depth plane and the accumulators (with the redo word behind
+// them) of an HQS frame in one launch of 16-byte stores.
+__global__ void __launch_bounds__(kThreads)
+    frame_clear(uint4 *depth4, size_t ndepth4, uint32_t *depth_tail, uint32_t ntail,
+                uint4 *accum, size_t naccum) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < naccum; i += stride)
+        accum[i] = z;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < ndepth4; i += stride)
+        depth4[i] = z;
+    if (blockIdx.x == 0 && threadIdx.x < ntail) depth_tail[threadIdx.x] = 0u;
+}
+
 // Top bit of every depth word flipped: unsigned order <-> signed order.
 __global__ void __launch_bounds__(kThreads)
     flip_depth_order(uint4 *d4, size_t n4, uint32_t *tail, uint32_t ntail) {
@@ -300,6 +314,16 @@ cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t
         redo);
     CR_CUDA(cudaGetLastError());
     f->final_rgba = 0;
+    return CR_OK;
+}
+
+cr_status launch_frame_clear(cr_frame *f, cudaStream_t s) {
+    const size_t npix = (size_t)f->width * (size_t)f->height;
+    const size_t n4 = npix / 4;  // depth words in whole 16-byte groups (the plane is 256-byte aligned)
+    frame_clear<<<f->ctx->sm_count * 8, kThreads, 0, s>>>(
+        reinterpret_cast<uint4 *>(f->d_depth), n4, f->d_depth + 4 * n4, (uint32_t)(npix - 4 * n4),
+        f->d_accum, npix + 1);
+    CR_CUDA(cudaGetLastError());
     return CR_OK;
 }
 
