@@ -931,10 +931,19 @@ constexpr uint32_t kHashSlots = 1u << kHashBits;
 constexpr int kHashProbes = 16;
 constexpr uint32_t kHashEmpty = 0xffffffffu;
 
+// Slot of pixel (x, y): x + 37 y over the table.  Distinct pixels of any
+// 37 × 27 window take distinct slots, and the 32 lanes of a warp, whose
+// fragments lie in one small patch of the screen, mostly fall in distinct
+// shared-memory banks (x + 5 y mod 32).
+__device__ __forceinline__ uint32_t hash_slot(uint32_t xy) {
+    return ((xy & 0xffffu) + 37u * (xy >> 16)) & (kHashSlots - 1u);
+}
+
 __device__ __forceinline__ void hash_add(uint32_t *hkey, uint32_t *hsum, const RasterArgs &a,
-                                         const ViewRegsT<false> &vr, uint32_t pix, uint32_t col) {
+                                         const ViewRegsT<false> &vr, uint32_t pix, uint32_t xy,
+                                         uint32_t col) {
     const uint32_t r = col & 0xffu, g = (col >> 8) & 0xffu, b = (col >> 16) & 0xffu;
-    uint32_t h = (pix * 2654435761u) >> (32 - kHashBits);
+    uint32_t h = hash_slot(xy);
     for (int probe = 0; probe < kHashProbes; ++probe) {
         uint32_t cur = hkey[h];
         if (cur == kHashEmpty) cur = atomicCAS(hkey + h, kHashEmpty, pix);
@@ -987,7 +996,7 @@ __global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(RasterArgs a) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
                     if (cl[q] != 0u && zs[q] >= crd::uint_to_depth(cl[q]) * a.keep_scale)
-                        hash_add(hkey, hsum, a, vr, pix[q], cs[q]);
+                        hash_add(hkey, hsum, a, vr, pix[q], xs[q], cs[q]);
             }
         } else {
             for (uint32_t f = threadIdx.x; f < n; f += kThreads) {
@@ -995,7 +1004,7 @@ __global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(RasterArgs a) {
                 const uint32_t pix = (xy >> 16) * (uint32_t)W + (xy & 0xffffu);
                 const uint32_t cl = __ldg(a.t.depth + pix);
                 if (cl != 0u && a.frag_z[base + f] >= crd::uint_to_depth(cl) * a.keep_scale)
-                    hash_add(hkey, hsum, a, vr, pix, a.frag_col[base + f]);
+                    hash_add(hkey, hsum, a, vr, pix, xy, a.frag_col[base + f]);
             }
         }
         __syncthreads();  // the chunk's sums are complete
