@@ -935,11 +935,19 @@ static cr_status render_impl(cr_context *ctx, cr_frame *f, cr_cloud *const *clou
                 RasterTargets tx = t;
                 tx.packed = 0;
                 tx.redo = f->d_redo;
-                if ((st = launch_accum_redo_clear(f, s))) return st;
-                for (cr_cloud *c : resident)
-                    if ((st = launch_raster(c, frags ? PASS_COLOR_FRAG : PASS_COLOR, rau, tx, s)))
+                if (frags && resident.size() <= hqs_redo_max_clouds()) {
+                    // From the fragments: all three steps in one launch.
+                    if ((st = launch_hqs_redo(f, resident.data(), (uint32_t)resident.size(), rau,
+                                              tx, ru, s)))
                         return st;
-                if ((st = launch_resolve_hqs(f, ru, s, false, f->d_redo))) return st;
+                } else {
+                    if ((st = launch_accum_redo_clear(f, s))) return st;
+                    for (cr_cloud *c : resident)
+                        if ((st = launch_raster(c, frags ? PASS_COLOR_FRAG : PASS_COLOR, rau, tx,
+                                                s)))
+                            return st;
+                    if ((st = launch_resolve_hqs(f, ru, s, false, f->d_redo))) return st;
+                }
             }
             f->last_mode = 0;
         }

@@ -395,6 +395,14 @@ cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t
                              const uint32_t *redo);
 // Zeroes the accumulators if *f->d_redo != 0.
 cr_status launch_accum_redo_clear(cr_frame *f, cudaStream_t s);
+// The exact re-run of a frame drawn from fragments, in one single-CTA launch
+// that returns at once unless *t.redo != 0: zero the accumulators, colour pass
+// of every cloud with 32-bit adds (t.packed = 0), resolve into d_rgba[0].
+// At most hqs_redo_max_clouds() clouds.
+cr_status launch_hqs_redo(cr_frame *f, cr_cloud *const *clouds, uint32_t nclouds,
+                          const RasterUniforms &u, const RasterTargets &t,
+                          const ResolveUniforms &ru, cudaStream_t s);
+uint32_t hqs_redo_max_clouds();
 // Zeroes the depth plane, the accumulators and the redo word of an HQS frame.
 cr_status launch_frame_clear(cr_frame *f, cudaStream_t s);
 // Coverage resolve (weighted-blended accumulation) into d_rgba[0].

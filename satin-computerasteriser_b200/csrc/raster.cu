@@ -42,6 +42,7 @@
 // bit-identical to a per-point atomic order either way.
 #include "cr_device.cuh"
 #include "cr_internal.h"
+#include "cr_resolve.cuh"
 
 namespace {
 
@@ -959,6 +960,60 @@ __device__ __forceinline__ void hash_add(uint32_t *hkey, uint32_t *hsum, const R
     color_global<false>(a, vr, pix, r, g, b, 1u);
 }
 
+// Clears the table (at kernel start).
+__device__ __forceinline__ void hash_clear(uint32_t *hkey, uint32_t *hsum) {
+    for (uint32_t i = threadIdx.x; i < kHashSlots; i += kThreads) {
+        hkey[i] = kHashEmpty;
+        hsum[i] = hsum[kHashSlots + i] = hsum[2 * kHashSlots + i] = hsum[3 * kHashSlots + i] = 0u;
+    }
+}
+
+// The colour pass over chunk k's fragments: sums into the table, then flushes
+// and clears it.  Every thread of the CTA calls this; the caller's barrier
+// before the next chunk orders the clearing before its first add.
+__device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<false> &vr,
+                                           uint32_t *hkey, uint32_t *hsum, uint32_t k) {
+    const int W = a.u.width;
+    const uint32_t n = __ldg(a.frag_count + k);
+    const uint32_t base = __ldg(&a.chunks[k].first);
+    if ((base & 3u) == 0u) {
+        for (uint32_t f = 4u * threadIdx.x; f < n; f += 4u * kThreads) {
+            const uint4 xy = __ldcs(reinterpret_cast<const uint4 *>(a.frag_xy + base + f));
+            const float4 z = __ldcs(reinterpret_cast<const float4 *>(a.frag_z + base + f));
+            const uint4 co = __ldcs(reinterpret_cast<const uint4 *>(a.frag_col + base + f));
+            const uint32_t xs[4] = {xy.x, xy.y, xy.z, xy.w}, cs[4] = {co.x, co.y, co.z, co.w};
+            const float zs[4] = {z.x, z.y, z.z, z.w};
+            uint32_t pix[4], cl[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                pix[q] = (xs[q] >> 16) * (uint32_t)W + (xs[q] & 0xffffu);
+                cl[q] = f + q < n ? __ldg(a.t.depth + pix[q]) : 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (cl[q] != 0u && zs[q] >= crd::uint_to_depth(cl[q]) * a.keep_scale)
+                    hash_add(hkey, hsum, a, vr, pix[q], xs[q], cs[q]);
+        }
+    } else {
+        for (uint32_t f = threadIdx.x; f < n; f += kThreads) {
+            const uint32_t xy = a.frag_xy[base + f];
+            const uint32_t pix = (xy >> 16) * (uint32_t)W + (xy & 0xffffu);
+            const uint32_t cl = __ldg(a.t.depth + pix);
+            if (cl != 0u && a.frag_z[base + f] >= crd::uint_to_depth(cl) * a.keep_scale)
+                hash_add(hkey, hsum, a, vr, pix, xy, a.frag_col[base + f]);
+        }
+    }
+    __syncthreads();  // the chunk's sums are complete
+    for (uint32_t i = threadIdx.x; i < kHashSlots; i += kThreads) {
+        const uint32_t pix = hkey[i];
+        if (pix == kHashEmpty) continue;
+        color_global<false>(a, vr, pix, hsum[i], hsum[kHashSlots + i], hsum[2 * kHashSlots + i],
+                            hsum[3 * kHashSlots + i]);
+        hkey[i] = kHashEmpty;
+        hsum[i] = hsum[kHashSlots + i] = hsum[2 * kHashSlots + i] = hsum[3 * kHashSlots + i] = 0u;
+    }
+}
+
 // 1024 slots (about three times a chunk's typical distinct visible pixels)
 // and at most 40 registers: six CTAs share an SM.
 __global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(RasterArgs a) {
@@ -968,55 +1023,13 @@ __global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(RasterArgs a) {
     __shared__ uint32_t s_k;
     const uint32_t nchunks = a.counters[CNT_CHUNKS];
     const ViewRegsT<false> vr(a);
-    const int W = a.u.width;
-    for (uint32_t i = threadIdx.x; i < kHashSlots; i += kThreads) {
-        hkey[i] = kHashEmpty;
-        hsum[i] = hsum[kHashSlots + i] = hsum[2 * kHashSlots + i] = hsum[3 * kHashSlots + i] = 0u;
-    }
+    hash_clear(hkey, hsum);
     for (;;) {
         if (threadIdx.x == 0) s_k = atomicAdd(a.counters + CNT_WORK_DEPTH, 1u);
         __syncthreads();  // s_k and the cleared table
         const uint32_t k = s_k;
         if (k >= nchunks) break;
-        const uint32_t n = __ldg(a.frag_count + k);
-        const uint32_t base = __ldg(&a.chunks[k].first);
-        if ((base & 3u) == 0u) {
-            for (uint32_t f = 4u * threadIdx.x; f < n; f += 4u * kThreads) {
-                const uint4 xy = __ldcs(reinterpret_cast<const uint4 *>(a.frag_xy + base + f));
-                const float4 z = __ldcs(reinterpret_cast<const float4 *>(a.frag_z + base + f));
-                const uint4 co = __ldcs(reinterpret_cast<const uint4 *>(a.frag_col + base + f));
-                const uint32_t xs[4] = {xy.x, xy.y, xy.z, xy.w}, cs[4] = {co.x, co.y, co.z, co.w};
-                const float zs[4] = {z.x, z.y, z.z, z.w};
-                uint32_t pix[4], cl[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    pix[q] = (xs[q] >> 16) * (uint32_t)W + (xs[q] & 0xffffu);
-                    cl[q] = f + q < n ? __ldg(a.t.depth + pix[q]) : 0u;
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (cl[q] != 0u && zs[q] >= crd::uint_to_depth(cl[q]) * a.keep_scale)
-                        hash_add(hkey, hsum, a, vr, pix[q], xs[q], cs[q]);
-            }
-        } else {
-            for (uint32_t f = threadIdx.x; f < n; f += kThreads) {
-                const uint32_t xy = a.frag_xy[base + f];
-                const uint32_t pix = (xy >> 16) * (uint32_t)W + (xy & 0xffffu);
-                const uint32_t cl = __ldg(a.t.depth + pix);
-                if (cl != 0u && a.frag_z[base + f] >= crd::uint_to_depth(cl) * a.keep_scale)
-                    hash_add(hkey, hsum, a, vr, pix, xy, a.frag_col[base + f]);
-            }
-        }
-        __syncthreads();  // the chunk's sums are complete
-        for (uint32_t i = threadIdx.x; i < kHashSlots; i += kThreads) {
-            const uint32_t pix = hkey[i];
-            if (pix == kHashEmpty) continue;
-            color_global<false>(a, vr, pix, hsum[i], hsum[kHashSlots + i],
-                                hsum[2 * kHashSlots + i], hsum[3 * kHashSlots + i]);
-            hkey[i] = kHashEmpty;
-            hsum[i] = hsum[kHashSlots + i] = hsum[2 * kHashSlots + i] = hsum[3 * kHashSlots + i] = 0u;
-        }
-        // The next claim's barrier orders the clearing before the next chunk.
+        hash_chunk(a, vr, hkey, hsum, k);
     }
     if (threadIdx.x == 0) {
         __threadfence();
@@ -1024,6 +1037,59 @@ __global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(RasterArgs a) {
             a.counters[CNT_WORK_DEPTH] = 0u;
             a.counters[CNT_DONE] = 0u;
         }
+    }
+}
+
+// Exact re-run of a frame whose packed colour adds may have carried (the
+// resolve set the redo word).  One CTA, launched every frame, that returns
+// at once unless the word is set; then, in order, it zeroes the
+// accumulators, runs the colour pass of every cloud over its fragments with
+// one 32-bit add per field, and resolves every pixel.  A single CTA orders
+// the three steps with block barriers, so they take one launch instead of
+// three; the re-run is rare and its speed does not matter.
+struct RedoCloud {
+    const ChunkRec *chunks;
+    const uint32_t *counters, *frag_count, *frag_xy, *frag_col;
+    const float *frag_z;
+};
+constexpr uint32_t kRedoMaxClouds = 32;
+struct RedoArgs {
+    RasterArgs a;  // frame targets (unpacked adds) and uniforms; per-cloud fields from clouds[]
+    RedoCloud clouds[kRedoMaxClouds];
+    uint32_t nclouds;
+    const uint32_t *redo;
+    uint32_t *rgba;
+    float *depthf;
+    uint32_t npix;
+    ResolveUniforms ru;
+};
+
+__global__ void __launch_bounds__(kThreads) hqs_redo_kernel(RedoArgs r) {
+    if (*r.redo == 0u) return;
+    __shared__ uint32_t hkey[kHashSlots];
+    __shared__ uint32_t hsum[4 * kHashSlots];
+    for (uint32_t p = threadIdx.x; p < r.npix; p += kThreads) r.a.t.accum[p] = make_uint4(0, 0, 0, 0);
+    hash_clear(hkey, hsum);
+    __syncthreads();  // accumulators and table zeroed
+    for (uint32_t ci = 0; ci < r.nclouds; ++ci) {
+        RasterArgs a = r.a;
+        a.chunks = r.clouds[ci].chunks;
+        a.frag_count = const_cast<uint32_t *>(r.clouds[ci].frag_count);
+        a.frag_xy = const_cast<uint32_t *>(r.clouds[ci].frag_xy);
+        a.frag_z = const_cast<float *>(r.clouds[ci].frag_z);
+        a.frag_col = const_cast<uint32_t *>(r.clouds[ci].frag_col);
+        const ViewRegsT<false> vr(a);
+        const uint32_t nchunks = r.clouds[ci].counters[CNT_CHUNKS];
+        for (uint32_t k = 0; k < nchunks; ++k) {
+            hash_chunk(a, vr, hkey, hsum, k);
+            __syncthreads();  // the table is clear again
+        }
+    }
+    __threadfence();
+    __syncthreads();  // every add of the block has reached L2
+    for (uint32_t p = threadIdx.x; p < r.npix; p += kThreads) {
+        const uint4 acc = __ldcg(r.a.t.accum + p);
+        crd::resolve_pixel(acc, acc.w ? r.a.t.depth[p] : 0u, r.ru, r.rgba[p], r.depthf[p]);
     }
 }
 
@@ -1170,6 +1236,30 @@ cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }
+
+cr_status launch_hqs_redo(cr_frame *f, cr_cloud *const *clouds, uint32_t nclouds,
+                          const RasterUniforms &u, const RasterTargets &t,
+                          const ResolveUniforms &ru, cudaStream_t s) {
+    if (nclouds > kRedoMaxClouds || t.packed || !t.redo)
+        return cri::fail(CR_ERR_INTERNAL, "launch_hqs_redo: arguments");
+    if (nclouds == 0) return CR_OK;  // no sample: the resolve cannot have asked for a re-run
+    RedoArgs r;
+    r.a = make_args(clouds[0], u, t);
+    for (uint32_t i = 0; i < nclouds; ++i)
+        r.clouds[i] = RedoCloud{clouds[i]->d_chunks,   clouds[i]->d_counters, clouds[i]->d_frag_count,
+                                clouds[i]->d_frag_xy, clouds[i]->d_frag_col, clouds[i]->d_frag_z};
+    r.nclouds = nclouds;
+    r.redo = t.redo;
+    r.rgba = f->d_rgba[0];
+    r.depthf = f->d_depthf;
+    r.npix = (uint32_t)f->width * (uint32_t)f->height;
+    r.ru = ru;
+    hqs_redo_kernel<<<1, kThreads, 0, s>>>(r);
+    CR_CUDA(cudaGetLastError());
+    return CR_OK;
+}
+
+uint32_t hqs_redo_max_clouds() { return kRedoMaxClouds; }
 
 cr_status launch_raster_f32(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
                             const RasterTargets &t, const float *colors, const float *dldimg,

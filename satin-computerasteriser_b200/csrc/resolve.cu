@@ -12,29 +12,14 @@
 
 #include "cr_device.cuh"
 #include "cr_internal.h"
+#include "cr_resolve.cuh"
 
 namespace {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ uint32_t pack_rgba(float r, float g, float b, float a) {
-    return crd::unorm8(r) | (crd::unorm8(g) << 8) | (crd::unorm8(b) << 16) | (crd::unorm8(a) << 24);
-}
-
-// resolveUpdate of one pixel (count path).
-__device__ __forceinline__ void resolve_pixel(const uint4 acc, uint32_t depth,
-                                              const ResolveUniforms &u, uint32_t &rgba,
-                                              float &depthf) {
-    if (acc.w == 0u) {
-        rgba = pack_rgba(u.background[0], u.background[1], u.background[2], 0.0f);
-        depthf = 0.0f;
-        return;
-    }
-    const float inv = 1.0f / (float)acc.w;
-    rgba = pack_rgba(((float)acc.x * inv) / 255.0f, ((float)acc.y * inv) / 255.0f,
-                     ((float)acc.z * inv) / 255.0f, 1.0f);
-    depthf = crd::uint_to_depth(depth);
-}
+using crd::pack_rgba;
+using crd::resolve_pixel;
 
 __global__ void __launch_bounds__(kThreads)
     resolve_hqs(const uint32_t *__restrict__ depth, const uint4 *__restrict__ accum,
