@@ -883,15 +883,22 @@ static cr_status render_impl(cr_context *ctx, cr_frame *f, cr_cloud *const *clou
         RasterTargets t{f->d_depth, f->d_accum, f->d_nearest};
         t.packed = packed ? 1 : 0;
         if (stages & CR_STAGE_DEPTH) {
-            {
+            // The frame's depth plane, accumulators and redo word are zeroed
+            // by extra CTAs of the first cull launch (its CTAs are few and
+            // latency-bound), or by their own launch without a cloud to cull.
+            const bool clear_in_cull = !resident.empty() && resident[0]->cap.maxResidentBatches > 0;
+            if (!clear_in_cull) {
                 PassTimer pt(ctx, CR_PASS_CLEAR);
-                if ((st = launch_frame_clear(f, s))) return st;  // depth, accumulators, redo flag
+                if ((st = launch_frame_clear(f, s))) return st;
             }
             const CullUniforms cu = make_cull_uniforms(cfg, cam, W, H);
             {
                 PassTimer pt(ctx, CR_PASS_CULL);
-                for (cr_cloud *c : resident)
-                    if ((st = launch_cull(c, cu, s))) return st;
+                const FrameClear fc = frame_clear_of(f);
+                for (size_t i = 0; i < resident.size(); ++i)
+                    if ((st = launch_cull(resident[i], cu, s,
+                                          i == 0 && clear_in_cull ? &fc : nullptr)))
+                        return st;
             }
             {
                 PassTimer pt(ctx, CR_PASS_DEPTH);

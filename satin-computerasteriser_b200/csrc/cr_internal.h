@@ -267,7 +267,21 @@ struct CullArgs {
                                 // view's fragment span, a multiple of 4 (NULL: not written)
 };
 
-cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s);
+// Zeroing of an HQS frame's depth plane (whole 16-byte groups, then a tail
+// of up to three words) and accumulators with the redo word behind them.
+struct FrameClear {
+    uint4 *depth4;
+    size_t ndepth4;
+    uint32_t *tail;
+    uint32_t ntail;
+    uint4 *accum;
+    size_t naccum;
+};
+FrameClear frame_clear_of(cr_frame *f);
+
+// clear: also zero that frame in the same launch (CTAs after the cull's).
+cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s,
+                      const FrameClear *clear = nullptr);
 // Culls of several views in one pair of launches; d_args holds one CullArgs
 // per view (device memory).
 cr_status launch_cull_views(const CullArgs *d_args, uint32_t nslots, uint32_t nviews,

@@ -292,7 +292,19 @@ constexpr uint32_t kCullSpinLimit = 1u << 20;
 // kCullSpinLimit times records kErrCullWait and counts that CTA as empty
 // (its writes stay inside the outputs, the frame is wrong).  The last CTA to
 // finish advances the epoch, so the flags never need clearing.
-__global__ void __launch_bounds__(kCullThreads) cull_one_pass(CullArgs a) {
+__global__ void __launch_bounds__(kCullThreads) cull_one_pass(CullArgs a, FrameClear clear) {
+    // CTAs past the cull's zero the frame (none wait on them, and they wait
+    // on nothing), overlapping the cull's latency-bound work.
+    const uint32_t cull_ctas = (a.nbatches + kCullThreads - 1) / kCullThreads;
+    if (blockIdx.x >= cull_ctas) {
+        const size_t stride = (size_t)(gridDim.x - cull_ctas) * kCullThreads;
+        const size_t t0 = (size_t)(blockIdx.x - cull_ctas) * kCullThreads + threadIdx.x;
+        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+        for (size_t i = t0; i < clear.naccum; i += stride) clear.accum[i] = z;
+        for (size_t i = t0; i < clear.ndepth4; i += stride) clear.depth4[i] = z;
+        if (t0 < clear.ntail) clear.tail[t0] = 0u;
+        return;
+    }
     __shared__ uint32_t warp_counts[kCullThreads / 32], warp_chunks[kCullThreads / 32],
         warp_points[kCullThreads / 32];
     __shared__ uint32_t part_v[kCullThreads / 32], part_c[kCullThreads / 32],
@@ -393,7 +405,7 @@ __global__ void __launch_bounds__(kCullThreads) cull_one_pass(CullArgs a) {
         a.chunks[base + j] = k;
         if (a.chunk_poff) a.chunk_poff[base + j] = pbase + j * round4(a.chunk_points);
     }
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+    if (blockIdx.x == cull_ctas - 1 && threadIdx.x == 0) {
         // cullFinalizeUpdate (CullFinalize/Shaders.metal:3-14): {count, 1, 1}.
         uint32_t *counters = a.counters;
         counters[CNT_VISIBLE] = off_v + total;
@@ -408,7 +420,7 @@ __global__ void __launch_bounds__(kCullThreads) cull_one_pass(CullArgs a) {
     }
     if (threadIdx.x == 0) {
         __threadfence();
-        if (atomicAdd(a.counters + CNT_CULL_DONE, 1u) == gridDim.x - 1u) {
+        if (atomicAdd(a.counters + CNT_CULL_DONE, 1u) == cull_ctas - 1u) {
             a.counters[CNT_CULL_DONE] = 0u;
             a.counters[CNT_CULL_EPOCH] = epoch;
         }
@@ -446,11 +458,13 @@ uint64_t chunk_capacity(const cr_capacity &cap, int chunk_points) {
     return std::max<uint64_t>(1, (uint64_t)cap.maxResidentBatches * per);
 }
 
-cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s) {
+cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s,
+                      const FrameClear *clear) {
     const uint32_t n = cloud->cap.maxResidentBatches;
     if (n == 0) {
         cull_empty<<<1, 1, 0, s>>>(cloud->d_counters);
         CR_CUDA(cudaGetLastError());
+        if (clear) return cri::fail(CR_ERR_INTERNAL, "launch_cull: clear with an empty pool");
         return CR_OK;
     }
     const uint32_t cp = (uint32_t)std::max(cloud->ctx->chunk_points, kMinChunkPoints);
@@ -458,7 +472,8 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s) {
     CullArgs a{cloud->d_batches, n,  cloud->d_files,   (uint32_t)cloud->files.size(),
                cloud->d_cull_tmp, cloud->d_cull_cta, cp, u, cloud->d_visible, cloud->d_chunks,
                cloud->d_counters, nullptr};
-    cull_one_pass<<<ctas, kCullThreads, 0, s>>>(a);
+    const uint32_t clear_ctas = clear ? (uint32_t)cloud->ctx->sm_count * 2u : 0u;
+    cull_one_pass<<<ctas + clear_ctas, kCullThreads, 0, s>>>(a, clear ? *clear : FrameClear{});
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

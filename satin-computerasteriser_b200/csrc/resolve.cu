@@ -302,12 +302,17 @@ cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t
     return CR_OK;
 }
 
-cr_status launch_frame_clear(cr_frame *f, cudaStream_t s) {
+FrameClear frame_clear_of(cr_frame *f) {
     const size_t npix = (size_t)f->width * (size_t)f->height;
     const size_t n4 = npix / 4;  // depth words in whole 16-byte groups (the plane is 256-byte aligned)
-    frame_clear<<<f->ctx->sm_count * 8, kThreads, 0, s>>>(
-        reinterpret_cast<uint4 *>(f->d_depth), n4, f->d_depth + 4 * n4, (uint32_t)(npix - 4 * n4),
-        f->d_accum, npix + 1);
+    return FrameClear{reinterpret_cast<uint4 *>(f->d_depth), n4, f->d_depth + 4 * n4,
+                      (uint32_t)(npix - 4 * n4), f->d_accum, npix + 1};
+}
+
+cr_status launch_frame_clear(cr_frame *f, cudaStream_t s) {
+    const FrameClear c = frame_clear_of(f);
+    frame_clear<<<f->ctx->sm_count * 8, kThreads, 0, s>>>(c.depth4, c.ndepth4, c.tail, c.ntail,
+                                                           c.accum, c.naccum);
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }
