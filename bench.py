@@ -412,7 +412,6 @@ def run_ours(args, dist):
     stream = torch.cuda.ExternalStream(ctx.stream(), device=f"cuda:{dist.local}")
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    ctx.set_profiling(True)
     sampler = ClockSampler(dist.local)
     dist.barrier()
     ctx.synchronize()
@@ -430,6 +429,14 @@ def run_ours(args, dist):
     ctx.synchronize()
     dist.barrier()
     ms = ev0.elapsed_time(ev1)
+    # Per-pass times from a second run of the same frames with a CUDA event
+    # around every pass; the timed run above records none, so that the
+    # passes follow one another as they do for a user.
+    ctx.set_profiling(True)
+    for p in timed:
+        ras.update(cams[p])
+        frame_encoder.encode()
+    ctx.synchronize()
     times = ctx.pass_times(len(timed))
     ctx.set_profiling(False)
     ms_max = dist.max(ms)

@@ -15,6 +15,17 @@
 
 namespace crd {
 
+// Programmatic dependent launch (sm_90+).  A kernel launched with
+// programmatic stream serialisation may start while the kernel before it on
+// the stream is still running; grid_wait() blocks until that kernel has
+// completed and its memory is visible (a no-op for a normal launch), so
+// every kernel calls it before touching memory the previous one writes.
+// launch_dependents() lets the next kernel's launch begin.
+__device__ __forceinline__ void grid_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 struct f3 {
     float x, y, z;
 };

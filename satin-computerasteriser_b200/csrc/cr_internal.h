@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <utility>
 #include <stdint.h>
 
 #include <string>
@@ -266,6 +267,25 @@ struct CullArgs {
     uint32_t *chunk_poff;       // per chunk record: offset of its fragments within the
                                 // view's fragment span, a multiple of 4 (NULL: not written)
 };
+
+// Launches a kernel that may begin while the previous kernel on the stream
+// finishes (programmatic stream serialisation); the kernel orders itself
+// after that kernel with crd::grid_wait().
+template <typename... Params, typename... Args>
+cudaError_t launch_programmatic(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                                cudaStream_t s, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Zeroing of an HQS frame's depth plane (whole 16-byte groups, then a tail
 // of up to three words) and accumulators with the redo word behind them.

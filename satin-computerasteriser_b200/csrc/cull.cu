@@ -293,6 +293,7 @@ constexpr uint32_t kCullSpinLimit = 1u << 20;
 // (its writes stay inside the outputs, the frame is wrong).  The last CTA to
 // finish advances the epoch, so the flags never need clearing.
 __global__ void __launch_bounds__(kCullThreads) cull_one_pass(CullArgs a, FrameClear clear) {
+    crd::launch_dependents();  // the depth pass waits for this grid itself
     // CTAs past the cull's zero the frame (none wait on them, and they wait
     // on nothing), overlapping the cull's latency-bound work.
     const uint32_t cull_ctas = (a.nbatches + kCullThreads - 1) / kCullThreads;

@@ -682,6 +682,8 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
     __shared__ uint32_t s_vbegin[MV ? kMaxViews + 1 : 1];
     __shared__ unsigned long long s_pbegin[MV && kFrag ? kMaxViews + 1 : 1];
     __shared__ uint32_t s_wsum[kThreads / 32];
+    crd::grid_wait();
+    crd::launch_dependents();
     if (a.t.redo && *a.t.redo == 0u) return;
     uint32_t nchunks;
     bool emit = true;  // fragments fit the arena (batched views)
@@ -1017,6 +1019,8 @@ __device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<
 // 1024 slots (about three times a chunk's typical distinct visible pixels)
 // and at most 40 registers: six CTAs share an SM.
 __global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(RasterArgs a) {
+    crd::grid_wait();
+    crd::launch_dependents();
     if (a.t.redo && *a.t.redo == 0u) return;
     __shared__ uint32_t hkey[kHashSlots];
     __shared__ uint32_t hsum[4 * kHashSlots];
@@ -1065,6 +1069,7 @@ struct RedoArgs {
 };
 
 __global__ void __launch_bounds__(kThreads) hqs_redo_kernel(RedoArgs r) {
+    crd::grid_wait();
     if (*r.redo == 0u) return;
     __shared__ uint32_t hkey[kHashSlots];
     __shared__ uint32_t hsum[4 * kHashSlots];
@@ -1211,9 +1216,15 @@ RasterArgs make_args(cr_cloud *cloud, const RasterUniforms &u, const RasterTarge
     return a;
 }
 
+// One-view passes start while the previous kernel drains (programmatic
+// dependent launch); batched views, captured in a graph, launch plainly.
 template <int PASS, bool MV>
 void launch_pass(const RasterArgs &a, int grid, cudaStream_t s) {
-    kernel_for<PASS, MV>()<<<grid, kThreads, TileCfg<PASS>::kBytes, s>>>(a);
+    if constexpr (MV)
+        kernel_for<PASS, MV>()<<<grid, kThreads, TileCfg<PASS>::kBytes, s>>>(a);
+    else
+        launch_programmatic(kernel_for<PASS, MV>(), dim3(grid), dim3(kThreads),
+                            (size_t)TileCfg<PASS>::kBytes, s, a);
 }
 
 }  // namespace
@@ -1229,7 +1240,7 @@ cr_status launch_raster(cr_cloud *cloud, RasterPass pass, const RasterUniforms &
     case PASS_COLOR: launch_pass<PASS_COLOR, false>(a, grid, s); break;
     case PASS_DEPTH_FRAG: launch_pass<PASS_DEPTH_FRAG, false>(a, grid, s); break;
     case PASS_COLOR_FRAG:
-        color_hash_kernel<<<grid, kThreads, 0, s>>>(a);
+        CR_CUDA(launch_programmatic(color_hash_kernel, dim3(grid), dim3(kThreads), 0, s, a));
         break;
     default: launch_pass<PASS_NEAREST, false>(a, grid, s); break;
     }
@@ -1254,7 +1265,7 @@ cr_status launch_hqs_redo(cr_frame *f, cr_cloud *const *clouds, uint32_t nclouds
     r.depthf = f->d_depthf;
     r.npix = (uint32_t)f->width * (uint32_t)f->height;
     r.ru = ru;
-    hqs_redo_kernel<<<1, kThreads, 0, s>>>(r);
+    CR_CUDA(launch_programmatic(hqs_redo_kernel, dim3(1), dim3(kThreads), 0, s, r));
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

@@ -25,6 +25,8 @@ __global__ void __launch_bounds__(kThreads)
     resolve_hqs(const uint32_t *__restrict__ depth, const uint4 *__restrict__ accum,
                 uint32_t *__restrict__ rgba, float *__restrict__ depthf, uint32_t npix,
                 ResolveUniforms u, uint32_t *redo_flag, int check, const uint32_t *redo) {
+    crd::grid_wait();
+    crd::launch_dependents();
     if (redo && *redo == 0u) return;
     for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < npix; p += gridDim.x * kThreads) {
         const uint4 acc = accum[p];
@@ -294,9 +296,10 @@ cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t
     // One pixel per thread; the gated re-run (rarely needed) uses a small
     // grid-stride grid so that skipping it costs little.
     const uint32_t grid = redo ? (uint32_t)f->ctx->sm_count * 4 : (npix + kThreads - 1) / kThreads;
-    resolve_hqs<<<grid, kThreads, 0, s>>>(
-        f->d_depth, f->d_accum, f->d_rgba[0], f->d_depthf, npix, u, f->d_redo, check ? 1 : 0,
-        redo);
+    CR_CUDA(launch_programmatic(resolve_hqs, dim3(grid), dim3(kThreads), 0, s,
+                                (const uint32_t *)f->d_depth, (const uint4 *)f->d_accum,
+                                f->d_rgba[0], f->d_depthf, npix, u, f->d_redo, check ? 1 : 0,
+                                redo));
     CR_CUDA(cudaGetLastError());
     f->final_rgba = 0;
     return CR_OK;
