@@ -293,6 +293,7 @@ constexpr uint32_t kCullSpinLimit = 1u << 20;
 // (its writes stay inside the outputs, the frame is wrong).  The last CTA to
 // finish advances the epoch, so the flags never need clearing.
 __global__ void __launch_bounds__(kCullThreads) cull_one_pass(CullArgs a, FrameClear clear) {
+    crd::grid_wait();          // the previous frame's passes have finished with the planes
     crd::launch_dependents();  // the depth pass waits for this grid itself
     // CTAs past the cull's zero the frame (none wait on them, and they wait
     // on nothing), overlapping the cull's latency-bound work.
@@ -474,7 +475,8 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s,
                cloud->d_cull_tmp, cloud->d_cull_cta, cp, u, cloud->d_visible, cloud->d_chunks,
                cloud->d_counters, nullptr};
     const uint32_t clear_ctas = clear ? (uint32_t)cloud->ctx->sm_count * 2u : 0u;
-    cull_one_pass<<<ctas + clear_ctas, kCullThreads, 0, s>>>(a, clear ? *clear : FrameClear{});
+    CR_CUDA(launch_programmatic(cull_one_pass, dim3(ctas + clear_ctas), dim3(kCullThreads), 0, s, a,
+                                clear ? *clear : FrameClear{}));
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }

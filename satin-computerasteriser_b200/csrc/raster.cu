@@ -1070,6 +1070,7 @@ struct RedoArgs {
 
 __global__ void __launch_bounds__(kThreads) hqs_redo_kernel(RedoArgs r) {
     crd::grid_wait();
+    crd::launch_dependents();
     if (*r.redo == 0u) return;
     __shared__ uint32_t hkey[kHashSlots];
     __shared__ uint32_t hsum[4 * kHashSlots];

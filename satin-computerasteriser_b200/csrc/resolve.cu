@@ -28,14 +28,30 @@ __global__ void __launch_bounds__(kThreads)
     crd::grid_wait();
     crd::launch_dependents();
     if (redo && *redo == 0u) return;
-    for (uint32_t p = blockIdx.x * kThreads + threadIdx.x; p < npix; p += gridDim.x * kThreads) {
-        const uint4 acc = accum[p];
-        // Packed colour adds are exact while every count is at most
-        // kPackedMaxCount: past it a channel sum may have carried into its
-        // neighbour field, and the frame's colour pass is re-run exactly.
-        if (check && acc.w > kPackedMaxCount) *redo_flag = 1u;
-        // The depth plane is read only where the pixel was covered.
-        resolve_pixel(acc, acc.w ? depth[p] : 0u, u, rgba[p], depthf[p]);
+    // Four pixels per thread, a grid-stride apart (each load coalesced over
+    // the warp), with all eight loads issued before any pixel is resolved.
+    const uint32_t stride = gridDim.x * kThreads;
+    for (uint32_t p0 = blockIdx.x * kThreads + threadIdx.x; p0 < npix; p0 += 4u * stride) {
+        uint4 acc[4];
+        uint32_t d[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t p = p0 + (uint32_t)j * stride;
+            acc[j] = p < npix ? accum[p] : make_uint4(0u, 0u, 0u, 0u);
+            d[j] = p < npix ? depth[p] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t p = p0 + (uint32_t)j * stride;
+            if (p >= npix) break;
+            // Packed colour adds are exact while every count is at most
+            // kPackedMaxCount: past it a channel sum may have carried into
+            // its neighbour field, and the frame's colour pass is re-run
+            // exactly.
+            if (check && acc[j].w > kPackedMaxCount) *redo_flag = 1u;
+            // An uncovered pixel's depth is not used.
+            resolve_pixel(acc[j], d[j], u, rgba[p], depthf[p]);
+        }
     }
 }
 
@@ -293,9 +309,12 @@ __global__ void __launch_bounds__(kThreads)
 cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t s, bool check,
                              const uint32_t *redo) {
     const uint32_t npix = (uint32_t)f->width * (uint32_t)f->height;
-    // One pixel per thread; the gated re-run (rarely needed) uses a small
-    // grid-stride grid so that skipping it costs little.
-    const uint32_t grid = redo ? (uint32_t)f->ctx->sm_count * 4 : (npix + kThreads - 1) / kThreads;
+    // A grid-stride grid of eight CTAs per SM at most (four pixels per
+    // thread per step); the gated re-run (rarely needed) uses four per SM so
+    // that skipping it costs little.
+    const uint32_t full = (npix + 4 * kThreads - 1) / (4 * kThreads);
+    const uint32_t grid =
+        redo ? (uint32_t)f->ctx->sm_count * 4 : std::min(full, (uint32_t)f->ctx->sm_count * 8);
     CR_CUDA(launch_programmatic(resolve_hqs, dim3(grid), dim3(kThreads), 0, s,
                                 (const uint32_t *)f->d_depth, (const uint4 *)f->d_accum,
                                 f->d_rgba[0], f->d_depthf, npix, u, f->d_redo, check ? 1 : 0,
