@@ -509,13 +509,13 @@ def run_ours(args, dist):
            "vs_baseline": None, "dtype": "f32+u32",
            "data": "synthetic (seeded fractal heightfield, generated and packed on the GPU)",
            "config": config_dict(args), "e2e": e2e, "roofline": roofline, "clocks": clocks,
-           # HQS: cull (classify, compact), depth, colour, resolve, and the
-           # exact re-run's clear, colour and resolve, which return at once
-           # unless a pixel passed 16,843,009 samples; nearest: cull (2),
-           # nearest pass, resolve.
-           # (+ 2 depth-order flips per frame split by points)
-           "gpu_launches": int(args.steps * ((8 if args.mode == "hqs" else 4) +
-                                             (2 if args.shard == "points" else 0))),
+           # HQS: the cull (whose trailing CTAs clear the frame), depth,
+           # colour, resolve, and the exact re-run, which returns at once
+           # unless a pixel passed 16,843,009 samples.  A frame split by
+           # points has no re-run (its colour adds are unpacked) but two
+           # depth-order flips.  Nearest: cull, nearest pass, resolve.
+           "gpu_launches": int(args.steps * (
+               (6 if args.shard == "points" else 5) if args.mode == "hqs" else 3)),
            "pass_ms": {n: round(float(v), 4) for n, v in zip(PASS_NAMES, avg)},
            "survivor_points_per_frame": int(active.mean()),
            "tuning": ctx.tuning(),
