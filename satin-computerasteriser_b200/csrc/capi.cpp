@@ -129,7 +129,20 @@ cr_status flush_mirror(cr_cloud *c) {
 
 namespace {
 
+static cr_status upload_files_now(cr_cloud *c, const std::vector<cr_raster_file> &files);
+
+// A table the one-view kernels can carry inline is copied to the device only
+// when a consumer of the device copy asks (ensure_device_files).
 cr_status upload_files(cr_cloud *c, const std::vector<cr_raster_file> &files) {
+    if (!files.empty() && files.size() <= kInlineFiles && c->h_files_ring) {
+        c->files_dirty = true;
+        return CR_OK;
+    }
+    c->files_dirty = false;
+    return upload_files_now(c, files);
+}
+
+static cr_status upload_files_now(cr_cloud *c, const std::vector<cr_raster_file> &files) {
     if (files.empty()) return CR_OK;
     if (files.size() > c->d_files_cap) {
         dfree(c->d_files);
@@ -295,6 +308,23 @@ int trunc_i(float x) {
 }
 
 }  // namespace
+
+cr_status ensure_device_files(cr_cloud *c) {
+    if (!c->files_dirty) return CR_OK;
+    c->files_dirty = false;
+    return upload_files_now(c, c->frame_files);
+}
+
+InlineFiles inline_files(const cr_cloud *c) {
+    InlineFiles out;
+    out.n = 0;
+    if (!c->frame_files.empty() && c->frame_files.size() <= kInlineFiles) {
+        out.n = (uint32_t)c->frame_files.size();
+        std::memcpy(out.f, c->frame_files.data(), out.n * sizeof(cr_raster_file));
+    }
+    return out;
+}
+
 
 cr_status validate_config(const cr_config *cfg) {
     if (cfg->mode != CR_MODE_HIGH_QUALITY_AVERAGE && cfg->mode != CR_MODE_NEAREST_POINT)

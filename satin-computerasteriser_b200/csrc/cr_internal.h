@@ -158,7 +158,12 @@ struct cr_cloud {
     UploadState *up = nullptr;  // asynchronous uploads (lazy)
     cr_capacity cap{0, 0};
     std::vector<cr_raster_file> files;        // file table (world matrices)
-    std::vector<cr_raster_file> frame_files;  // last updateFiles snapshot
+    std::vector<cr_raster_file> frame_files;  // last updateFiles snapshot (what the kernels read)
+    // frame_files not yet copied to d_files: a table of at most kInlineFiles
+    // files travels in the one-view kernels' parameters instead, and the
+    // device copy is made only for the consumers that read it
+    // (ensure_device_files).
+    bool files_dirty = false;
     std::vector<cr_raster_batch> mirror;      // host mirror of every slot
     std::vector<int32_t> free_slots;          // LIFO, back() is handed out first
     int64_t dirty_lo = INT64_MAX, dirty_hi = -1;
@@ -286,6 +291,19 @@ cudaError_t launch_programmatic(void (*kernel)(Params...), dim3 grid, dim3 block
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
+
+// File tables of at most this many files ride in the kernel parameters of
+// the one-view passes (read through a __grid_constant__ parameter), so a
+// camera move enqueues no copy between frames.
+constexpr uint32_t kInlineFiles = 4;
+struct InlineFiles {
+    cr_raster_file f[kInlineFiles];
+    uint32_t n;  // 0: read the device table
+};
+// The inline table of a cloud (n = 0 when its table is larger).
+InlineFiles inline_files(const cr_cloud *c);
+// Copies frame_files to d_files if a camera update left it only on the host.
+cr_status ensure_device_files(cr_cloud *c);
 
 // Zeroing of an HQS frame's depth plane (whole 16-byte groups, then a tail
 // of up to three words) and accumulators with the redo word behind them.

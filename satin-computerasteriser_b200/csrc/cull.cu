@@ -64,13 +64,15 @@ __device__ __forceinline__ void screen_rect(const cr_raster_batch &b, const floa
 }
 
 // One slot of cullUpdate (Cull/Shaders.metal:28-82).
-__device__ __forceinline__ bool cull_slot(const CullArgs &a, uint32_t gid, CullRec &out) {
+// files: the cull's file table (a.files, or the one-view launch's inline copy).
+__device__ __forceinline__ bool cull_slot(const CullArgs &a, const cr_raster_file *files,
+                                          uint32_t gid, CullRec &out) {
     const cr_raster_batch b = a.batches[gid];
     if (b.state == 0) return false;  // residency gate (:33-36)
     // A fileIndex past the file table is rejected here (the reference would
     // read past its buffer); the host also refuses such batches on upload.
     if (b.fileIndex >= a.nfiles) return false;
-    const cr_raster_file *file = &a.files[b.fileIndex];
+    const cr_raster_file *file = &files[b.fileIndex];
     if (a.u.enableFrustumCulling != 0) {
         if (!crd::intersects_frustum(file->transformFrustum, crd::f3{b.minX, b.minY, b.minZ},
                                      crd::f3{b.maxX, b.maxY, b.maxZ}))
@@ -136,7 +138,7 @@ __device__ __forceinline__ void classify_body(const CullArgs &a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     CullRec rec;
     bool keep = false;
-    if (gid < a.nbatches) keep = cull_slot(a, gid, rec);
+    if (gid < a.nbatches) keep = cull_slot(a, a.files, gid, rec);
     const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
     const uint32_t ch = __reduce_add_sync(
         0xffffffffu, keep ? nchunks(rec.vb.activePoints, a.chunk_points) : 0u);
@@ -292,7 +294,11 @@ constexpr uint32_t kCullSpinLimit = 1u << 20;
 // kCullSpinLimit times records kErrCullWait and counts that CTA as empty
 // (its writes stay inside the outputs, the frame is wrong).  The last CTA to
 // finish advances the epoch, so the flags never need clearing.
-__global__ void __launch_bounds__(kCullThreads) cull_one_pass(CullArgs a, FrameClear clear) {
+// ifl: the cloud's file table when small (read in place from the
+// __grid_constant__ parameter; n = 0: a.files).
+__global__ void __launch_bounds__(kCullThreads)
+    cull_one_pass(const __grid_constant__ CullArgs a, FrameClear clear,
+                  const __grid_constant__ InlineFiles ifl) {
     crd::grid_wait();          // the previous frame's passes have finished with the planes
     crd::launch_dependents();  // the depth pass waits for this grid itself
     // CTAs past the cull's zero the frame (none wait on them, and they wait
@@ -316,7 +322,7 @@ __global__ void __launch_bounds__(kCullThreads) cull_one_pass(CullArgs a, FrameC
     const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     CullRec rec;
-    const bool keep = gid < a.nbatches && cull_slot(a, gid, rec);
+    const bool keep = gid < a.nbatches && cull_slot(a, ifl.n ? ifl.f : a.files, gid, rec);
     const uint32_t c = keep ? nchunks(rec.vb.activePoints, a.chunk_points) : 0u;
     const uint32_t n = keep ? fragment_span(rec.vb.activePoints, a.chunk_points) : 0u;
     const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
@@ -475,8 +481,13 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s,
                cloud->d_cull_tmp, cloud->d_cull_cta, cp, u, cloud->d_visible, cloud->d_chunks,
                cloud->d_counters, nullptr};
     const uint32_t clear_ctas = clear ? (uint32_t)cloud->ctx->sm_count * 2u : 0u;
+    const InlineFiles ifl = inline_files(cloud);
+    if (!ifl.n) {
+        const cr_status st = ensure_device_files(cloud);
+        if (st) return st;
+    }
     CR_CUDA(launch_programmatic(cull_one_pass, dim3(ctas + clear_ctas), dim3(kCullThreads), 0, s, a,
-                                clear ? *clear : FrameClear{}));
+                                clear ? *clear : FrameClear{}, ifl));
     CR_CUDA(cudaGetLastError());
     return CR_OK;
 }
@@ -518,7 +529,7 @@ __global__ void __launch_bounds__(kCullThreads)
     __shared__ uint32_t warp_counts[kCullThreads / 32];
     const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
     CullRec rec;
-    const bool keep = gid < a.nbatches && cull_slot(a, gid, rec);
+    const bool keep = gid < a.nbatches && cull_slot(a, a.files, gid, rec);
     const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
     if ((threadIdx.x & 31) == 0) warp_counts[threadIdx.x >> 5] = __popc(ballot);
     __syncthreads();
@@ -540,7 +551,7 @@ __global__ void __launch_bounds__(kCullThreads)
     if (lane == 0) part[warp] = s;
     const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
     CullRec rec;
-    const bool keep = gid < a.nbatches && cull_slot(a, gid, rec);
+    const bool keep = gid < a.nbatches && cull_slot(a, a.files, gid, rec);
     const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
     if (lane == 0) warp_counts[warp] = __popc(ballot);
     __syncthreads();

@@ -85,6 +85,7 @@ __host__ __device__ constexpr bool is_color(int p) { return p == PASS_COLOR || p
 struct RasterArgs {
     const ChunkRec *chunks;
     const cr_raster_file *files;
+    InlineFiles ifiles;  // the one-view file table, when small (else ifiles.n = 0)
     uint32_t *counters;
     const uint32_t *low, *med, *high, *colors;
     const uint8_t *levels;
@@ -798,7 +799,9 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
         if (new_file || tiled) {
             __syncthreads();  // everyone has read sb.file (and the view state)
             if (new_file) {
-                const cr_raster_file *file = &a.files[file_id];
+                // The kernels take RasterArgs as a __grid_constant__
+                // parameter, so the inline table is read in place.
+                const cr_raster_file *file = &(a.ifiles.n ? a.ifiles.f : a.files)[file_id];
                 if (threadIdx.x < 16)
                     sb.T[threadIdx.x] = file->transform[threadIdx.x];
                 else if (threadIdx.x < 32)
@@ -1018,7 +1021,7 @@ __device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<
 
 // 1024 slots (about three times a chunk's typical distinct visible pixels)
 // and at most 40 registers: six CTAs share an SM.
-__global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(const __grid_constant__ RasterArgs a) {
     crd::grid_wait();
     crd::launch_dependents();
     if (a.t.redo && *a.t.redo == 0u) return;
@@ -1100,14 +1103,14 @@ __global__ void __launch_bounds__(kThreads) hqs_redo_kernel(RedoArgs r) {
 }
 
 template <int PASS, bool MV>
-__global__ void __launch_bounds__(kThreads) raster_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(kThreads) raster_kernel(const __grid_constant__ RasterArgs a) {
     raster_body<PASS, MV>(a);
 }
 
 // The one-view depth passes fit 64 registers without spilling, so four CTAs
 // (and their 32 KB screen tiles) share an SM.
 template <int PASS>
-__global__ void __launch_bounds__(kThreads, 4) depth_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) depth_kernel(const __grid_constant__ RasterArgs a) {
     raster_body<PASS, false>(a);
 }
 
@@ -1115,13 +1118,13 @@ __global__ void __launch_bounds__(kThreads, 4) depth_kernel(RasterArgs a) {
 // most three CTAs share an SM whatever their registers; saying so lets the
 // compiler use up to 85 registers per thread instead of spilling.
 template <bool MV>
-__global__ void __launch_bounds__(kThreads, 3) raster_kernel_color(RasterArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) raster_kernel_color(const __grid_constant__ RasterArgs a) {
     raster_body<PASS_COLOR, MV>(a);
 }
 
 // Colour pass of batched views with fragments: the fragments when the depth
 // pass could store them all, else the decode-and-project pass.
-__global__ void __launch_bounds__(kThreads, 3) color_views_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) color_views_kernel(const __grid_constant__ RasterArgs a) {
     if (*a.frag_overflow)
         raster_body<PASS_COLOR, true>(a);
     else
@@ -1187,6 +1190,7 @@ RasterArgs make_args(cr_cloud *cloud, const RasterUniforms &u, const RasterTarge
     RasterArgs a;
     a.chunks = cloud->d_chunks;
     a.files = cloud->d_files;
+    a.ifiles = inline_files(cloud);
     a.counters = cloud->d_counters;
     a.low = cloud->d_low;
     a.med = cloud->d_med;
@@ -1312,6 +1316,7 @@ cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUnif
     RasterArgs a = make_args(cloud, u, t);
     a.chunks = chunks;
     a.files = files;
+    a.ifiles.n = 0;  // the views' own tables
     a.counters = counters;
     a.views = views;
     a.nviews = nviews;

@@ -210,6 +210,8 @@ __global__ void __launch_bounds__(kThreads) variant_pass(VariantArgs a) {
 
 cr_status launch_variant_pass(cr_cloud *cloud, bool color, const RasterUniforms &u,
                               const cr_config &cfg, const RasterTargets &t, cudaStream_t s) {
+    // The variant passes read the device file table.
+    if (const cr_status st = ensure_device_files(cloud)) return st;
     VariantArgs a;
     a.chunks = cloud->d_chunks;
     a.counters = cloud->d_counters;
