@@ -496,9 +496,12 @@ __device__ __forceinline__ void do_point(const RasterArgs &a, const ViewRegsT<MV
     o.color = color;
     o.ok = valid;
     if (!all_keep) o.ok = o.ok && keep_point(a, c, o.pointIndex, lvl);
-    if (!__any_sync(kFull, o.ok)) return;
+    // The depth passes keep nearly every point, so a warp vote to skip the
+    // projection or the emission would cost more than it saves (the
+    // emission is correct for a warp with no kept point).
+    if (!is_depth(PASS) && !__any_sync(kFull, o.ok)) return;
     project_point<PASS, MV>(a, vr, sb, c, lo, me, hi, o);
-    if (!__any_sync(kFull, o.ok)) return;
+    if (!is_depth(PASS) && !__any_sync(kFull, o.ok)) return;
     if (!a.radius_zero)
         emit_footprint<PASS, MV>(a, vr, sb, o);
     else if (tiled)
