@@ -979,8 +979,11 @@ __device__ __forceinline__ void hash_clear(uint32_t *hkey, uint32_t *hsum) {
 // The colour pass over chunk k's fragments: sums into the table, then flushes
 // and clears it.  Every thread of the CTA calls this; the caller's barrier
 // before the next chunk orders the clearing before its first add.
+// With a cursor, thread 0 also claims the next chunk into *next during the
+// flush, so the claim's round trip overlaps the flush.
 __device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<false> &vr,
-                                           uint32_t *hkey, uint32_t *hsum, uint32_t k) {
+                                           uint32_t *hkey, uint32_t *hsum, uint32_t k,
+                                           uint32_t *cursor = nullptr, uint32_t *next = nullptr) {
     const int W = a.u.width;
     const uint32_t n = __ldg(a.frag_count + k);
     const uint32_t base = __ldg(&a.chunks[k].first);
@@ -1011,7 +1014,9 @@ __device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<
                 hash_add(hkey, hsum, a, vr, pix, xy, a.frag_col[base + f]);
         }
     }
-    __syncthreads();  // the chunk's sums are complete
+    __syncthreads();  // the chunk's sums are complete (and k has been read by all)
+    uint32_t claimed = 0u;
+    if (cursor && threadIdx.x == 0) claimed = atomicAdd(cursor, 1u);
     for (uint32_t i = threadIdx.x; i < kHashSlots; i += kThreads) {
         const uint32_t pix = hkey[i];
         if (pix == kHashEmpty) continue;
@@ -1020,6 +1025,7 @@ __device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<
         hkey[i] = kHashEmpty;
         hsum[i] = hsum[kHashSlots + i] = hsum[2 * kHashSlots + i] = hsum[3 * kHashSlots + i] = 0u;
     }
+    if (cursor && threadIdx.x == 0) *next = claimed;
 }
 
 // 1024 slots (about three times a chunk's typical distinct visible pixels)
@@ -1034,12 +1040,13 @@ __global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(const __grid_co
     const uint32_t nchunks = a.counters[CNT_CHUNKS];
     const ViewRegsT<false> vr(a);
     hash_clear(hkey, hsum);
+    uint32_t *cursor = a.counters + CNT_WORK_DEPTH;
+    if (threadIdx.x == 0) s_k = atomicAdd(cursor, 1u);
     for (;;) {
-        if (threadIdx.x == 0) s_k = atomicAdd(a.counters + CNT_WORK_DEPTH, 1u);
         __syncthreads();  // s_k and the cleared table
         const uint32_t k = s_k;
         if (k >= nchunks) break;
-        hash_chunk(a, vr, hkey, hsum, k);
+        hash_chunk(a, vr, hkey, hsum, k, cursor, &s_k);  // claims the next chunk into s_k
     }
     if (threadIdx.x == 0) {
         __threadfence();
