@@ -948,8 +948,9 @@ __device__ __forceinline__ uint32_t hash_slot(uint32_t xy) {
     return ((xy & 0xffffu) + 37u * (xy >> 16)) & (kHashSlots - 1u);
 }
 
+template <bool MV>
 __device__ __forceinline__ void hash_add(uint32_t *hkey, uint32_t *hsum, const RasterArgs &a,
-                                         const ViewRegsT<false> &vr, uint32_t pix, uint32_t xy,
+                                         const ViewRegsT<MV> &vr, uint32_t pix, uint32_t xy,
                                          uint32_t col) {
     const uint32_t r = col & 0xffu, g = (col >> 8) & 0xffu, b = (col >> 16) & 0xffu;
     uint32_t h = hash_slot(xy);
@@ -965,7 +966,7 @@ __device__ __forceinline__ void hash_add(uint32_t *hkey, uint32_t *hsum, const R
         }
         h = (h + 1u) & (kHashSlots - 1u);
     }
-    color_global<false>(a, vr, pix, r, g, b, 1u);
+    color_global<MV>(a, vr, pix, r, g, b, 1u);
 }
 
 // Clears the table (at kernel start).
@@ -976,17 +977,12 @@ __device__ __forceinline__ void hash_clear(uint32_t *hkey, uint32_t *hsum) {
     }
 }
 
-// The colour pass over chunk k's fragments: sums into the table, then flushes
-// and clears it.  Every thread of the CTA calls this; the caller's barrier
-// before the next chunk orders the clearing before its first add.
-// With a cursor, thread 0 also claims the next chunk into *next during the
-// flush, so the claim's round trip overlaps the flush.
-__device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<false> &vr,
-                                           uint32_t *hkey, uint32_t *hsum, uint32_t k,
-                                           uint32_t *cursor = nullptr, uint32_t *next = nullptr) {
-    const int W = a.u.width;
-    const uint32_t n = __ldg(a.frag_count + k);
-    const uint32_t base = __ldg(&a.chunks[k].first);
+// The colour pass over one chunk's n fragments starting at base, against
+// the frame of W columns whose depth plane is `depth`: sums into the table.
+template <bool MV>
+__device__ __forceinline__ void hash_frags(const RasterArgs &a, const ViewRegsT<MV> &vr,
+                                           uint32_t *hkey, uint32_t *hsum, uint32_t n,
+                                           uint32_t base, int W, const uint32_t *depth) {
     if ((base & 3u) == 0u) {
         for (uint32_t f = 4u * threadIdx.x; f < n; f += 4u * kThreads) {
             const uint4 xy = __ldcs(reinterpret_cast<const uint4 *>(a.frag_xy + base + f));
@@ -998,34 +994,55 @@ __device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 pix[q] = (xs[q] >> 16) * (uint32_t)W + (xs[q] & 0xffffu);
-                cl[q] = f + q < n ? __ldg(a.t.depth + pix[q]) : 0u;
+                cl[q] = f + q < n ? __ldg(depth + pix[q]) : 0u;
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q)
                 if (cl[q] != 0u && zs[q] >= crd::uint_to_depth(cl[q]) * a.keep_scale)
-                    hash_add(hkey, hsum, a, vr, pix[q], xs[q], cs[q]);
+                    hash_add<MV>(hkey, hsum, a, vr, pix[q], xs[q], cs[q]);
         }
     } else {
         for (uint32_t f = threadIdx.x; f < n; f += kThreads) {
             const uint32_t xy = a.frag_xy[base + f];
             const uint32_t pix = (xy >> 16) * (uint32_t)W + (xy & 0xffffu);
-            const uint32_t cl = __ldg(a.t.depth + pix);
+            const uint32_t cl = __ldg(depth + pix);
             if (cl != 0u && a.frag_z[base + f] >= crd::uint_to_depth(cl) * a.keep_scale)
-                hash_add(hkey, hsum, a, vr, pix, xy, a.frag_col[base + f]);
+                hash_add<MV>(hkey, hsum, a, vr, pix, xy, a.frag_col[base + f]);
         }
     }
-    __syncthreads();  // the chunk's sums are complete (and k has been read by all)
+}
+
+// Flushes the table (one global add pair per distinct pixel) and clears it.
+// With a cursor, thread 0 also claims the next chunk into *next, so the
+// claim's round trip overlaps the flush.  Called after a barrier that
+// completes the sums (and after every thread has read the current claim).
+template <bool MV>
+__device__ __forceinline__ void hash_flush(const RasterArgs &a, const ViewRegsT<MV> &vr,
+                                           uint32_t *hkey, uint32_t *hsum,
+                                           uint32_t *cursor = nullptr, uint32_t *next = nullptr) {
     uint32_t claimed = 0u;
     if (cursor && threadIdx.x == 0) claimed = atomicAdd(cursor, 1u);
     for (uint32_t i = threadIdx.x; i < kHashSlots; i += kThreads) {
         const uint32_t pix = hkey[i];
         if (pix == kHashEmpty) continue;
-        color_global<false>(a, vr, pix, hsum[i], hsum[kHashSlots + i], hsum[2 * kHashSlots + i],
-                            hsum[3 * kHashSlots + i]);
+        color_global<MV>(a, vr, pix, hsum[i], hsum[kHashSlots + i], hsum[2 * kHashSlots + i],
+                         hsum[3 * kHashSlots + i]);
         hkey[i] = kHashEmpty;
         hsum[i] = hsum[kHashSlots + i] = hsum[2 * kHashSlots + i] = hsum[3 * kHashSlots + i] = 0u;
     }
     if (cursor && threadIdx.x == 0) *next = claimed;
+}
+
+// The colour pass over chunk k of one view.  Every thread of the CTA calls
+// this; the caller's barrier before the next chunk orders the clearing
+// before its first add.
+__device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<false> &vr,
+                                           uint32_t *hkey, uint32_t *hsum, uint32_t k,
+                                           uint32_t *cursor = nullptr, uint32_t *next = nullptr) {
+    hash_frags<false>(a, vr, hkey, hsum, __ldg(a.frag_count + k), __ldg(&a.chunks[k].first),
+                      a.u.width, a.t.depth);
+    __syncthreads();  // the chunk's sums are complete (and k has been read by all)
+    hash_flush<false>(a, vr, hkey, hsum, cursor, next);
 }
 
 // 1024 slots (about three times a chunk's typical distinct visible pixels)
@@ -1047,6 +1064,82 @@ __global__ void __launch_bounds__(kThreads, 6) color_hash_kernel(const __grid_co
         const uint32_t k = s_k;
         if (k >= nchunks) break;
         hash_chunk(a, vr, hkey, hsum, k, cursor, &s_k);  // claims the next chunk into s_k
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(a.counters + CNT_DONE, 1u) == gridDim.x - 1u) {
+            a.counters[CNT_WORK_DEPTH] = 0u;
+            a.counters[CNT_DONE] = 0u;
+        }
+    }
+}
+
+// The colour pass of a group of batched views over their fragments: the
+// one-view hash kernel with each chunk's view found by binary search over
+// the per-view chunk prefix (as the point passes do), accumulating into that
+// view's planes.  It returns at once when the group's fragments overflowed
+// the arena; color_views_kernel then decodes the points instead.
+__global__ void __launch_bounds__(kThreads, 6)
+    color_hash_views_kernel(const __grid_constant__ RasterArgs a) {
+    crd::grid_wait();
+    if (*a.frag_overflow) return;
+    __shared__ uint32_t hkey[kHashSlots];
+    __shared__ uint32_t hsum[4 * kHashSlots];
+    __shared__ uint32_t s_vbegin[kMaxViews + 1];
+    __shared__ unsigned long long s_pbegin[kMaxViews + 1];
+    __shared__ uint32_t s_wsum[kThreads / 32];
+    __shared__ unsigned long long s_psum[kThreads / 32];
+    __shared__ uint32_t s_k;
+    // Exclusive prefixes over the views (at most kMaxViews = kThreads) of
+    // their chunk counts and fragment spans.
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const uint32_t *vc = a.counters + threadIdx.x * CNT_COUNT;
+        uint32_t x = threadIdx.x < a.nviews ? vc[CNT_CHUNKS] : 0u;
+        unsigned long long y = threadIdx.x < a.nviews ? vc[CNT_POINTS] : 0ull;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t xs = __shfl_up_sync(kFull, x, o);
+            const unsigned long long ys = __shfl_up_sync(kFull, y, o);
+            if (lane >= o) {
+                x += xs;
+                y += ys;
+            }
+        }
+        if (lane == 31) {
+            s_wsum[warp] = x;
+            s_psum[warp] = y;
+        }
+        __syncthreads();
+        for (int w = 0; w < warp; ++w) {
+            x += s_wsum[w];
+            y += s_psum[w];
+        }
+        s_vbegin[threadIdx.x + 1] = x;
+        s_pbegin[threadIdx.x + 1] = y;
+        if (threadIdx.x == 0) {
+            s_vbegin[0] = 0u;
+            s_pbegin[0] = 0ull;
+        }
+    }
+    hash_clear(hkey, hsum);
+    uint32_t *cursor = a.counters + CNT_WORK_DEPTH;
+    if (threadIdx.x == 0) s_k = atomicAdd(cursor, 1u);
+    __syncthreads();  // prefixes, table and first claim
+    const uint32_t nchunks = s_vbegin[a.nviews];
+    for (;;) {
+        const uint32_t k = s_k;
+        if (k >= nchunks) break;
+        const uint32_t view = find_view(s_vbegin, a.nviews, k);
+        const uint32_t slot = view * a.chunk_stride + (k - s_vbegin[view]);
+        const ViewDesc &vd = a.views[view];
+        const ViewRegsT<true> vr{vd.width, vd.height, vd.depth, vd.accum, vd.nearest};
+        hash_frags<true>(a, vr, hkey, hsum, __ldg(a.frag_count + slot),
+                         (uint32_t)(s_pbegin[view] + __ldg(a.chunk_poff + slot)), vd.width,
+                         vd.depth);
+        __syncthreads();  // the chunk's sums are complete (and k has been read by all)
+        hash_flush<true>(a, vr, hkey, hsum, cursor, &s_k);
+        __syncthreads();  // the next claim and the cleared table
     }
     if (threadIdx.x == 0) {
         __threadfence();
@@ -1132,13 +1225,10 @@ __global__ void __launch_bounds__(kThreads, 3) raster_kernel_color(const __grid_
     raster_body<PASS_COLOR, MV>(a);
 }
 
-// Colour pass of batched views with fragments: the fragments when the depth
-// pass could store them all, else the decode-and-project pass.
+// Colour pass of batched views whose fragments overflowed the arena: the
+// decode-and-project pass (color_hash_views_kernel draws the others).
 __global__ void __launch_bounds__(kThreads, 3) color_views_kernel(const __grid_constant__ RasterArgs a) {
-    if (*a.frag_overflow)
-        raster_body<PASS_COLOR, true>(a);
-    else
-        raster_body<PASS_COLOR_FRAG, true>(a);
+    if (*a.frag_overflow) raster_body<PASS_COLOR, true>(a);
 }
 
 // The kernel a pass launches.
@@ -1313,6 +1403,13 @@ cr_status launch_raster_f32(cr_cloud *cloud, RasterPass pass, const RasterUnifor
 void raster_prepare_views(cr_context *ctx) {
     for (int p : {PASS_DEPTH, PASS_COLOR, PASS_DEPTH_FRAG, PASS_COLOR_FRAG})
         if (ctx->blocks_per_sm_views[p] == 0) ctx->blocks_per_sm_views[p] = raster_blocks_per_sm<true>(p);
+    if (ctx->blocks_per_sm_hash_views == 0) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, color_hash_views_kernel, kThreads, 0) !=
+            cudaSuccess)
+            n = 1;
+        ctx->blocks_per_sm_hash_views = n < 1 ? 1 : n;
+    }
 }
 
 cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUniforms &u,
@@ -1349,9 +1446,13 @@ cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUnif
     case PASS_DEPTH: launch_pass<PASS_DEPTH, true>(a, grid, s); break;
     case PASS_COLOR: launch_pass<PASS_COLOR, true>(a, grid, s); break;
     case PASS_DEPTH_FRAG: launch_pass<PASS_DEPTH_FRAG, true>(a, grid, s); break;
-    default:  // PASS_COLOR_FRAG
+    default: {  // PASS_COLOR_FRAG: fragments, or decode when they overflowed
+        if (ctx->blocks_per_sm_hash_views == 0) raster_prepare_views(ctx);
+        color_hash_views_kernel<<<ctx->sm_count * ctx->blocks_per_sm_hash_views, kThreads, 0, s>>>(
+            a);
         color_views_kernel<<<grid, kThreads, TileCfg<PASS_COLOR>::kBytes, s>>>(a);
         break;
+    }
     }
     CR_CUDA(cudaGetLastError());
     return CR_OK;
