@@ -523,6 +523,9 @@ def run_ours(args, dist):
 
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"], out["parity"] = cpu_baseline(args, cr, ctx, ras, cloud, cams)
+    if dist.world == 1 and args.mode == "hqs" and args.shard == "frames":
+        out["nearest"] = run_nearest(args, cr, ctx, ras, cloud, cams, timed, stream,
+                                     check=not args.no_cpu_baseline)
     for b in pinned:
         b.close()
     if args.mv_views > 0:
@@ -1036,6 +1039,50 @@ def cpu_baseline(args, cr, ctx, ras, cloud, cams):
              "sample": f"{frames} whole frame(s) of the {args.points:,}-point "
                        f"{W}x{H} workload (poses 0..{frames - 1}), single-threaded C++ oracle",
              "seconds": round(cpu_s, 2)}, parity)
+
+
+def run_nearest(args, cr, ctx, ras, cloud, cams, timed, stream, check):
+    """The nearest-point mode on the same cloud and frames: the timed HQS
+    frames' poses drawn again with .nearestPoint (device time, CUDA events
+    around the whole run), and the first frame compared bit for bit with the
+    oracle (RGBA8, nearest depth and index planes)."""
+    import torch
+    hqs = ras.configuration
+    ras.configuration = cr.ComputeRasteriserConfiguration(mode=cr.MODE_NEAREST)
+    try:
+        for p in timed[:3]:
+            ras.update(cams[p])
+            ras.encode()
+        ctx.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for p in timed:
+            ras.update(cams[p])
+            ras.encode()
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1) / len(timed)
+        res = {"value": round(args.points / (ms / 1e3) / 1e9, 4), "unit": "Gpts/s",
+               "ms_per_step": round(ms, 4), "frames": len(timed),
+               "timing": "CUDA events around the run; the HQS run's poses"}
+        if check:
+            import oracle as orc
+            orc.build()
+            p = timed[0]
+            ras.update(cams[p])
+            ras.encode()
+            ref = orc.render(oracle_cloud(orc, cloud), oracle_config(orc, ras.configuration),
+                             cams[p].viewMatrix, cams[p].projectionMatrix, args.width,
+                             args.height, threads=1)
+            res["parity"] = {"pose": int(p),
+                             "rgba8_bit_exact": bool(np.array_equal(ras.outputRGBA8(), ref.rgba)),
+                             "nearest_depth_bit_exact": bool(np.array_equal(ras.nearestDepths(),
+                                                                            ref.nearest_depth)),
+                             "nearest_index_bit_exact": bool(np.array_equal(ras.nearestIndices(),
+                                                                            ref.nearest_index))}
+        return res
+    finally:
+        ras.configuration = hqs
 
 
 # ---------------------------------------------------------------------------
