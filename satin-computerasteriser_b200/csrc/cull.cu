@@ -318,6 +318,8 @@ __global__ void __launch_bounds__(kCullThreads)
     __shared__ uint32_t part_v[kCullThreads / 32], part_c[kCullThreads / 32],
         part_p[kCullThreads / 32];
     __shared__ uint32_t scan_c[kCullThreads / 32], scan_p[kCullThreads / 32];
+    __shared__ CullRec s_rec[kCullThreads];
+    __shared__ uint32_t s_cbase[kCullThreads];
     const uint32_t epoch = *(volatile const uint32_t *)(a.counters + CNT_CULL_EPOCH) + 1u;
     const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -389,29 +391,51 @@ __global__ void __launch_bounds__(kCullThreads)
     }
     // Survivors in slot order, then their chunk records (exclusive scans of
     // the chunk and point counts in slot order, which is survivor order).
-    if (keep) a.visible[off_v + before + __popc(ballot & ((1u << lane) - 1u))] = rec.vb;
-    const uint32_t base = off_c + block_exclusive_scan(c, scan_c);
+    const uint32_t lpos = before + __popc(ballot & ((1u << lane) - 1u));  // survivor in the CTA
+    if (keep) a.visible[off_v + lpos] = rec.vb;
+    // The CTA's chunk records, one record per thread in record order (the
+    // records of a survivor are consecutive): each survivor's values and the
+    // first of its records go to shared memory, and every thread finds the
+    // survivor of its record by binary search.
+    const uint32_t lbase = block_exclusive_scan(c, scan_c);
     const uint32_t pbase = off_p + block_exclusive_scan(n, scan_p);
-    for (uint32_t j = 0; j < c; ++j) {
+    if (keep) {
+        s_rec[lpos] = rec;
+        s_cbase[lpos] = lbase;
+        if (a.chunk_poff)
+            for (uint32_t j = 0; j < c; ++j)
+                a.chunk_poff[off_c + lbase + j] = pbase + j * round4(a.chunk_points);
+    }
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < total_chunks; r += kCullThreads) {
+        uint32_t lo = 0, hi = total;  // survivors' first records ascend (each has one at least)
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_cbase[mid] <= r)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const CullRec &sr = s_rec[lo];
+        const uint32_t j = r - s_cbase[lo];
         ChunkRec k;
-        k.first = rec.first + j * a.chunk_points;
-        k.count = min(a.chunk_points, rec.vb.activePoints - j * a.chunk_points);
-        k.level = rec.vb.level;
-        k.thr = rec.vb.lodThreshold;
-        k.batchIndex = rec.vb.batchIndex;
-        k.file = rec.file;
-        k.minX = rec.minX;
-        k.minY = rec.minY;
-        k.minZ = rec.minZ;
-        k.qx = rec.qx;
-        k.qy = rec.qy;
-        k.qz = rec.qz;
-        k.x0 = rec.x0;
-        k.y0 = rec.y0;
-        k.tw = rec.tw;
-        k.th = rec.th;
-        a.chunks[base + j] = k;
-        if (a.chunk_poff) a.chunk_poff[base + j] = pbase + j * round4(a.chunk_points);
+        k.first = sr.first + j * a.chunk_points;
+        k.count = min(a.chunk_points, sr.vb.activePoints - j * a.chunk_points);
+        k.level = sr.vb.level;
+        k.thr = sr.vb.lodThreshold;
+        k.batchIndex = sr.vb.batchIndex;
+        k.file = sr.file;
+        k.minX = sr.minX;
+        k.minY = sr.minY;
+        k.minZ = sr.minZ;
+        k.qx = sr.qx;
+        k.qy = sr.qy;
+        k.qz = sr.qz;
+        k.x0 = sr.x0;
+        k.y0 = sr.y0;
+        k.tw = sr.tw;
+        k.th = sr.th;
+        a.chunks[off_c + r] = k;
     }
     if (blockIdx.x == cull_ctas - 1 && threadIdx.x == 0) {
         // cullFinalizeUpdate (CullFinalize/Shaders.metal:3-14): {count, 1, 1}.
