@@ -538,7 +538,7 @@ CR_API cr_status cr_context_pass_times(cr_context *ctx, int32_t nframes, float *
  * nearest passes (>= 256); useTiles: accumulate compact batches in
  * shared-memory screen tiles.  Results do not depend on either value. */
 typedef struct cr_tuning {
-    int32_t chunkPoints;     /* default 4096 */
+    int32_t chunkPoints;     /* default 2048 */
     int32_t useTiles;        /* default 1    */
     /* Batched views: the depth and colour passes run over groups of
      * consecutive views of at most this many pixels in all (a view larger

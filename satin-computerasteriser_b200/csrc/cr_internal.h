@@ -90,7 +90,7 @@ struct cr_context {
     int blocks_per_sm[7] = {};        // occupancy of the persistent point passes (per RasterPass)
     int blocks_per_sm_views[7] = {};  // the same, batched-view kernels
     int blocks_per_sm_hash_views = 0;  // the batched-view colour hash kernel
-    int chunk_points = 4096;           // points per chunk work record
+    int chunk_points = 2048;           // points per chunk work record
     int view_group_pixels = 4194304;   // batched views: pixels per depth/colour group
     bool use_tiles = true;             // shared-memory screen tiles
     // Profiling: a ring of frames, each with a start/stop event per pass.

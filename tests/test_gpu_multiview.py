@@ -144,7 +144,7 @@ def test_autotune_sets_and_caches_the_launch_shape(cr, orc, ctx, tmp_path):
         mv.render(cams)
         assert_views_match(cr, ctx, mv, [cloud], mv.configuration, cams, SIZES[:3])
     finally:
-        ctx.set_tuning(chunkPoints=4096, useTiles=True, viewGroupPixels=4194304)
+        ctx.set_tuning(chunkPoints=2048, useTiles=True, viewGroupPixels=4194304)
 
 
 @pytest.mark.parametrize("group_pixels", [1, 40000, 0])

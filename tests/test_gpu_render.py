@@ -291,4 +291,4 @@ def test_tuning_does_not_change_results(cr, orc, ctx, mode, chunk, tiles):
         if mode == 0:
             assert ref.accum[..., 3].max() > 10  # many points per pixel
     finally:
-        ctx.set_tuning(chunkPoints=4096, useTiles=True)
+        ctx.set_tuning(chunkPoints=2048, useTiles=True)
