@@ -469,15 +469,18 @@ def run_ours(args, dist):
     # End to end through the public API: per frame camera upload, render,
     # RGBA8 read-back into pinned host memory.  Pipelined: frame k's image is
     # copied (outputRGBA8Async, two pinned buffers) while frame k+1 renders;
-    # before enqueueing frame k's copy the loop waits for frame k-1's, whose
-    # buffer is then complete, and the clock stops after the last copy.
+    # the host sets the next frame's camera (encode has already captured
+    # frame k's), then waits for frame k-1's copy, whose buffer is then
+    # complete, and enqueues frame k's.  The clock stops after the last copy.
     pinned = [cr.HostBuffer((H, W, 4), np.uint8) for _ in range(2)]
     dist.barrier()
     ctx.synchronize()
     t0 = time.perf_counter()
-    for k, p in enumerate(timed):
-        ras.update(cams[p])
+    ras.update(cams[timed[0]])
+    for k in range(len(timed)):
         frame_encoder.encode()
+        if k + 1 < len(timed):
+            ras.update(cams[timed[k + 1]])
         ras.waitOutput()
         ras.outputRGBA8Async(pinned[k & 1].array)
     ras.waitOutput()
