@@ -309,12 +309,12 @@ __global__ void __launch_bounds__(kThreads)
 cr_status launch_resolve_hqs(cr_frame *f, const ResolveUniforms &u, cudaStream_t s, bool check,
                              const uint32_t *redo) {
     const uint32_t npix = (uint32_t)f->width * (uint32_t)f->height;
-    // A grid-stride grid of eight CTAs per SM at most (four pixels per
-    // thread per step); the gated re-run (rarely needed) uses four per SM so
-    // that skipping it costs little.
+    // A grid-stride grid of sixteen CTAs per SM at most (four pixels per
+    // thread per step: one step covers a 1080p frame); the gated re-run
+    // (rarely needed) uses four per SM so that skipping it costs little.
     const uint32_t full = (npix + 4 * kThreads - 1) / (4 * kThreads);
     const uint32_t grid =
-        redo ? (uint32_t)f->ctx->sm_count * 4 : std::min(full, (uint32_t)f->ctx->sm_count * 8);
+        redo ? (uint32_t)f->ctx->sm_count * 4 : std::min(full, (uint32_t)f->ctx->sm_count * 16);
     CR_CUDA(launch_programmatic(resolve_hqs, dim3(grid), dim3(kThreads), 0, s,
                                 (const uint32_t *)f->d_depth, (const uint4 *)f->d_accum,
                                 f->d_rgba[0], f->d_depthf, npix, u, f->d_redo, check ? 1 : 0,
