@@ -206,7 +206,18 @@ CR_API cr_status cr_config_default(cr_config *out);
 /* ------------------------------------------------------------------------ */
 CR_API cr_status cr_context_create(int device, cr_context **out);
 CR_API cr_status cr_context_destroy(cr_context *ctx);
-/* Wait for all work queued on the context's stream. */
+/* Wait for all work queued on the context's stream.
+ *
+ * Device-side status.  The one-view cull waits, with a bounded number of
+ * polls (cr_tuning.cullSpinLimit), for the survivor counts of the cull CTAs
+ * before it.  A CTA whose wait runs out counts that predecessor as empty, so
+ * the frame's survivor list and image are incomplete, and records the event
+ * in a word of the context.  The next call that synchronises with the
+ * context's work (cr_context_synchronize, the cr_frame_read_* calls,
+ * cr_frame_read_wait, cr_cloud_read_visible, cr_pick) returns
+ * CR_ERR_TIMEOUT, with the detail in cr_last_error_detail, and clears the
+ * word.  The reference's passes report nothing from the GPU (their guards
+ * are silent no-ops, ComputeRasteriser.swift:278-283). */
 CR_API cr_status cr_context_synchronize(cr_context *ctx);
 /* The context's cudaStream_t, as an opaque pointer. */
 CR_API cr_status cr_context_stream(cr_context *ctx, void **stream_out);
@@ -546,6 +557,11 @@ typedef struct cr_tuning {
      * stay in L2 between the two passes; 0 = all views in one group.
      * Default 4194304. */
     int32_t viewGroupPixels;
+    /* Polls of a predecessor's published counts before a cull CTA gives up
+     * (about 0.1 us each; default 1048576).  0 gives up at once: every cull
+     * CTA after the first reports CR_ERR_TIMEOUT (a test of the error path;
+     * nothing waits). */
+    int32_t cullSpinLimit;
 } cr_tuning;
 
 CR_API cr_status cr_context_get_tuning(cr_context *ctx, cr_tuning *out);

@@ -83,6 +83,56 @@ VISIBLE_DTYPE = np.dtype([("batchIndex", "<u4"), ("level", "<i4"), ("lodThreshol
                           ("activePoints", "<u4")])
 
 
+class orc_terrain(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("extent", C.c_float), ("amplitude", C.c_float),
+                ("baseWavelength", C.c_float), ("octaves", C.c_int32), ("lacunarity", C.c_float),
+                ("gain", C.c_float), ("outlierFraction", C.c_float),
+                ("outlierMargin", C.c_float), ("colorNoiseSigma", C.c_float)]
+
+
+@dataclass
+class Terrain:
+    """Parameters of the seeded fractal heightfield (the library's defaults)."""
+    seed: int = 0xC0FFEE02
+    extent: float = 4000.0
+    amplitude: float = 200.0
+    baseWavelength: float = 1500.0
+    octaves: int = 6
+    lacunarity: float = 2.0
+    gain: float = 0.5
+    outlierFraction: float = 0.05
+    outlierMargin: float = 50.0
+    colorNoiseSigma: float = 10.0
+
+    def to_c(self) -> orc_terrain:
+        return orc_terrain(self.seed, self.extent, self.amplitude, self.baseWavelength,
+                           self.octaves, self.lacunarity, self.gain, self.outlierFraction,
+                           self.outlierMargin, self.colorNoiseSigma)
+
+
+def terrain_height(t: Terrain, x: float, y: float) -> float:
+    """Height of the heightfield's noise surface at (x, y)."""
+    return float(_load().orc_terrain_height(C.byref(t.to_c()), x, y))
+
+
+def synth_terrain(t: Terrain, count: int, first: int = 0, threads: int = 1) -> np.ndarray:
+    """(count, 4) float32 records {x, y, z, rgba8 bits} of points [first, first+count),
+    bit-identical to the library's device generator."""
+    out = np.empty((count, 4), np.float32)
+    if _load().orc_synth_terrain(C.byref(t.to_c()), first, count, _ptr(out), threads) != 0:
+        raise ValueError("bad terrain parameters")
+    return out
+
+
+def synth_lattice(n_axis: int, seed: int = 0xC0FFEE01, lo: float = -1.0, hi: float = 1.0,
+                  jitter: float = 0.002, threads: int = 1) -> np.ndarray:
+    """(n^3, 4) float32 records of the jittered lattice, bit-identical to the
+    library's device generator."""
+    out = np.empty((n_axis ** 3, 4), np.float32)
+    _load().orc_synth_lattice(seed, n_axis, lo, hi, jitter, _ptr(out), threads)
+    return out
+
+
 def _load():
     global _lib
     if _lib is not None:
@@ -122,6 +172,20 @@ def _load():
     lib.orc_pack.restype = C.c_int
     lib.orc_pack.argtypes = [P, P, P, C.c_uint64, C.c_uint32, C.c_int, C.c_int, C.c_int,
                              P, P, P, P, P, P, P, P, P]
+    lib.orc_pack_threads.restype = C.c_int
+    lib.orc_pack_threads.argtypes = [P, P, P, C.c_uint64, C.c_uint32, C.c_int, C.c_int, C.c_int,
+                                     P, P, P, P, P, P, P, P, P, C.c_int]
+    lib.orc_terrain_height.restype = C.c_float
+    lib.orc_terrain_height.argtypes = [C.POINTER(orc_terrain), C.c_float, C.c_float]
+    lib.orc_synth_terrain.restype = C.c_int
+    lib.orc_synth_terrain.argtypes = [C.POINTER(orc_terrain), C.c_uint64, C.c_uint64, P, C.c_int]
+    lib.orc_synth_lattice.restype = C.c_int
+    lib.orc_synth_lattice.argtypes = [C.c_uint64, C.c_uint32, C.c_float, C.c_float, C.c_float, P,
+                                      C.c_int]
+    lib.orc_ln_unit.restype = C.c_float
+    lib.orc_ln_unit.argtypes = [C.c_float]
+    lib.orc_cos_2pi.restype = C.c_float
+    lib.orc_cos_2pi.argtypes = [C.c_float]
     _lib = lib
     return lib
 
@@ -287,8 +351,11 @@ class Packed:
 
 
 def pack(positions, colors=None, colors_rgba8=None, pointsPerBatch: int = 10240,
-         lodLevels: int = 4, coarseVoxelDivisions: int = 64, morton_bits: int = 10) -> Packed:
-    """PackedPointCloudFixtures.pack (PackedPointCloudFixtures.swift:30-167)."""
+         lodLevels: int = 4, coarseVoxelDivisions: int = 64, morton_bits: int = 10,
+         threads: int = 1) -> Packed:
+    """PackedPointCloudFixtures.pack (PackedPointCloudFixtures.swift:30-167).
+
+    threads > 1 runs the bit-identical multi-threaded pack (orc_pack_threads)."""
     pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float32).reshape(-1, 3))
     n = len(pos)
     if n == 0:
@@ -309,10 +376,10 @@ def pack(positions, colors=None, colors_rgba8=None, pointsPerBatch: int = 10240,
     src = np.zeros(n, np.uint32)
     opos = np.zeros((n, 3), np.float32)
     bounds = np.zeros(6, np.float32)
-    rc = _load().orc_pack(_ptr(pos), _ptr(cf), _ptr(c8), n, pointsPerBatch, lodLevels,
-                          coarseVoxelDivisions, morton_bits, _ptr(batches), _ptr(low), _ptr(med),
-                          _ptr(high), _ptr(cols), _ptr(levels), _ptr(src), _ptr(opos),
-                          _ptr(bounds))
+    args = (_ptr(pos), _ptr(cf), _ptr(c8), n, pointsPerBatch, lodLevels, coarseVoxelDivisions,
+            morton_bits, _ptr(batches), _ptr(low), _ptr(med), _ptr(high), _ptr(cols),
+            _ptr(levels), _ptr(src), _ptr(opos), _ptr(bounds))
+    rc = _load().orc_pack(*args) if threads <= 1 else _load().orc_pack_threads(*args, threads)
     if rc != 0:
         raise ValueError(f"orc_pack failed ({rc})")
     return Packed(batches, identity_file(), low, med, high, cols, levels, bounds[:3].copy(),

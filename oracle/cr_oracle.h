@@ -155,6 +155,35 @@ int orc_pack(const float *positions, const float *colors_f32, const uint32_t *co
              uint32_t *xyz_high, uint32_t *colors, uint8_t *levels, uint32_t *source_indices,
              float *ordered_positions, float *bounds);
 
+/* The same pack on `threads` host threads, bit-identical to orc_pack: a
+ * stable LSD radix sort (contiguous per-thread ranges, digit-major then
+ * thread-major offsets), the LOD claims as a minimum point index per voxel
+ * in a concurrent table (the first unassigned point of a voxel in sorted
+ * order is its minimum index), and the per-batch steps split by batch.
+ * source_indices, ordered_positions and bounds may be NULL. */
+int orc_pack_threads(const float *positions, const float *colors_f32,
+                     const uint32_t *colors_rgba8, uint64_t n, uint32_t points_per_batch,
+                     int lod_levels, int coarse_voxel_divisions, int morton_bits,
+                     orc_batch *batches, uint32_t *xyz_low, uint32_t *xyz_med, uint32_t *xyz_high,
+                     uint32_t *colors, uint8_t *levels, uint32_t *source_indices,
+                     float *ordered_positions, float *bounds, int threads);
+
+/* Seeded synthetic clouds (host restatement of the library's generators,
+ * bit-identical records {float x, y, z; uint32 rgba8}). */
+typedef struct orc_terrain {
+    uint64_t seed;
+    float extent, amplitude, baseWavelength;
+    int32_t octaves;
+    float lacunarity, gain, outlierFraction, outlierMargin, colorNoiseSigma;
+} orc_terrain;
+float orc_terrain_height(const orc_terrain *t, float x, float y);
+int orc_synth_terrain(const orc_terrain *t, uint64_t first, uint64_t count, float *records,
+                      int threads);
+int orc_synth_lattice(uint64_t seed, uint32_t n_axis, float lo, float hi, float jitter,
+                      float *records, int threads);
+float orc_ln_unit(float u);
+float orc_cos_2pi(float u);
+
 #ifdef __cplusplus
 }
 #endif

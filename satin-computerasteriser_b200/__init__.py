@@ -106,16 +106,21 @@ class Context:
         t = N.cr_tuning()
         N.check(N.lib().cr_context_get_tuning(self._h, C.byref(t)))
         return {"chunkPoints": t.chunkPoints, "useTiles": bool(t.useTiles),
-                "viewGroupPixels": t.viewGroupPixels}
+                "viewGroupPixels": t.viewGroupPixels, "cullSpinLimit": t.cullSpinLimit}
 
     def set_tuning(self, chunkPoints: int | None = None, useTiles: bool | None = None,
-                   viewGroupPixels: int | None = None):
-        """Launch tuning of the point passes (results do not depend on it)."""
+                   viewGroupPixels: int | None = None, cullSpinLimit: int | None = None):
+        """Launch tuning of the point passes (results do not depend on it).
+
+        cullSpinLimit bounds the cull's wait for its predecessors' counts; a
+        wait that runs out makes the next synchronising call raise CRError
+        with CR_ERR_TIMEOUT (0 gives up at once, to exercise that path)."""
         cur = self.tuning()
         t = N.cr_tuning(int(cur["chunkPoints"] if chunkPoints is None else chunkPoints),
                         int(cur["useTiles"] if useTiles is None else useTiles),
                         int(cur["viewGroupPixels"] if viewGroupPixels is None
-                            else viewGroupPixels))
+                            else viewGroupPixels),
+                        int(cur["cullSpinLimit"] if cullSpinLimit is None else cullSpinLimit))
         N.check(N.lib().cr_context_set_tuning(self._h, C.byref(t)))
 
     def set_profiling(self, enable: bool):

@@ -90,7 +90,7 @@ class cr_cloud_arrays(C.Structure):
 
 class cr_tuning(C.Structure):
     _fields_ = [("chunkPoints", C.c_int32), ("useTiles", C.c_int32),
-                ("viewGroupPixels", C.c_int32)]
+                ("viewGroupPixels", C.c_int32), ("cullSpinLimit", C.c_int32)]
 
 
 class cr_cloud_info(C.Structure):

@@ -352,6 +352,20 @@ cr_status reject_variants(const cr_config *cfg, const char *where) {
 // ===========================================================================
 // Exported API
 // ===========================================================================
+cr_status device_status(cr_context *ctx) {
+    volatile uint32_t *w = ctx->h_status;
+    const uint32_t code = w ? *w : 0u;
+    if (code == 0u) return CR_OK;
+    *w = 0u;
+    if (code == kErrCullWait)
+        return fail(CR_ERR_TIMEOUT,
+                    "a cull CTA gave up waiting for the survivor counts of the CTAs before it "
+                    "(cr_tuning.cullSpinLimit = " + std::to_string(ctx->cull_spin_limit) +
+                        " polls); the survivor lists and images of the frames enqueued before "
+                        "this call may be incomplete");
+    return fail(CR_ERR_TIMEOUT, "device-side status " + std::to_string(code));
+}
+
 cr_status frame_copy_fence(cr_frame *f, cudaStream_t s) {
     if (!f->copy_pending) return CR_OK;
     CR_CUDA(cudaStreamWaitEvent(s, f->ev_copied, 0));
@@ -433,6 +447,20 @@ CR_API cr_status cr_context_create(int device, cr_context **out) {
         delete ctx;
         return cri::cuda_fail(e, "cudaStreamCreateWithFlags");
     }
+    // The device-side status word: page-locked host memory mapped into the
+    // device's address space, so a kernel's store needs no copy to be seen.
+    e = cudaHostAlloc(reinterpret_cast<void **>(&ctx->h_status), sizeof(uint32_t),
+                      cudaHostAllocMapped);
+    if (e == cudaSuccess)
+        e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&ctx->d_status), ctx->h_status, 0);
+    if (e != cudaSuccess) {
+        if (ctx->h_status) cudaFreeHost(ctx->h_status);
+        cudaStreamDestroy(ctx->stream);
+        delete ctx->pack;
+        delete ctx;
+        return cri::cuda_fail(e, "cudaHostAlloc (status word)");
+    }
+    *ctx->h_status = 0u;
     *out = ctx;
     return CR_OK;
 }
@@ -456,6 +484,7 @@ CR_API cr_status cr_context_destroy(cr_context *ctx) {
         cudaStreamDestroy(ctx->copy_stream);
     }
     cudaStreamDestroy(ctx->stream);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
     delete ctx;
     return CR_OK;
 }
@@ -465,7 +494,7 @@ CR_API cr_status cr_context_synchronize(cr_context *ctx) {
     DeviceGuard g(ctx->device);
     CR_CUDA(cudaStreamSynchronize(ctx->stream));
     if (ctx->copy_stream) CR_CUDA(cudaStreamSynchronize(ctx->copy_stream));
-    return CR_OK;
+    return device_status(ctx);
 }
 
 CR_API cr_status cr_context_stream(cr_context *ctx, void **stream_out) {
@@ -799,7 +828,7 @@ CR_API cr_status cr_cloud_read_visible(cr_cloud *c, cr_visible_batch *out, uint3
                                 cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
     }
-    return CR_OK;
+    return device_status(c->ctx);
 }
 
 // ---------------------------------------------------------------- frame
@@ -1064,7 +1093,7 @@ static cr_status read_plane(cr_frame *f, void *out, const void *src, size_t byte
     DeviceGuard g(f->ctx->device);
     CR_CUDA(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, f->ctx->stream));
     CR_CUDA(cudaStreamSynchronize(f->ctx->stream));
-    return CR_OK;
+    return device_status(f->ctx);
 }
 
 CR_API cr_status cr_frame_read_rgba8(cr_frame *f, uint8_t *out) {
@@ -1094,7 +1123,7 @@ CR_API cr_status cr_frame_read_wait(cr_frame *f) {
     if (!f->ev_copied) return CR_OK;
     DeviceGuard g(f->ctx->device);
     CR_CUDA(cudaEventSynchronize(f->ev_copied));
-    return CR_OK;
+    return device_status(f->ctx);
 }
 
 CR_API cr_status cr_frame_read_depth_f32(cr_frame *f, float *out) {
@@ -1334,6 +1363,7 @@ CR_API cr_status cr_context_get_tuning(cr_context *ctx, cr_tuning *out) {
     out->chunkPoints = ctx->chunk_points;
     out->useTiles = ctx->use_tiles ? 1 : 0;
     out->viewGroupPixels = ctx->view_group_pixels;
+    out->cullSpinLimit = ctx->cull_spin_limit;
     return CR_OK;
 }
 
@@ -1343,9 +1373,11 @@ CR_API cr_status cr_context_set_tuning(cr_context *ctx, const cr_tuning *t) {
         return fail(CR_ERR_INVALID_ARGUMENT, "chunkPoints must be in [256, 65536]");
     if (t->viewGroupPixels < 0)
         return fail(CR_ERR_INVALID_ARGUMENT, "viewGroupPixels must be >= 0");
+    if (t->cullSpinLimit < 0) return fail(CR_ERR_INVALID_ARGUMENT, "cullSpinLimit must be >= 0");
     ctx->chunk_points = t->chunkPoints;
     ctx->use_tiles = t->useTiles != 0;
     ctx->view_group_pixels = t->viewGroupPixels;
+    ctx->cull_spin_limit = t->cullSpinLimit;
     return CR_OK;
 }
 

@@ -42,6 +42,7 @@ enum CounterSlot : int {
     CNT_DONE = 9,        // CTAs finished with the dynamic cursor (the last one resets both)
     CNT_CULL_EPOCH = 10,  // one-pass cull: launches completed (its CTAs' publish flags are epoch + 1)
     CNT_CULL_DONE = 11,   // one-pass cull: CTAs finished (the last one advances the epoch)
+    CNT_CULL_TICKET = 12, // one-pass cull: next CTA ticket (wraps to 0 after the launch's last)
     CNT_COUNT = 32
 };
 
@@ -93,6 +94,12 @@ struct cr_context {
     int chunk_points = 2048;           // points per chunk work record
     int view_group_pixels = 4194304;   // batched views: pixels per depth/colour group
     bool use_tiles = true;             // shared-memory screen tiles
+    int cull_spin_limit = 1 << 20;     // polls of a predecessor before a cull CTA gives up
+    // Device-side status word (page-locked, mapped into the device's address
+    // space): kernels store an error code into it, and the host reads it
+    // after the calls that synchronise with the context's stream.
+    uint32_t *h_status = nullptr;
+    uint32_t *d_status = nullptr;
     // Profiling: a ring of frames, each with a start/stop event per pass.
     static constexpr int kProfRing = 256;
     bool profiling = false;
@@ -239,6 +246,11 @@ cr_status flush_mirror(cr_cloud *c);
 // asynchronous read-backs; call before the first write of the RGBA8 planes.
 cr_status frame_copy_fence(cr_frame *f, cudaStream_t s);
 
+// The device-side status word of the context, read after a call has
+// synchronised with the context's stream: CR_ERR_TIMEOUT (and the word
+// cleared) when a bounded device-side wait gave up, else CR_OK.
+cr_status device_status(cr_context *ctx);
+
 // ---------------------------------------------------------------------------
 // Kernel launch interfaces
 // ---------------------------------------------------------------------------
@@ -272,6 +284,8 @@ struct CullArgs {
     uint32_t *counters;         // CNT_COUNT words
     uint32_t *chunk_poff;       // per chunk record: offset of its fragments within the
                                 // view's fragment span, a multiple of 4 (NULL: not written)
+    uint32_t spin_limit;        // one-pass cull: polls of a predecessor before giving up
+    uint32_t *status;           // one-pass cull: the context's device-side status word
 };
 
 // Launches a kernel that may begin while the previous kernel on the stream

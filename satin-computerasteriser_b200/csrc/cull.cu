@@ -282,18 +282,21 @@ __device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Polls of a predecessor's flag before a CTA gives up (about 0.1 s).
-constexpr uint32_t kCullSpinLimit = 1u << 20;
-
 // The one-view cull in one pass: every CTA classifies its 256 slots,
 // publishes its survivor, chunk and point counts (flag = this launch's
 // epoch + 1, after a release), sums the counts of the CTAs before it and
-// writes its survivors and chunk records at those offsets.  The CTAs of a
-// launch start in block order and all fit on the GPU at once (a few hundred
-// at most), so every predecessor publishes; a CTA that has polled a flag
-// kCullSpinLimit times records kErrCullWait and counts that CTA as empty
-// (its writes stay inside the outputs, the frame is wrong).  The last CTA to
-// finish advances the epoch, so the flags never need clearing.
+// writes its survivors and chunk records at those offsets.
+//
+// A CTA's slots are chosen by a ticket it claims on arrival (an atomic
+// counter that wraps to zero after the launch's last CTA), not by its block
+// index: the CTAs a CTA waits for hold smaller tickets, so they have already
+// started, and each of them waits only for CTAs that started before it.  The
+// waits therefore end whatever order or number of CTAs the GPU runs at once.
+// A CTA that has polled a flag a.spin_limit times nevertheless gives up,
+// counts that predecessor as empty (its writes stay inside the outputs; the
+// frame is wrong) and stores kErrCullWait into the cloud's error counter and
+// the context's status word, which the host reports as CR_ERR_TIMEOUT.  The
+// last CTA to finish advances the epoch, so the flags never need clearing.
 // ifl: the cloud's file table when small (read in place from the
 // __grid_constant__ parameter; n = 0: a.files).
 __global__ void __launch_bounds__(kCullThreads)
@@ -301,12 +304,16 @@ __global__ void __launch_bounds__(kCullThreads)
                   const __grid_constant__ InlineFiles ifl) {
     crd::grid_wait();          // the previous frame's passes have finished with the planes
     crd::launch_dependents();  // the depth pass waits for this grid itself
-    // CTAs past the cull's zero the frame (none wait on them, and they wait
-    // on nothing), overlapping the cull's latency-bound work.
+    __shared__ uint32_t s_ticket;
+    if (threadIdx.x == 0) s_ticket = atomicInc(a.counters + CNT_CULL_TICKET, gridDim.x - 1u);
+    __syncthreads();
+    const uint32_t ticket = s_ticket;
+    // Tickets past the cull's zero the frame (none wait on them, and they
+    // wait on nothing), overlapping the cull's latency-bound work.
     const uint32_t cull_ctas = (a.nbatches + kCullThreads - 1) / kCullThreads;
-    if (blockIdx.x >= cull_ctas) {
+    if (ticket >= cull_ctas) {
         const size_t stride = (size_t)(gridDim.x - cull_ctas) * kCullThreads;
-        const size_t t0 = (size_t)(blockIdx.x - cull_ctas) * kCullThreads + threadIdx.x;
+        const size_t t0 = (size_t)(ticket - cull_ctas) * kCullThreads + threadIdx.x;
         const uint4 z = make_uint4(0u, 0u, 0u, 0u);
         for (size_t i = t0; i < clear.naccum; i += stride) clear.accum[i] = z;
         for (size_t i = t0; i < clear.ndepth4; i += stride) clear.depth4[i] = z;
@@ -321,7 +328,7 @@ __global__ void __launch_bounds__(kCullThreads)
     __shared__ CullRec s_rec[kCullThreads];
     __shared__ uint32_t s_cbase[kCullThreads];
     const uint32_t epoch = *(volatile const uint32_t *)(a.counters + CNT_CULL_EPOCH) + 1u;
-    const uint32_t gid = blockIdx.x * kCullThreads + threadIdx.x;
+    const uint32_t gid = ticket * kCullThreads + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     CullRec rec;
     const bool keep = gid < a.nbatches && cull_slot(a, ifl.n ? ifl.f : a.files, gid, rec);
@@ -345,7 +352,7 @@ __global__ void __launch_bounds__(kCullThreads)
         total_points += warp_points[w];
     }
     if (threadIdx.x == 0) {
-        uint32_t *mine = a.cta_counts + kCullCtaWords * blockIdx.x;
+        uint32_t *mine = a.cta_counts + kCullCtaWords * ticket;
         mine[0] = total;
         mine[1] = total_chunks;
         mine[2] = total_points;
@@ -354,10 +361,10 @@ __global__ void __launch_bounds__(kCullThreads)
     // Counts of the CTAs before this one, a thread per predecessor.
     uint32_t sv = 0, sc = 0, sp = 0;
     bool gave_up = false;
-    for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kCullThreads) {
+    for (uint32_t i = threadIdx.x; i < ticket; i += kCullThreads) {
         const uint32_t *w = a.cta_counts + kCullCtaWords * i;
         bool published = false;
-        for (uint32_t polls = 0; polls < kCullSpinLimit; ++polls) {
+        for (uint32_t polls = 0; polls < a.spin_limit; ++polls) {
             if (ld_acquire(w + 3) == epoch) {
                 published = true;
                 break;
@@ -372,7 +379,10 @@ __global__ void __launch_bounds__(kCullThreads)
         sc += __ldcg(w + 1);
         sp += __ldcg(w + 2);
     }
-    if (gave_up) atomicCAS(a.counters + CNT_ERROR, 0u, kErrCullWait);
+    if (gave_up) {
+        atomicCAS(a.counters + CNT_ERROR, 0u, kErrCullWait);
+        if (a.status) *(volatile uint32_t *)a.status = kErrCullWait;
+    }
     sv = __reduce_add_sync(0xffffffffu, sv);
     sc = __reduce_add_sync(0xffffffffu, sc);
     sp = __reduce_add_sync(0xffffffffu, sp);
@@ -437,7 +447,7 @@ __global__ void __launch_bounds__(kCullThreads)
         k.th = sr.th;
         a.chunks[off_c + r] = k;
     }
-    if (blockIdx.x == cull_ctas - 1 && threadIdx.x == 0) {
+    if (ticket == cull_ctas - 1 && threadIdx.x == 0) {
         // cullFinalizeUpdate (CullFinalize/Shaders.metal:3-14): {count, 1, 1}.
         uint32_t *counters = a.counters;
         counters[CNT_VISIBLE] = off_v + total;
@@ -501,9 +511,13 @@ cr_status launch_cull(cr_cloud *cloud, const CullUniforms &u, cudaStream_t s,
     }
     const uint32_t cp = (uint32_t)std::max(cloud->ctx->chunk_points, kMinChunkPoints);
     const uint32_t ctas = (n + kCullThreads - 1) / kCullThreads;
-    CullArgs a{cloud->d_batches, n,  cloud->d_files,   (uint32_t)cloud->files.size(),
-               cloud->d_cull_tmp, cloud->d_cull_cta, cp, u, cloud->d_visible, cloud->d_chunks,
-               cloud->d_counters, nullptr};
+    CullArgs a{cloud->d_batches,  n,
+               cloud->d_files,    (uint32_t)cloud->files.size(),
+               cloud->d_cull_tmp, cloud->d_cull_cta,
+               cp,                u,
+               cloud->d_visible,  cloud->d_chunks,
+               cloud->d_counters, nullptr,
+               (uint32_t)std::max(cloud->ctx->cull_spin_limit, 0), cloud->ctx->d_status};
     const uint32_t clear_ctas = clear ? (uint32_t)cloud->ctx->sm_count * 2u : 0u;
     const InlineFiles ifl = inline_files(cloud);
     if (!ifl.n) {

@@ -67,8 +67,14 @@ struct TileCfg<PASS_NEAREST> {
     static constexpr int kBytes = kPx * 8;
 };
 
+// The depth pass that writes fragments keeps two words per tile pixel: the
+// running maximum (seeded with the frame's depth plane) and the plane value
+// it was seeded with, so that the flush writes back only raised pixels.
 template <>
-struct TileCfg<PASS_DEPTH_FRAG> : TileCfg<PASS_DEPTH> {};
+struct TileCfg<PASS_DEPTH_FRAG> {
+    static constexpr int kPx = 4096;
+    static constexpr int kBytes = kPx * 8;
+};
 template <>
 struct TileCfg<PASS_COLOR_FRAG> : TileCfg<PASS_COLOR> {};
 template <>
@@ -216,6 +222,7 @@ struct BatchShared {
 
 struct PointOut {
     bool ok;
+    bool doomed;  // depth pass: the fragment cannot pass the colour pass's depth test
     int ix, iy;  // pixel after the y flip
     uint32_t depth;
     float nz;
@@ -304,6 +311,14 @@ __device__ __forceinline__ void red_max_u32(uint32_t *p, uint32_t v) {
     asm volatile("red.global.max.u32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v)
                  : "memory");
 }
+__device__ __forceinline__ uint32_t atom_max_u32(uint32_t *p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.global.max.u32 %0, [%1], %2;"
+                 : "=r"(old)
+                 : "l"(__cvta_generic_to_global(p)), "r"(v)
+                 : "memory");
+    return old;
+}
 __device__ __forceinline__ void red_max_u64(unsigned long long *p, unsigned long long v) {
     asm volatile("red.global.max.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v)
                  : "memory");
@@ -364,10 +379,17 @@ __device__ __forceinline__ void color_global(const RasterArgs &a, const ViewRegs
 
 // Direct path, radius 0: one global atomic per point (batches large on
 // screen, where points rarely share a pixel).
+#ifndef CR_DIRECT_EARLY_REJECT
+#define CR_DIRECT_EARLY_REJECT 0
+#endif
 template <int PASS, bool MV>
-__device__ __forceinline__ void emit_direct(const RasterArgs &a, const ViewRegsT<MV> &vr, const PointOut &o) {
+__device__ __forceinline__ void emit_direct(const RasterArgs &a, const ViewRegsT<MV> &vr, PointOut &o) {
     const uint32_t pix = (uint32_t)(o.iy * vw<MV>(vr) + o.ix);
-    if (is_depth(PASS)) {
+    if (PASS == PASS_DEPTH_FRAG && CR_DIRECT_EARLY_REJECT) {
+        uint32_t seen = 0u;
+        if (o.ok) seen = atom_max_u32(&vdepth<MV>(vr)[pix], o.depth);
+        o.doomed = o.nz < crd::uint_to_depth(seen) * a.keep_scale;
+    } else if (is_depth(PASS)) {
         if (o.ok) red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
     } else if (is_color(PASS)) {
         const uint32_t closest = o.ok ? vdepth<MV>(vr)[pix] : 0u;
@@ -392,15 +414,29 @@ __device__ __forceinline__ void emit_direct(const RasterArgs &a, const ViewRegsT
 // Tile path, radius 0: shared-memory accumulation, global atomics for points
 // that round outside the rectangle.  Colour tiles hold R | count << 20, G and
 // B per pixel in 32-bit words (exact while a chunk has at most 4095 points).
+//
+// Depth pass with fragments: the tile starts from the frame's depth plane, so
+// the value a point's shared max returns is a lower bound of the pixel's
+// final depth (depths only grow during the pass).  The colour pass keeps a
+// fragment iff z >= uint_to_depth(final) * (1 - tolerance), which is
+// monotone in the depth word for a positive factor (and true for every
+// fragment when the factor is not positive), so a fragment with
+// z < uint_to_depth(running maximum) * (1 - tolerance) fails it with the
+// final depth too and is not written (o.doomed).
 template <int PASS, bool MV>
 __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ViewRegsT<MV> &vr, const ChunkRec &c,
-                                          unsigned char *smem, const PointOut &o) {
+                                          unsigned char *smem, PointOut &o) {
     const int lx = o.ix - c.x0, ly = o.iy - c.y0;
     const bool inside = (unsigned)lx < (unsigned)c.tw && (unsigned)ly < (unsigned)c.th;
     const bool in_tile = o.ok && inside, outside = o.ok && !inside;
     const uint32_t pix = (uint32_t)(o.iy * vw<MV>(vr) + o.ix);
     const int l = inside ? ly * c.tw + lx : 0;
-    if (is_depth(PASS)) {
+    if (PASS == PASS_DEPTH_FRAG) {
+        uint32_t seen = 0u;
+        if (in_tile) seen = atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
+        if (outside) red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
+        o.doomed = o.nz < crd::uint_to_depth(seen) * a.keep_scale;
+    } else if (is_depth(PASS)) {
         if (in_tile) atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
         if (outside) red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
     } else if (is_color(PASS)) {
@@ -471,12 +507,13 @@ __shared__ uint32_t s_frag_count;
 // one shared-memory atomic per warp, lanes placed by ballot rank.
 __device__ __forceinline__ void emit_fragment(const RasterArgs &a, uint32_t fbase,
                                               const PointOut &o) {
-    const uint32_t ballot = __ballot_sync(kFull, o.ok);
+    const bool keep = o.ok && !o.doomed;
+    const uint32_t ballot = __ballot_sync(kFull, keep);
     const int lane = threadIdx.x & 31;
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&s_frag_count, __popc(ballot));
     base = __shfl_sync(kFull, base, 0);
-    if (o.ok) {
+    if (keep) {
         const uint32_t i = fbase + base + __popc(ballot & ((1u << lane) - 1u));
         a.frag_xy[i] = (uint32_t)o.ix | ((uint32_t)o.iy << 16);
         a.frag_z[i] = o.nz;
@@ -495,6 +532,7 @@ __device__ __forceinline__ void do_point(const RasterArgs &a, const ViewRegsT<MV
     o.pointIndex = c.first + local;
     o.color = color;
     o.ok = valid;
+    o.doomed = false;
     if (!all_keep) o.ok = o.ok && keep_point(a, c, o.pointIndex, lvl);
     // The depth passes keep nearly every point, so a warp vote to skip the
     // projection or the emission would cost more than it saves (the
@@ -518,6 +556,7 @@ __device__ __forceinline__ void do_fragment(const RasterArgs &a, const ViewRegsT
                                             uint32_t xy, float nz, uint32_t color) {
     PointOut o;
     o.ok = valid;
+    o.doomed = false;
     o.ix = (int)(xy & 0xffffu);
     o.iy = (int)(xy >> 16);
     o.nz = nz;
@@ -598,7 +637,15 @@ __device__ __forceinline__ void tile_init(const RasterArgs &a, const ChunkRec &c
                                           unsigned char *smem) {
     const int n = c.tw * c.th;
     for (int l = threadIdx.x; l < n; l += kThreads) {
-        if (is_depth(PASS)) {
+        if (PASS == PASS_DEPTH_FRAG) {
+            // Running maximum and seed: the plane's current value (a lower
+            // bound of the final depth; any earlier value of this frame is one).
+            constexpr int kPx = TileCfg<PASS_DEPTH_FRAG>::kPx;
+            const int gx = c.x0 + l % c.tw, gy = c.y0 + l / c.tw;
+            const uint32_t d = view_depth<MV>(a)[gy * view_w<MV>(a) + gx];
+            reinterpret_cast<uint32_t *>(smem)[l] = d;
+            reinterpret_cast<uint32_t *>(smem)[kPx + l] = d;
+        } else if (is_depth(PASS)) {
             reinterpret_cast<uint32_t *>(smem)[l] = 0u;
         } else if (is_color(PASS)) {
             constexpr int kPx = TileCfg<PASS_COLOR>::kPx;
@@ -620,7 +667,12 @@ __device__ __forceinline__ void tile_flush(const RasterArgs &a, const ViewRegsT<
     const int n = c.tw * c.th;
     for (int l = threadIdx.x; l < n; l += kThreads) {
         const uint32_t pix = (uint32_t)((c.y0 + l / c.tw) * vw<MV>(vr) + c.x0 + l % c.tw);
-        if (is_depth(PASS)) {
+        if (PASS == PASS_DEPTH_FRAG) {
+            constexpr int kPx = TileCfg<PASS_DEPTH_FRAG>::kPx;
+            const uint32_t v = reinterpret_cast<const uint32_t *>(smem)[l];
+            if (v > reinterpret_cast<const uint32_t *>(smem)[kPx + l])
+                red_max_u32(&vdepth<MV>(vr)[pix], v);
+        } else if (is_depth(PASS)) {
             const uint32_t v = reinterpret_cast<const uint32_t *>(smem)[l];
             if (v) red_max_u32(&vdepth<MV>(vr)[pix], v);
         } else if (is_color(PASS)) {

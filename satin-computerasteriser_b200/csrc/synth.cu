@@ -5,11 +5,15 @@
 //            lattice hash -> one of eight unit gradients, quintic fade),
 //            summed over octaves with lacunarity 2 and gain 0.5, scaled to
 //            the amplitude; a fraction of the points are uniform volumetric
-//            outliers; colour = height ramp + per-channel normal noise.
+//            outliers; colour = height ramp + per-channel normal noise
+//            (Box-Muller with the project-written ln and cos below).
 //   lattice  an n^3 lattice over [lo, hi]^3 with uniform jitter and uniform
 //            RGB8 (alpha 255), the 1M-point cube workload at n = 100.
 // Both are pure functions of (seed, point index), so any range of points can
 // be generated independently and the cloud is identical for every caller.
+// Every operation is rounded on its own (-fmad=false) and no math-library
+// function is used, so a host restatement with the same operations produces
+// bit-identical records.
 #include <cmath>
 
 #include "cr_internal.h"
@@ -87,6 +91,57 @@ __host__ __device__ __forceinline__ float height_bound(const cr_synth_terrain &t
     return s * t.amplitude;
 }
 
+// Natural log of u in (0, 1] for the colour noise, written for this project
+// so that a host restatement evaluates identical bits: u = m 2^e with m in
+// [sqrt(1/2), sqrt(2)), ln m = 2 atanh(s), s = (m - 1)/(m + 1), by the odd
+// series through s^11 (Abramowitz & Stegun 4.1.27), ln u = e ln 2 + ln m.
+__device__ __forceinline__ float ln_unit(float u) {
+    const uint32_t b = __float_as_uint(u);
+    int e = (int)((b >> 23) & 0xffu) - 127;
+    float m = __uint_as_float((b & 0x007fffffu) | 0x3f800000u);
+    if (m > 1.41421356f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    const float s = (m - 1.0f) / (m + 1.0f);
+    const float s2 = s * s;
+    float p = 0.0909090936f;
+    p = p * s2 + 0.111111112f;
+    p = p * s2 + 0.142857149f;
+    p = p * s2 + 0.200000003f;
+    p = p * s2 + 0.333333343f;
+    p = p * s2 + 1.0f;
+    return (float)e * 0.693147182f + (s * p) * 2.0f;
+}
+
+// cos(2 pi u) for u in [0, 1), written for this project: q = the nearest
+// quarter turn (u - q/4 is exact), then the Taylor series of cos (through
+// r^8) or sin (through r^9) of the remainder r = 2 pi (u - q/4), |r| <= pi/4,
+// with the quadrant's sign.
+__device__ __forceinline__ float cos_2pi(float u) {
+    const float q = floorf(u * 4.0f + 0.5f);
+    const float d = u - q * 0.25f;
+    const float r = d * 6.28318531f;
+    const float r2 = r * r;
+    float c = 2.48015873e-05f;
+    c = c * r2 + -1.38888889e-03f;
+    c = c * r2 + 4.16666667e-02f;
+    c = c * r2 + -0.5f;
+    c = c * r2 + 1.0f;
+    float sn = 2.75573192e-06f;
+    sn = sn * r2 + -1.98412698e-04f;
+    sn = sn * r2 + 8.33333333e-03f;
+    sn = sn * r2 + -1.66666667e-01f;
+    sn = sn * r2 + 1.0f;
+    sn = sn * r;
+    switch ((int)q & 3) {
+    case 0: return c;
+    case 1: return -sn;
+    case 2: return -c;
+    default: return sn;
+    }
+}
+
 __device__ __forceinline__ uint32_t clamp_byte(float v) {
     return (uint32_t)fminf(fmaxf(rintf(v), 0.0f), 255.0f);
 }
@@ -116,7 +171,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = 0; c < 3; ++c) {
         const float u1 = fmaxf(unit(hash3(lo, hi, s ^ (0x5555u + 2u * c))), 1e-7f);
         const float u2 = unit(hash3(lo, hi, s ^ (0x5556u + 2u * c)));
-        const float g = sqrtf(-2.0f * logf(u1)) * cosf(6.28318531f * u2);
+        const float g = sqrtf(-2.0f * ln_unit(u1)) * cos_2pi(u2);
         rgb |= clamp_byte(base[c] + t.colorNoiseSigma * g) << (8 * c);
     }
     out[k] = make_float4(x, y, z, __uint_as_float(rgb | 0xff000000u));

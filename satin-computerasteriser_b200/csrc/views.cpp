@@ -612,7 +612,7 @@ CR_API cr_status cr_autotune_multiview(cr_context *ctx, cr_frame *const *frames,
             ctx->chunk_points = cpn;
             ctx->use_tiles = tiles != 0;
             ctx->view_group_pixels = group;
-            if (best_out) *best_out = cr_tuning{cpn, tiles, group};
+            if (best_out) *best_out = cr_tuning{cpn, tiles, group, ctx->cull_spin_limit};
             if (best_ms_out)
                 *best_ms_out = m == std::string::npos ? 0.0f : (float)std::atof(line.c_str() + m + 6);
             return CR_OK;
@@ -663,7 +663,9 @@ CR_API cr_status cr_autotune_multiview(cr_context *ctx, cr_frame *const *frames,
     ctx->chunk_points = candidates[best][0];
     ctx->use_tiles = candidates[best][1] != 0;
     ctx->view_group_pixels = candidates[best][2];
-    if (best_out) *best_out = cr_tuning{candidates[best][0], candidates[best][1], candidates[best][2]};
+    if (best_out)
+        *best_out = cr_tuning{candidates[best][0], candidates[best][1], candidates[best][2],
+                              ctx->cull_spin_limit};
     if (best_ms_out) *best_ms_out = best_ms;
     if (cache_path) {
         std::ofstream out(cache_path, std::ios::app);

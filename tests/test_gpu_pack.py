@@ -210,3 +210,38 @@ def test_heightfield_63_bit_pack_bit_exact(cr, orc, ctx):
     src = cr.GPUPacker(ctx, mortonBits=21).pack(records=recs, into=cloud, sourceIndices=True)
     recs.close()
     check_region(cloud, ref, 0, ppb, src)
+
+
+def test_device_generators_match_host_restatement(cr, orc, ctx):
+    """The device's seeded generators and the oracle's host restatement give
+    bit-identical records (the benchmark's CPU side builds its clouds with the
+    restatement, without the library)."""
+    params = cr.TerrainParams(seed=0xC0FFEE02)
+    n = 3_000_000
+    dev = cr.synth_terrain(ctx, params, n)
+    got = dev.download()
+    dev.close()
+    want = orc.synth_terrain(orc.Terrain(seed=0xC0FFEE02), n, threads=8)
+    assert got.tobytes() == want.tobytes()
+    for x, y in ((0.0, 0.0), (1234.5, 3210.25), (3999.0, 17.0)):
+        assert np.float32(cr.terrain_height(params, x, y)) == np.float32(
+            orc.terrain_height(orc.Terrain(seed=0xC0FFEE02), x, y))
+    lat = cr.synth_lattice(ctx, 100)
+    got = lat.download()
+    lat.close()
+    assert got.tobytes() == orc.synth_lattice(100, threads=8).tobytes()
+
+
+def test_lattice_1m_pack_bit_exact(cr, orc, ctx):
+    """The 1,000,000-point jittered 100^3 lattice (seed 0xC0FFEE01) packed into
+    10,240-point batches on the GPU equals the CPU pack bit for bit."""
+    recs = cr.synth_lattice(ctx, 100)
+    host = recs.download()
+    ref = orc.pack(np.ascontiguousarray(host[:, :3]), colors_rgba8=host[:, 3].view(np.uint32).copy(),
+                   pointsPerBatch=10240, threads=8)
+    cloud = cr.ComputeRasteriserPointCloud(ctx, cr.ComputeRasteriserCapacity(ref.batchCount, 10240))
+    src = cr.GPUPacker(ctx).pack(records=recs, into=cloud, sourceIndices=True)
+    recs.close()
+    assert ref.batchCount == 98
+    check_region(cloud, ref, 0, 10240, src)
+    cloud.close()

@@ -292,3 +292,30 @@ def test_tuning_does_not_change_results(cr, orc, ctx, mode, chunk, tiles):
             assert ref.accum[..., 3].max() > 10  # many points per pixel
     finally:
         ctx.set_tuning(chunkPoints=2048, useTiles=True)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_lattice_1m_1280x720_bit_exact(cr, orc, ctx, mode):
+    """The small plain configuration at its stated size: 1,000,000 points on the
+    100^3 lattice over [-1, 1]^3 with +-0.002 jitter and uniform RGB8 (the
+    seeded generator, seed 0xC0FFEE01), packed into 10,240-point Morton
+    batches (98 batches), one camera at (0, 0, 3) looking at the origin (fov
+    60, near 0.01, far 100), 1280x720, depth tolerance 1 %.  The depth plane,
+    the R, G, B, count planes, the survivor list, the RGBA8 image and the
+    float depth are compared bit for bit with the oracle (HQS); the nearest
+    depth and index planes in the nearest mode."""
+    recs = orc.synth_lattice(100, seed=0xC0FFEE01, threads=8)
+    packed = orc.pack(np.ascontiguousarray(recs[:, :3]), colors_rgba8=recs[:, 3].view(np.uint32),
+                      pointsPerBatch=10240, threads=8)
+    assert packed.batchCount == 98
+    cloud = cr.ComputeRasteriserPointCloud(ctx, packed=to_product_packed(cr, packed))
+    cfg = cr.ComputeRasteriserConfiguration(mode=mode, depthTolerance=0.01)
+    cam = camera(cr, (0, 0, 3), w=1280, h=720, fov=60.0, near=0.01, far=100.0)
+    ras, gpu, ref = render_both(cr, orc, ctx, [cloud], cfg, cam, 1280, 720)
+    assert_same(cr, cfg, gpu, ref)
+    if mode == 0:
+        assert (ref.accum[..., 3] > 0).sum() > 100_000
+        assert ref.visible[0]["activePoints"].sum() > 100_000
+    else:
+        assert (ref.nearest_index != 0xFFFFFFFF).sum() > 100_000
+    cloud.close()
