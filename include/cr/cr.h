@@ -689,9 +689,12 @@ CR_API cr_status cr_autotune_multiview(cr_context *ctx, cr_frame *const *frames,
  * library's device image, held by every GPU that loads the library until the
  * process exits, so at most 1,048,576 slots are accepted (CR_ERR_CAPACITY
  * above that).  The first call on a device looks up that array's address on
- * the current device; make it before any stream capture.  All calls share the
- * array: calls whose work overlaps on the GPU race.  Asynchronous: the
- * results are valid once the stream has reached them. */
+ * the current device; make it before any stream capture.  The pointers must
+ * belong to the device that is current when the call is made, and the
+ * address is kept for the life of the process, so after a reset of that
+ * device (cudaDeviceReset) this entry point must not be called again.  All
+ * calls share the array: calls whose work overlaps on the GPU race.
+ * Asynchronous: the results are valid once the stream has reached them. */
 CR_API cr_status cr_cull_noalloc(const cr_raster_batch *batches, uint32_t nbatches,
                                  const cr_raster_file *files, uint32_t nfiles,
                                  const cr_config *config, const cr_camera *camera, int width,

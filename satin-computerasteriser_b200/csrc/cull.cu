@@ -578,6 +578,11 @@ __global__ void __launch_bounds__(kCullThreads)
     }
 }
 
+// The write kernel evaluates cull_slot again for its 256 slots instead of
+// reading survivors that the count kernel kept (which would need scratch per
+// slot); cull_slot is a pure function of the inputs, so both kernels agree.
+// Each CTA sums the counts of all CTAs before it: at most kNoAllocMaxCtas
+// (4,096) words, 16 loads per thread, which the slot limit keeps cheap.
 __global__ void __launch_bounds__(kCullThreads)
     cull_noalloc_write(CullArgs a, const uint32_t *cta_counts, cr_visible_batch *out,
                        uint32_t *count_out) {

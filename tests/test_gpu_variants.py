@@ -1,6 +1,8 @@
-"""The colour variants (§8(f)4: displacement, tint, translucent-defocus
-coverage, motion blur) on the GPU against the oracle, bit for bit on every
-plane: RGBA8, depth, R, G, B, count, depth f32.
+"""The colour variants of the reference's colour pass
+(Pipelines/ColorPass/Shaders.metal:106-199: displacement, tint,
+translucent-defocus coverage, motion blur; Resolve/Shaders.metal:27-45) on
+the GPU against the oracle, bit for bit on every plane: RGBA8, depth, R, G,
+B, count, depth f32.
 
 The per-point attributes are written into the cloud's device buffers (here
 with uploads, and through DisplacementPass / TintPass with a torch kernel),
