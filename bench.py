@@ -372,6 +372,16 @@ def ncu_traffic(workload: str, kernel: str):
         return None
 
 
+def ncu_kernel_figures(kernel: str):
+    """Issue and L2-atomic figures of `kernel` from a committed ncu summary
+    (profiles/kernel_figures.json: one small-case capture of that kernel)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "kernel_figures.json")) as f:
+            return json.load(f)[kernel]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def build_cloud(cr, ctx, args, params):
     ppb = 10240
     nb = (args.points + ppb - 1) // ppb
@@ -515,6 +525,16 @@ def run_ours(args, dist):
                 "bytes_per_launch": int(dom_bytes.mean()),
                 "launch_ms": round(float(dom_ms.mean()), 4),
                 "traffic": ncu_traffic(config_dict(args)["workload"], PASS_NAMES[dom])}
+    # The instruction-issue bound and the L2 atomic rate of the same kernel,
+    # from its small-case ncu capture (instructions per survivor point, the
+    # fraction of the SMs' issue slots used, L2 reduction/atomic throughput
+    # as a fraction of its peak).
+    figures = ncu_kernel_figures(kernel)
+    if figures:
+        roofline["issue"] = {k: figures[k] for k in ("inst_per_survivor_point", "issue_frac",
+                                                     "source") if k in figures}
+        if "l2_atomic_frac" in figures:
+            roofline["l2_atomic_frac"] = figures["l2_atomic_frac"]
 
     # End to end through the public API: per frame camera upload, render,
     # RGBA8 read-back into pinned host memory.  Pipelined: frame k's image is
@@ -571,6 +591,7 @@ def run_ours(args, dist):
                (6 if args.shard == "points" else 5) if args.mode == "hqs" else 3)),
            "pass_ms": {n: round(float(v), 4) for n, v in zip(PASS_NAMES, avg)},
            "survivor_points_per_frame": int(active.mean()),
+           "survivors_by_pose": {int(p): int(pose_bytes[p][2]) for p in sorted(pose_bytes)},
            "tuning": ctx.tuning(),
            "pack_s": round(pack_s, 3)}
 
