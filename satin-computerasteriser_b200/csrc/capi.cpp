@@ -363,6 +363,10 @@ cr_status device_status(cr_context *ctx) {
                     "(cr_tuning.cullSpinLimit = " + std::to_string(ctx->cull_spin_limit) +
                         " polls); the survivor lists and images of the frames enqueued before "
                         "this call may be incomplete");
+    if (code == kErrSortWait)
+        return fail(CR_ERR_TIMEOUT,
+                    "a radix sort tile of the packer gave up waiting for the digit counts of "
+                    "the tiles before it; the packed cloud may be wrong");
     return fail(CR_ERR_TIMEOUT, "device-side status " + std::to_string(code));
 }
 

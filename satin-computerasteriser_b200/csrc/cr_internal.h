@@ -268,6 +268,9 @@ struct CullUniforms {
 constexpr uint32_t kCullCtaWords = 4;
 // CNT_ERROR code: a one-pass cull CTA gave up waiting for a predecessor.
 constexpr uint32_t kErrCullWait = 1u;
+// Status code: a radix sort tile of the packer gave up waiting for a
+// predecessor's digit counts.
+constexpr uint32_t kErrSortWait = 2u;
 
 // Arguments of the cull of one view of one cloud (inputs, scratch, outputs).
 struct CullArgs {

@@ -6,11 +6,27 @@
 
 #include "cr/cr.h"
 
+// Grow-only scratch of the radix sort: look-back words (256 per 4096-key
+// tile), the histograms and digit bases of up to 8 passes, one tile ticket
+// counter per pass, and the epoch of the last pass (look-back words carry it).
+struct RadixScratch {
+    unsigned long long *lookback = nullptr;
+    uint64_t cap_tiles = 0;
+    uint32_t *hist = nullptr;
+    uint32_t *bases = nullptr;
+    uint32_t *tiles = nullptr;
+    uint32_t epoch = 0;
+};
+void radix_scratch_free(RadixScratch &r);
+
+// Stable sort of n (key, value) pairs by the low key_bits bits of the keys;
+// the result is in (keys_alt, vals_alt) when *result_in_alt.  Synchronises
+// once (the histograms are read back to skip constant digits).  A bounded
+// wait that gives up stores kErrSortWait into *status.
 template <typename K>
 cr_status radix_sort_pairs(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, uint64_t n,
-                           int key_bits, uint32_t *hist, uint32_t *digit_total, cudaStream_t s,
-                           bool *result_in_alt);
-uint64_t radix_hist_words(uint64_t n);
+                           int key_bits, RadixScratch &rs, uint32_t *status, int sm_count,
+                           cudaStream_t s, bool *result_in_alt);
 
 // Grow-only device scratch of the packer, owned by the context (the
 // reference's PackScratch, GPUPacker.swift:453-484).
@@ -18,7 +34,6 @@ struct PackScratch {
     uint64_t cap_points = 0;
     uint64_t cap_raw_bytes = 0;
     uint64_t cap_grid = 0;
-    uint64_t cap_hist = 0;
     void *raw = nullptr;                    // staged host input
     float4 *pos = nullptr;                  // input x, y, z and RGBA8 bits in w
     void *keys[2] = {nullptr, nullptr};     // Morton keys (u32 or u64), ping-pong
@@ -28,8 +43,7 @@ struct PackScratch {
     uint8_t *lv_out = nullptr;              // levels in final order
     uint32_t *perm = nullptr;               // final order -> Morton position
     uint32_t *grid = nullptr;               // dense LOD occupancy grid
-    uint32_t *hist = nullptr;               // radix histograms
-    uint32_t *digit_total = nullptr;        // 256 digit totals
+    RadixScratch radix;                     // the sort's look-back words and histograms
     uint32_t *bounds = nullptr;             // 6 flipped words: min xyz, max xyz
     uint32_t *src_idx = nullptr;            // final order -> input index
 };

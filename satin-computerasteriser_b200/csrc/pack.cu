@@ -6,7 +6,9 @@
 // PackedPointCloudFixtures.pack (PackedPointCloudFixtures.swift:30-344):
 //   1 bounds        global AABB (order-preserving flipped-bit min/max)
 //   2 morton        10 bits/axis (30-bit key) or 21 bits/axis (63-bit key)
-//   3 sort          stable LSD radix of (key, input index)      [radix.cu]
+//   3 sort          stable LSD radix of (key, input index), one read of the
+//                   keys for every digit's histogram, then one single-sweep
+//                   pass per digit (decoupled look-back)         [radix.cu]
 //   4 gather        positions in Morton order, levels = maxLevel
 //   5 LOD           per level, coarsest first: dense voxel grid, atomicMin
 //                   of the Morton position claims a voxel for the first
@@ -384,7 +386,6 @@ cr_status ensure_points(PackScratch &s, uint64_t n) {
     ALLOC(s.lv_out, (m + 15) & ~15ull);
     ALLOC(s.perm, m * 4);
     ALLOC(s.src_idx, m * 4);
-    ALLOC(s.digit_total, 256 * 4);
     ALLOC(s.bounds, 8 * 4);
 #undef ALLOC
     s.cap_points = n;
@@ -395,10 +396,10 @@ cr_status ensure_points(PackScratch &s, uint64_t n) {
 
 void pack_scratch_free(PackScratch &s) {
     void *ptrs[] = {s.raw, s.pos, s.keys[0], s.keys[1], s.idx[0], s.idx[1], s.sorted,
-                    s.lv_morton, s.lv_out, s.perm, s.grid, s.hist, s.digit_total, s.bounds,
-                    s.src_idx};
+                    s.lv_morton, s.lv_out, s.perm, s.grid, s.bounds, s.src_idx};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    radix_scratch_free(s.radix);
     s = PackScratch{};
 }
 
@@ -474,7 +475,6 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
         ma.bmin[k] = bmin[k];
         ma.scale[k] = ma.top / ext[k];
     }
-    if ((st = grow(&sc.hist, sc.cap_hist, radix_hist_words(count)))) return st;
     bool in_alt = false;
     if (wide) {
         auto *k0 = static_cast<unsigned long long *>(sc.keys[0]);
@@ -482,15 +482,16 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
         pack_morton<unsigned long long><<<grid_for(count), kThreads, 0, s>>>(sc.pos, count, ma, k0,
                                                                              sc.idx[0]);
         CR_CUDA(cudaGetLastError());
-        st = radix_sort_pairs<unsigned long long>(k0, sc.idx[0], k1, sc.idx[1], count, 63, sc.hist,
-                                                  sc.digit_total, s, &in_alt);
+        st = radix_sort_pairs<unsigned long long>(k0, sc.idx[0], k1, sc.idx[1], count, 63,
+                                                  sc.radix, ctx->d_status, ctx->sm_count, s,
+                                                  &in_alt);
     } else {
         auto *k0 = static_cast<uint32_t *>(sc.keys[0]);
         auto *k1 = static_cast<uint32_t *>(sc.keys[1]);
         pack_morton<uint32_t><<<grid_for(count), kThreads, 0, s>>>(sc.pos, count, ma, k0, sc.idx[0]);
         CR_CUDA(cudaGetLastError());
-        st = radix_sort_pairs<uint32_t>(k0, sc.idx[0], k1, sc.idx[1], count, 30, sc.hist,
-                                        sc.digit_total, s, &in_alt);
+        st = radix_sort_pairs<uint32_t>(k0, sc.idx[0], k1, sc.idx[1], count, 30, sc.radix,
+                                        ctx->d_status, ctx->sm_count, s, &in_alt);
     }
     if (st) return st;
     const uint32_t *idx_sorted = sc.idx[in_alt ? 1 : 0];

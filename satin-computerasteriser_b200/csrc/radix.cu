@@ -3,19 +3,31 @@
 // The reference packer (Pipelines/GPUPacker/Shaders.metal:134-215) sorts
 // 30-bit Morton keys with four 8-bit passes, one *thread* per 1024-key tile
 // walking the tile serially so histogram and scatter agree on order.  Here
-// each pass is three kernels over 16384-key partitions, all threads busy:
-//   upsweep  per-partition 256-bin histogram (per-warp sub-histograms in
-//            shared memory), written digit-major;
-//   scan     one CTA per digit turns its row into exclusive partition
-//            offsets and the digit total;
-//   scatter  each partition re-reads its keys in tiles of 4096, ranks them
-//            among equal digits in input order (warp multisplit with
-//            __match_any_sync, then scans over warps and digits), sorts the
-//            tile by digit in shared memory and writes one coalesced run per
-//            digit, so equal keys keep their input order (stable), as the
-//            CPU's stable sort does.
-// 32-bit keys (30-bit Morton) take 4 passes, 64-bit keys (63-bit Morton) 8.
+// the sort reads the keys once for the histograms of every digit, then runs
+// one kernel per 8-bit digit that reads each key and value once and writes
+// them once (a single-sweep pass with decoupled look-back):
+//   radix_histograms  one read of all keys: the 256-bin histogram of every
+//                     digit position; the host reads them back, skips the
+//                     passes whose digit is the same for every key and turns
+//                     the rest into digit bases (exclusive scans);
+//   radix_onesweep    per pass, 4096-key tiles taken in ticket order: a tile
+//                     ranks its keys among equal digits in input order (warp
+//                     multisplit with __match_any_sync, then scans over warps
+//                     and digits), publishes its per-digit counts, sums the
+//                     counts of the tiles before it per digit (look-back over
+//                     their published counts and inclusive prefixes, a
+//                     thread per digit), sorts the tile by digit in shared
+//                     memory and writes one coalesced run per digit.  Equal
+//                     keys keep their input order (stable), as the CPU's
+//                     stable sort does.
+// A tile waits only for tiles with smaller tickets, which started before it,
+// so the waits end whatever the GPU schedules; each wait is nevertheless
+// bounded (kLookbackLimit polls), after which the tile counts the missing
+// predecessor as empty and stores kErrSortWait into the status word, which
+// the host reports as CR_ERR_TIMEOUT.
 #include <algorithm>
+#include <cstring>
+#include <vector>
 
 #include "cr_internal.h"
 #include "cr_pack.h"
@@ -24,216 +36,260 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr uint32_t kPartition = 16384;
-
-template <typename K>
-__global__ void __launch_bounds__(kThreads)
-    radix_upsweep(const K *__restrict__ keys, uint64_t n, int shift, uint32_t *__restrict__ hist,
-                  uint32_t nparts) {
-    __shared__ uint32_t sh[kWarps][256];
-    const int warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < kWarps * 256; i += kThreads) (&sh[0][0])[i] = 0;
-    __syncthreads();
-    const uint64_t base = (uint64_t)blockIdx.x * kPartition;
-    const uint64_t end = (base + kPartition < n) ? base + kPartition : n;
-    for (uint64_t i = base + threadIdx.x; i < end; i += kThreads) {
-        const uint32_t d = (uint32_t)(keys[i] >> shift) & 0xffu;
-        atomicAdd(&sh[warp][d], 1u);
-    }
-    __syncthreads();
-    for (int d = threadIdx.x; d < 256; d += kThreads) {
-        uint32_t s = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) s += sh[w][d];
-        hist[(size_t)d * nparts + blockIdx.x] = s;
-    }
-}
-
-// One CTA per digit: exclusive scan of hist[d][0..nparts) in place, total out.
-__global__ void __launch_bounds__(1024)
-    radix_scan(uint32_t *__restrict__ hist, uint32_t nparts, uint32_t *__restrict__ digit_total) {
-    __shared__ uint32_t warp_sums[32];
-    __shared__ uint32_t carry;
-    uint32_t *row = hist + (size_t)blockIdx.x * nparts;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (uint32_t c0 = 0; c0 < nparts; c0 += 1024) {
-        const uint32_t i = c0 + threadIdx.x;
-        const uint32_t v = i < nparts ? row[i] : 0u;
-        uint32_t x = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) warp_sums[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t s = warp_sums[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-                if (lane >= o) s += y;
-            }
-            warp_sums[lane] = s;  // inclusive over warps
-        }
-        __syncthreads();
-        const uint32_t before = (warp > 0 ? warp_sums[warp - 1] : 0u) + (x - v);
-        if (i < nparts) row[i] = carry + before;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += warp_sums[31];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) digit_total[blockIdx.x] = carry;
-}
-
-// Scatter of one pass, a partition per CTA in tiles of kTileKeys keys:
-//   1. each warp takes 512 consecutive keys, 16 per lane in warp-striped
-//      order (key j*32 + lane), and ranks them among equal digits with
-//      __match_any_sync against running per-warp digit counts, in input
-//      order (j, then lane);
-//   2. per digit, exclusive scans over the warps and then over the digits
-//      give each key its slot in a tile sorted by digit, stable;
-//   3. the keys and values move to that slot in shared memory;
-//   4. threads read the sorted tile in order and write each key to its
-//      digit's running global offset: keys of one digit are consecutive in
-//      shared memory and land at consecutive addresses (coalesced runs).
 constexpr int kKeysPerLane = 16;
-constexpr int kTileKeys = kThreads * kKeysPerLane;
-static_assert(kPartition % kTileKeys == 0, "a partition is whole tiles");
+constexpr int kTileKeys = kThreads * kKeysPerLane;  // 4096
+constexpr uint32_t kLookbackLimit = 1u << 22;
 
+// Look-back word of one (tile, digit): epoch (16 bits) | flag (2 bits) |
+// count (46 bits).  Flag 1: the tile's own count; flag 2: the inclusive count
+// over the tiles up to and including it.
+constexpr unsigned long long kFlagAgg = 1ull, kFlagPrefix = 2ull;
+__device__ __forceinline__ unsigned long long lookback_word(uint32_t epoch, unsigned long long flag,
+                                                            unsigned long long count) {
+    return ((unsigned long long)epoch << 48) | (flag << 46) | count;
+}
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Histograms of every 8-bit digit of the keys (grid-stride, per-CTA shared
+// counts added to global memory once per CTA).
 template <typename K>
-size_t scatter_smem_bytes() {
-    return (size_t)kTileKeys * (sizeof(K) + sizeof(uint32_t)) +
-           ((size_t)kWarps * 256 + 256 + 256) * sizeof(uint32_t);
+__global__ void __launch_bounds__(kThreads)
+    radix_histograms(const K *__restrict__ keys, uint64_t n, int passes,
+                     uint32_t *__restrict__ hist) {
+    __shared__ uint32_t sh[8 * 256];
+    for (int i = threadIdx.x; i < passes * 256; i += kThreads) sh[i] = 0u;
+    __syncthreads();
+    for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * kThreads) {
+        const K k = keys[i];
+        for (int p = 0; p < passes; ++p)
+            atomicAdd(&sh[p * 256 + ((uint32_t)(k >> (8 * p)) & 0xffu)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kThreads)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// Inclusive warp scan.
+__device__ __forceinline__ uint32_t warp_inclusive(uint32_t x, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
 }
 
 template <typename K>
+size_t onesweep_smem_bytes() {
+    return (size_t)kTileKeys * (sizeof(K) + sizeof(uint32_t)) +
+           ((size_t)kWarps * 256 + 256 + 256 + 32) * sizeof(uint32_t);
+}
+
+// One pass: a tile of kTileKeys keys per CTA, in ticket order.
+//   1. each warp takes 512 consecutive keys, 16 per lane in warp-striped order
+//      (key j*32 + lane), and ranks them among equal digits with
+//      __match_any_sync against running per-warp digit counts, in input order;
+//   2. thread d: the tile's count of digit d and the exclusive bases of the
+//      warps; the count is published, the counts of the tiles before it are
+//      summed (look-back), the inclusive prefix is published;
+//   3. exclusive scan over the digits gives each key its slot in a tile
+//      sorted by digit; keys and values move there in shared memory;
+//   4. threads read the sorted tile in order and write each key to its
+//      digit's global offset: keys of one digit are consecutive in shared
+//      memory and land at consecutive addresses (coalesced runs).
+template <typename K>
 __global__ void __launch_bounds__(kThreads)
-    radix_scatter(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
-                  K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, uint64_t n, int shift,
-                  const uint32_t *__restrict__ hist, uint32_t nparts,
-                  const uint32_t *__restrict__ digit_total) {
+    radix_onesweep(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                   K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, uint64_t n,
+                   int shift, const uint32_t *__restrict__ digit_base,
+                   unsigned long long *__restrict__ lookback, uint32_t epoch,
+                   uint32_t *__restrict__ tile_counter, uint32_t *status) {
     extern __shared__ __align__(16) unsigned char smem[];
     K *skey = reinterpret_cast<K *>(smem);
     uint32_t *sval = reinterpret_cast<uint32_t *>(skey + kTileKeys);
-    uint32_t *wcnt = sval + kTileKeys;        // [kWarps][256]
-    uint32_t *offset = wcnt + kWarps * 256;   // running global offset per digit
-    uint32_t *tbase = offset + 256;           // tile-local digit base
+    uint32_t *wcnt = sval + kTileKeys;       // [kWarps][256]: counts, then warp bases
+    uint32_t *offset = wcnt + kWarps * 256;  // global offset of the tile's run of each digit
+    uint32_t *tbase = offset + 256;          // tile-local digit base
+    uint32_t *misc = tbase + 256;            // [0] ticket, [1..8] warp sums of the digit scan
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
-    // Digit bases: exclusive scan of the 256 digit totals, plus this
-    // partition's offset within each digit.
-    {
-        const uint32_t t = digit_total[threadIdx.x];
-        tbase[threadIdx.x] = t;
-        __syncthreads();
-        for (int o = 1; o < 256; o <<= 1) {
-            const uint32_t y = threadIdx.x >= (unsigned)o ? tbase[threadIdx.x - o] : 0u;
-            __syncthreads();
-            tbase[threadIdx.x] += y;
-            __syncthreads();
-        }
-        offset[threadIdx.x] =
-            tbase[threadIdx.x] - t + hist[(size_t)threadIdx.x * nparts + blockIdx.x];
+    if (threadIdx.x == 0) misc[0] = atomicAdd(tile_counter, 1u);
+    for (int i = threadIdx.x; i < kWarps * 256; i += kThreads) wcnt[i] = 0u;
+    __syncthreads();
+    const uint32_t tile = misc[0];
+    const uint64_t tile0 = (uint64_t)tile * kTileKeys;
+    const uint32_t tile_n =
+        (n - tile0 < (uint64_t)kTileKeys) ? (uint32_t)(n - tile0) : (uint32_t)kTileKeys;
+    // 1. Warp-level ranking in input order; a key's rank within its warp
+    //    (< 512) and digit are kept packed, the key and value are read again
+    //    (from L1 / L2) when they move.
+    uint32_t rd[kKeysPerLane];
+    uint32_t *wc = wcnt + warp * 256;
+#pragma unroll
+    for (int j = 0; j < kKeysPerLane; ++j) {
+        const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
+        const bool v = li < tile_n;
+        const K key = v ? keys_in[tile0 + li] : K(0);
+        const uint32_t d = v ? ((uint32_t)(key >> shift) & 0xffu) : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = v ? wc[d] : 0u;
+        rd[j] = (before + __popc(peers & lt)) | (d << 16);
+        __syncwarp();
+        if (v && (peers & lt) == 0u) wc[d] = before + __popc(peers);
+        __syncwarp();
     }
-    const uint64_t pbase = (uint64_t)blockIdx.x * kPartition;
-    for (uint32_t t0 = 0; t0 < kPartition; t0 += kTileKeys) {
-        const uint64_t tile0 = pbase + t0;
-        if (tile0 >= n) break;  // uniform across the CTA
-        const uint32_t tile_n = (n - tile0 < (uint64_t)kTileKeys) ? (uint32_t)(n - tile0)
-                                                                  : (uint32_t)kTileKeys;
-        for (int i = threadIdx.x; i < kWarps * 256; i += kThreads) wcnt[i] = 0u;
-        __syncthreads();
-        // 1. Warp-level ranking in input order; a key's rank within its
-        //    warp (< 512) and digit are kept packed, the key and value are
-        //    read again (from L1 / L2) when they move.
-        uint32_t rd[kKeysPerLane];
-        uint32_t *wc = wcnt + warp * 256;
+    __syncthreads();
+    // 2. Digit d = thread: the tile's count, the warps' exclusive bases, the
+    //    look-back over the tiles before this one.
+    const uint32_t dd = threadIdx.x;
+    uint32_t total = 0;
 #pragma unroll
-        for (int j = 0; j < kKeysPerLane; ++j) {
-            const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
-            const bool v = li < tile_n;
-            const K key = v ? keys_in[tile0 + li] : K(0);
-            const uint32_t d = v ? ((uint32_t)(key >> shift) & 0xffu) : 256u;
-            const uint32_t peers = __match_any_sync(0xffffffffu, d);
-            const uint32_t before = v ? wc[d] : 0u;
-            rd[j] = (before + __popc(peers & lt)) | (d << 16);
-            __syncwarp();
-            if (v && (peers & lt) == 0u) wc[d] = before + __popc(peers);
-            __syncwarp();
-        }
-        __syncthreads();
-        // 2. Per digit: warp bases (exclusive over warps) and tile bases
-        //    (exclusive over digits).
-        const uint32_t dd = threadIdx.x;
-        uint32_t total = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const uint32_t c = wcnt[w * 256 + dd];
-            wcnt[w * 256 + dd] = total;
-            total += c;
-        }
-        tbase[dd] = total;
-        __syncthreads();
-        for (int o = 1; o < 256; o <<= 1) {
-            const uint32_t y = dd >= (unsigned)o ? tbase[dd - o] : 0u;
-            __syncthreads();
-            tbase[dd] += y;
-            __syncthreads();
-        }
-        tbase[dd] -= total;  // inclusive -> exclusive
-        __syncthreads();
-        // 3. Keys and values to their sorted slots in the tile.
-#pragma unroll
-        for (int j = 0; j < kKeysPerLane; ++j) {
-            const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
-            if (li < tile_n) {
-                const uint32_t d = rd[j] >> 16;
-                const uint32_t slot = tbase[d] + wcnt[warp * 256 + d] + (rd[j] & 0xffffu);
-                skey[slot] = keys_in[tile0 + li];
-                sval[slot] = vals_in[tile0 + li];
+    for (int w = 0; w < kWarps; ++w) {
+        const uint32_t c = wcnt[w * 256 + dd];
+        wcnt[w * 256 + dd] = total;
+        total += c;
+    }
+    unsigned long long *my = lookback + (size_t)tile * 256 + dd;
+    unsigned long long excl = 0;
+    if (tile == 0) {
+        st_release64(my, lookback_word(epoch, kFlagPrefix, total));
+    } else {
+        st_release64(my, lookback_word(epoch, kFlagAgg, total));
+        bool gave_up = false;
+        for (int64_t t = (int64_t)tile - 1; t >= 0; --t) {
+            const unsigned long long *w = lookback + (size_t)t * 256 + dd;
+            unsigned long long v = 0;
+            uint32_t polls = 0;
+            for (;;) {
+                v = ld_acquire64(w);
+                if ((uint32_t)(v >> 48) == epoch && ((v >> 46) & 3ull) != 0ull) break;
+                if (++polls >= kLookbackLimit) break;
+                __nanosleep(32);
             }
-        }
-        __syncthreads();
-        // 4. Coalesced runs per digit to the global output.
-        for (uint32_t i = threadIdx.x; i < tile_n; i += kThreads) {
-            const K k = skey[i];
-            const uint32_t d = (uint32_t)(k >> shift) & 0xffu;
-            const uint64_t dst = (uint64_t)offset[d] + (i - tbase[d]);
-            if (dst < n) {  // always true when the histograms are consistent
-                keys_out[dst] = k;
-                vals_out[dst] = sval[i];
+            if (polls >= kLookbackLimit) {
+                gave_up = true;
+                break;
             }
+            excl += v & ((1ull << 46) - 1);
+            if (((v >> 46) & 3ull) == kFlagPrefix) break;
         }
-        __syncthreads();
-        offset[dd] += total;
-        __syncthreads();
+        if (gave_up && status) *(volatile uint32_t *)status = kErrSortWait;
+        st_release64(my, lookback_word(epoch, kFlagPrefix, excl + total));
+    }
+    offset[dd] = digit_base[dd] + (uint32_t)excl;
+    // 3. Exclusive scan of the tile's digit counts (a warp scan per 32
+    //    digits, then over the warps).
+    const uint32_t incl = warp_inclusive(total, lane);
+    if (lane == 31) misc[1 + warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w)
+        if (w < warp) wbase += misc[1 + w];
+    tbase[dd] = wbase + incl - total;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kKeysPerLane; ++j) {
+        const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
+        if (li < tile_n) {
+            const uint32_t d = rd[j] >> 16;
+            const uint32_t slot = tbase[d] + wcnt[warp * 256 + d] + (rd[j] & 0xffffu);
+            skey[slot] = keys_in[tile0 + li];
+            sval[slot] = vals_in[tile0 + li];
+        }
+    }
+    __syncthreads();
+    // 4. Coalesced runs per digit to the global output.
+    for (uint32_t i = threadIdx.x; i < tile_n; i += kThreads) {
+        const K k = skey[i];
+        const uint32_t d = (uint32_t)(k >> shift) & 0xffu;
+        const uint64_t dst = (uint64_t)offset[d] + (i - tbase[d]);
+        if (dst < n) {  // always true when the counts are consistent
+            keys_out[dst] = k;
+            vals_out[dst] = sval[i];
+        }
     }
 }
 
 }  // namespace
 
+void radix_scratch_free(RadixScratch &r) {
+    void *ptrs[] = {r.lookback, r.hist, r.bases, r.tiles};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    r = RadixScratch{};
+}
+
 template <typename K>
 cr_status radix_sort_pairs(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, uint64_t n,
-                           int key_bits, uint32_t *hist, uint32_t *digit_total, cudaStream_t s,
-                           bool *result_in_alt) {
+                           int key_bits, RadixScratch &rs, uint32_t *status, int sm_count,
+                           cudaStream_t s, bool *result_in_alt) {
     *result_in_alt = false;
     if (n <= 1) return CR_OK;
-    const uint32_t nparts = (uint32_t)((n + kPartition - 1) / kPartition);
+    if (n >= (1ull << 32)) return cri::fail(CR_ERR_CAPACITY, "radix sort: at most 2^32 - 1 keys");
+    const int passes = (key_bits + 7) / 8;
+    const uint64_t ntiles = (n + kTileKeys - 1) / kTileKeys;
+    // Scratch: look-back words (tiles x 256), histograms and bases (8 x 256),
+    // tile tickets (one per pass).
+    if (!rs.lookback || rs.cap_tiles < ntiles) {
+        radix_scratch_free(rs);
+        CR_CUDA(cudaMalloc((void **)&rs.lookback, ntiles * 256 * sizeof(unsigned long long)));
+        CR_CUDA(cudaMalloc((void **)&rs.hist, 8 * 256 * sizeof(uint32_t)));
+        CR_CUDA(cudaMalloc((void **)&rs.bases, 8 * 256 * sizeof(uint32_t)));
+        CR_CUDA(cudaMalloc((void **)&rs.tiles, 8 * sizeof(uint32_t)));
+        CR_CUDA(cudaMemsetAsync(rs.lookback, 0, ntiles * 256 * sizeof(unsigned long long), s));
+        rs.cap_tiles = ntiles;
+        rs.epoch = 0;
+    }
+    CR_CUDA(cudaMemsetAsync(rs.hist, 0, 8 * 256 * sizeof(uint32_t), s));
+    CR_CUDA(cudaMemsetAsync(rs.tiles, 0, 8 * sizeof(uint32_t), s));
+    const unsigned hgrid = (unsigned)std::min<uint64_t>((n + kThreads - 1) / kThreads,
+                                                        (uint64_t)std::max(sm_count, 1) * 8);
+    radix_histograms<K><<<hgrid, kThreads, 0, s>>>(keys, n, passes, rs.hist);
+    CR_CUDA(cudaGetLastError());
+    // The histograms on the host: skip the passes whose digit every key
+    // shares, exclusive scans into the digit bases of the others.
+    std::vector<uint32_t> hist(8 * 256), bases(8 * 256, 0u);
+    CR_CUDA(cudaMemcpyAsync(hist.data(), rs.hist, passes * 256 * sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> run;
+    for (int p = 0; p < passes; ++p) {
+        uint32_t acc = 0;
+        bool constant = false;
+        for (int d = 0; d < 256; ++d) {
+            bases[p * 256 + d] = acc;
+            acc += hist[p * 256 + d];
+            if (hist[p * 256 + d] == n) constant = true;
+        }
+        if (!constant) run.push_back(p);
+    }
+    CR_CUDA(cudaMemcpyAsync(rs.bases, bases.data(), passes * 256 * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, s));
+    const size_t smem = onesweep_smem_bytes<K>();
+    CR_CUDA(cudaFuncSetAttribute(radix_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
     K *kin = keys, *kout = keys_alt;
     uint32_t *vin = vals, *vout = vals_alt;
-    for (int shift = 0; shift < key_bits; shift += 8) {
-        radix_upsweep<K><<<nparts, kThreads, 0, s>>>(kin, n, shift, hist, nparts);
-        CR_CUDA(cudaGetLastError());
-        radix_scan<<<256, 1024, 0, s>>>(hist, nparts, digit_total);
-        CR_CUDA(cudaGetLastError());
-        const size_t smem = scatter_smem_bytes<K>();
-        CR_CUDA(cudaFuncSetAttribute(radix_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-        radix_scatter<K><<<nparts, kThreads, smem, s>>>(kin, vin, kout, vout, n, shift, hist, nparts,
-                                                        digit_total);
+    for (int p : run) {
+        // A fresh epoch per pass, so the look-back words never need clearing;
+        // after 65534 epochs the words are cleared once.
+        if (++rs.epoch >= 0xffffu) {
+            CR_CUDA(cudaMemsetAsync(rs.lookback, 0,
+                                    rs.cap_tiles * 256 * sizeof(unsigned long long), s));
+            rs.epoch = 1;
+        }
+        radix_onesweep<K><<<(unsigned)ntiles, kThreads, smem, s>>>(
+            kin, vin, kout, vout, n, 8 * p, rs.bases + p * 256, rs.lookback, rs.epoch,
+            rs.tiles + p, status);
         CR_CUDA(cudaGetLastError());
         std::swap(kin, kout);
         std::swap(vin, vout);
@@ -242,12 +298,10 @@ cr_status radix_sort_pairs(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_
     return CR_OK;
 }
 
-uint64_t radix_hist_words(uint64_t n) { return 256ull * ((n + kPartition - 1) / kPartition); }
-
 template cr_status radix_sort_pairs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *,
-                                              uint64_t, int, uint32_t *, uint32_t *, cudaStream_t,
-                                              bool *);
+                                              uint64_t, int, RadixScratch &, uint32_t *, int,
+                                              cudaStream_t, bool *);
 template cr_status radix_sort_pairs<unsigned long long>(unsigned long long *, uint32_t *,
                                                         unsigned long long *, uint32_t *, uint64_t,
-                                                        int, uint32_t *, uint32_t *, cudaStream_t,
-                                                        bool *);
+                                                        int, RadixScratch &, uint32_t *, int,
+                                                        cudaStream_t, bool *);
