@@ -367,6 +367,10 @@ cr_status device_status(cr_context *ctx) {
         return fail(CR_ERR_TIMEOUT,
                     "a radix sort tile of the packer gave up waiting for the digit counts of "
                     "the tiles before it; the packed cloud may be wrong");
+    if (code == kErrStageWait)
+        return fail(CR_ERR_TIMEOUT,
+                    "a point pass gave up waiting for a bulk copy into shared memory; the "
+                    "frames enqueued before this call may be wrong");
     return fail(CR_ERR_TIMEOUT, "device-side status " + std::to_string(code));
 }
 

@@ -271,6 +271,8 @@ constexpr uint32_t kErrCullWait = 1u;
 // Status code: a radix sort tile of the packer gave up waiting for a
 // predecessor's digit counts.
 constexpr uint32_t kErrSortWait = 2u;
+// Status code: a point pass gave up waiting for a bulk copy into shared memory.
+constexpr uint32_t kErrStageWait = 3u;
 
 // Arguments of the cull of one view of one cloud (inputs, scratch, outputs).
 struct CullArgs {

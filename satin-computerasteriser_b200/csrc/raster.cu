@@ -44,6 +44,10 @@
 #include "cr_internal.h"
 #include "cr_resolve.cuh"
 
+#ifndef CR_PACKED_F32X2
+#define CR_PACKED_F32X2 0
+#endif
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -70,10 +74,17 @@ struct TileCfg<PASS_NEAREST> {
 // The depth pass that writes fragments keeps two words per tile pixel: the
 // running maximum (seeded with the frame's depth plane) and the plane value
 // it was seeded with, so that the flush writes back only raised pixels.
+#ifndef CR_BULK_STAGE
+#define CR_BULK_STAGE 0
+#endif
 template <>
 struct TileCfg<PASS_DEPTH_FRAG> {
     static constexpr int kPx = 4096;
+#if CR_BULK_STAGE
+    static constexpr int kBytes = kPx * 8 + 2 * 2048 * 9;  // + two bulk stage buffers
+#else
     static constexpr int kBytes = kPx * 8;
+#endif
 };
 template <>
 struct TileCfg<PASS_COLOR_FRAG> : TileCfg<PASS_COLOR> {};
@@ -119,6 +130,7 @@ struct RasterArgs {
     const uint32_t *chunk_poff;
     unsigned long long frag_cap;
     uint32_t *frag_overflow;
+    uint32_t *status;  // the context's device-side status word
 };
 
 // The frame and camera of the view whose chunk a CTA is drawing (MV kernels).
@@ -265,18 +277,39 @@ __device__ __forceinline__ void project_point(const RasterArgs &a, const ViewReg
         y = (((lo >> 10) & 1023u) << sl) | (((me >> 10) & 1023u) << sm) | ((hi >> 10) & 1023u);
         z = (((lo >> 20) & 1023u) << sl) | (((me >> 20) & 1023u) << sm) | ((hi >> 20) & 1023u);
     }
+#if CR_PACKED_F32X2 & 2
+    // x and y lanes paired in packed FP32 instructions (identical roundings).
+    const float2 pxy = crd::add2(crd::mul2(make_float2((float)x, (float)y), make_float2(c.qx, c.qy)),
+                                 make_float2(c.minX, c.minY));
+    o.px = pxy.x;
+    o.py = pxy.y;
+    o.pz = (float)z * c.qz + c.minZ;
+#else
     o.px = (float)x * c.qx + c.minX;
     o.py = (float)y * c.qy + c.minY;
     o.pz = (float)z * c.qz + c.minZ;
+#endif
+#if CR_PACKED_F32X2 & 1
+    const crd::f4 clip = crd::mulp2(sb.T, o.px, o.py, o.pz);
+#else
     const crd::f4 clip = crd::mulp(sb.T, o.px, o.py, o.pz);
+#endif
     bool ok = o.ok;
     if (clip.w <= 0.0f) ok = false;
     const float nx = clip.x / clip.w, ny = clip.y / clip.w, nz = clip.z / clip.w;
     if (nx < -1.0f || ny < -1.0f || nx > 1.0f || ny > 1.0f || nz > 1.0f) ok = false;
     if (PASS == PASS_NEAREST ? (nz <= 0.0f) : (nz < 0.0f)) ok = false;
     const int W = vw<MV>(vr), H = vh<MV>(vr);
+#if CR_PACKED_F32X2 & 4
+    const float2 sxy = crd::mul2(crd::add2(crd::mul2(make_float2(nx, ny), make_float2(0.5f, 0.5f)),
+                                           make_float2(0.5f, 0.5f)),
+                                 make_float2((float)W, (float)H));
+    o.ix = (int)sxy.x;
+    const int iy = (int)sxy.y;
+#else
     o.ix = (int)((nx * 0.5f + 0.5f) * (float)W);
     const int iy = (int)((ny * 0.5f + 0.5f) * (float)H);
+#endif
     if (o.ix < 0 || o.ix >= W || iy < 0 || iy >= H) ok = false;
     o.iy = H - 1 - iy;
     o.depth = crd::depth_to_uint(nz);
@@ -292,6 +325,24 @@ __device__ __forceinline__ void project_point(const RasterArgs &a, const ViewReg
 
 __device__ __forceinline__ unsigned long long nearest_key(uint32_t depth, uint32_t index) {
     return ((unsigned long long)depth << 32) | (unsigned long long)(~index);
+}
+
+#ifndef CR_MATCH_MERGE
+#define CR_MATCH_MERGE 0
+#endif
+// Warp pre-merge of 64-bit maxima on the same address: the lanes with
+// `valid` and the same `pix` reduce their keys (high words first, then the
+// low words of the lanes holding the high maximum); returns true on the one
+// lane per group that then updates memory with `k` (the group's maximum).
+__device__ __forceinline__ bool warp_merge_max_u64(bool valid, uint32_t pix,
+                                                   unsigned long long &k) {
+    const unsigned act = __ballot_sync(kFull, valid);
+    if (!valid) return false;
+    const unsigned peers = __match_any_sync(act, pix);
+    const uint32_t hi = __reduce_max_sync(peers, (uint32_t)(k >> 32));
+    const uint32_t lo = __reduce_max_sync(peers, (uint32_t)(k >> 32) == hi ? (uint32_t)k : 0u);
+    k = ((unsigned long long)hi << 32) | lo;
+    return (int)(threadIdx.x & 31) == __ffs(peers) - 1;
 }
 
 // Reductions into the frame planes (global memory).  Written as red.global
@@ -407,7 +458,12 @@ __device__ __forceinline__ void emit_direct(const RasterArgs &a, const ViewRegsT
             grad_store(a, o.pointIndex, g);
         }
     } else {
+#if CR_MATCH_MERGE & 1
+        unsigned long long k = nearest_key(o.depth, o.pointIndex);
+        if (warp_merge_max_u64(o.ok, pix, k)) red_max_u64(&vnearest<MV>(vr)[pix], k);
+#else
         if (o.ok) red_max_u64(&vnearest<MV>(vr)[pix], nearest_key(o.depth, o.pointIndex));
+#endif
     }
 }
 
@@ -432,10 +488,31 @@ __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ViewRegsT<M
     const uint32_t pix = (uint32_t)(o.iy * vw<MV>(vr) + o.ix);
     const int l = inside ? ly * c.tw + lx : 0;
     if (PASS == PASS_DEPTH_FRAG) {
+#if CR_MATCH_MERGE & 2
+        // Lanes on one pixel merge their depths first; every lane of the
+        // group tests its fragment against the group's maximum and what the
+        // tile held before.
+        const unsigned act = __ballot_sync(kFull, o.ok);
+        uint32_t seen = 0u;
+        if (o.ok) {
+            const unsigned peers = __match_any_sync(act, pix);
+            const uint32_t gmax = __reduce_max_sync(peers, o.depth);
+            const int leader = __ffs(peers) - 1;
+            if ((int)(threadIdx.x & 31) == leader) {
+                if (inside)
+                    seen = atomicMax(reinterpret_cast<uint32_t *>(smem) + l, gmax);
+                else
+                    red_max_u32(&vdepth<MV>(vr)[pix], gmax);
+            }
+            seen = max(__shfl_sync(peers, seen, leader), gmax);
+        }
+        o.doomed = o.nz < crd::uint_to_depth(seen) * a.keep_scale;
+#else
         uint32_t seen = 0u;
         if (in_tile) seen = atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
         if (outside) red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
         o.doomed = o.nz < crd::uint_to_depth(seen) * a.keep_scale;
+#endif
     } else if (is_depth(PASS)) {
         if (in_tile) atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
         if (outside) red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
@@ -456,9 +533,15 @@ __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ViewRegsT<M
         }
         if (vis && !inside) color_global<MV>(a, vr, pix, r, g, b, 1u);
     } else {
-        const unsigned long long k = nearest_key(o.depth, o.pointIndex);
+        unsigned long long k = nearest_key(o.depth, o.pointIndex);
+#if CR_MATCH_MERGE & 1
+        const bool lead = warp_merge_max_u64(o.ok, pix, k);
+        if (lead && inside) atomicMax(reinterpret_cast<unsigned long long *>(smem) + l, k);
+        if (lead && !inside) red_max_u64(&vnearest<MV>(vr)[pix], k);
+#else
         if (in_tile) atomicMax(reinterpret_cast<unsigned long long *>(smem) + l, k);
         if (outside) red_max_u64(&vnearest<MV>(vr)[pix], k);
+#endif
     }
 }
 
@@ -706,6 +789,65 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// Bulk staging of a chunk's level bytes, coarse words and colours into shared
+// memory (cp.async.bulk completing on an mbarrier; this GPU's memory only,
+// no multicast).  A chunk is staged when its first point is 16-byte aligned
+// in the level array and it has at most kStagePoints points.
+constexpr uint32_t kStagePoints = 2048;
+constexpr uint32_t kStageBytes = kStagePoints * (1 + 4 + 4);
+constexpr uint32_t kStageWaitLimit = 1u << 20;  // polls of an mbarrier before giving up
+__device__ __forceinline__ bool stage_ok(uint32_t first, uint32_t count) {
+    return (first & 15u) == 0u && count <= kStagePoints && count > 0u;
+}
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// Bounded wait for the mbarrier phase `parity`; false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// Thread 0: the bulk copies of one chunk's level bytes, coarse words and
+// colours into a stage buffer, completing on `bar`.
+__device__ __forceinline__ void stage_issue(unsigned char *stage, uint64_t *bar,
+                                            const uint8_t *levels, const uint32_t *low,
+                                            const uint32_t *colors, uint32_t first,
+                                            uint32_t count) {
+    const uint32_t nl = (count + 15u) & ~15u, nw = ((count + 3u) & ~3u) * 4u;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, nl + 2u * nw);
+    bulk_g2s(stage, levels + first, nl, bar);
+    bulk_g2s(stage + kStagePoints, low + first, nw, bar);
+    bulk_g2s(stage + 5 * kStagePoints, colors + first, nw, bar);
+}
+
 // Largest view v with begin[v] <= k (views without chunks share their
 // begin with the next view, so the view found holds chunk k).
 __device__ __forceinline__ uint32_t find_view(const uint32_t *begin, uint32_t nviews, uint32_t k) {
@@ -790,6 +932,10 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
     // and record and prefetches the record while the CTA draws the current
     // one.
     __shared__ uint32_t s_k[2], s_kview[2], s_kslot[2];  // per record buffer
+    constexpr bool kStage = CR_BULK_STAGE && PASS == PASS_DEPTH_FRAG && !MV;
+    __shared__ __align__(8) uint64_t s_mbar[2];
+    unsigned char *stage_base = smem + TileCfg<PASS>::kPx * 8;
+    uint32_t stage_phase = 0u;  // per buffer: the parity of its next completion
     auto finish = [&]() {
         if (threadIdx.x == 0) {
             __threadfence();
@@ -823,7 +969,18 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                        reinterpret_cast<const uint4 *>(a.chunks + slot) + q);
         if (PASS == PASS_COLOR_FRAG) cp_async4(&rec_frags[b][0], a.frag_count + slot);
         if (MV && kFrag) cp_async4(&rec_frags[b][1], a.chunk_poff + slot);
+        if (kStage) {
+            const uint32_t f = __ldg(&a.chunks[slot].first), n = __ldg(&a.chunks[slot].count);
+            if (stage_ok(f, n))
+                stage_issue(stage_base + b * kStageBytes, &s_mbar[b], a.levels, a.low, a.colors,
+                            f, n);
+        }
     };
+    if (kStage && threadIdx.x == 0) {
+        mbar_init(&s_mbar[0], 1u);
+        mbar_init(&s_mbar[1], 1u);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     if (threadIdx.x == 0) {
         claim(0);
         sb.file = 0xffffffffu;
@@ -923,7 +1080,18 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                 }
             }
         } else if ((c.first & 3u) == 0u) {
-            // Four points per thread, 16-byte loads.
+            // Four points per thread, 16-byte loads (from the bulk-staged
+            // copy in shared memory when the chunk was staged).
+            bool staged = false;
+            const unsigned char *stg = stage_base + buf * kStageBytes;
+            if (kStage && stage_ok(c.first, c.count)) {
+                staged = mbar_wait(&s_mbar[buf], (stage_phase >> buf) & 1u, kStageWaitLimit);
+                if (!staged) {  // give up: record it, wait once more, read global memory
+                    if (a.status) *(volatile uint32_t *)a.status = kErrStageWait;
+                    mbar_wait(&s_mbar[buf], (stage_phase >> buf) & 1u, kStageWaitLimit);
+                }
+                stage_phase ^= 1u << buf;
+            }
             const uint32_t nquads = (c.count + 3u) >> 2;
             for (uint32_t q0 = 0; q0 < nquads; q0 += kThreads) {
                 const uint32_t q = q0 + threadIdx.x;
@@ -931,7 +1099,13 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                 const uint32_t base = c.first + 4u * q;
                 uint32_t lv4 = 0;
                 uint4 lo4 = make_uint4(0, 0, 0, 0), me4 = lo4, hi4 = lo4, co4 = lo4;
-                if (qv) {
+                if (qv && staged) {
+                    lv4 = reinterpret_cast<const uint32_t *>(stg)[q];
+                    lo4 = reinterpret_cast<const uint4 *>(stg + kStagePoints)[q];
+                    co4 = reinterpret_cast<const uint4 *>(stg + 5 * kStagePoints)[q];
+                    if (need_med) me4 = __ldg(reinterpret_cast<const uint4 *>(a.med + base));
+                    if (need_high) hi4 = __ldg(reinterpret_cast<const uint4 *>(a.high + base));
+                } else if (qv) {
                     lv4 = __ldg(reinterpret_cast<const uint32_t *>(a.levels + base));
                     lo4 = __ldg(reinterpret_cast<const uint4 *>(a.low + base));
                     if (need_med) me4 = __ldg(reinterpret_cast<const uint4 *>(a.med + base));
@@ -1001,10 +1175,9 @@ __device__ __forceinline__ uint32_t hash_slot(uint32_t xy) {
 }
 
 template <bool MV>
-__device__ __forceinline__ void hash_add(uint32_t *hkey, uint32_t *hsum, const RasterArgs &a,
-                                         const ViewRegsT<MV> &vr, uint32_t pix, uint32_t xy,
-                                         uint32_t col) {
-    const uint32_t r = col & 0xffu, g = (col >> 8) & 0xffu, b = (col >> 16) & 0xffu;
+__device__ __forceinline__ void hash_add_sums(uint32_t *hkey, uint32_t *hsum, const RasterArgs &a,
+                                              const ViewRegsT<MV> &vr, uint32_t pix, uint32_t xy,
+                                              uint32_t r, uint32_t g, uint32_t b, uint32_t n) {
     uint32_t h = hash_slot(xy);
     for (int probe = 0; probe < kHashProbes; ++probe) {
         uint32_t cur = hkey[h];
@@ -1013,12 +1186,20 @@ __device__ __forceinline__ void hash_add(uint32_t *hkey, uint32_t *hsum, const R
             atomicAdd(hsum + h, r);
             atomicAdd(hsum + kHashSlots + h, g);
             atomicAdd(hsum + 2 * kHashSlots + h, b);
-            atomicAdd(hsum + 3 * kHashSlots + h, 1u);
+            atomicAdd(hsum + 3 * kHashSlots + h, n);
             return;
         }
         h = (h + 1u) & (kHashSlots - 1u);
     }
-    color_global<MV>(a, vr, pix, r, g, b, 1u);
+    color_global<MV>(a, vr, pix, r, g, b, n);
+}
+
+template <bool MV>
+__device__ __forceinline__ void hash_add(uint32_t *hkey, uint32_t *hsum, const RasterArgs &a,
+                                         const ViewRegsT<MV> &vr, uint32_t pix, uint32_t xy,
+                                         uint32_t col) {
+    hash_add_sums<MV>(hkey, hsum, a, vr, pix, xy, col & 0xffu, (col >> 8) & 0xffu,
+                      (col >> 16) & 0xffu, 1u);
 }
 
 // Clears the table (at kernel start).
@@ -1048,10 +1229,28 @@ __device__ __forceinline__ void hash_frags(const RasterArgs &a, const ViewRegsT<
                 pix[q] = (xs[q] >> 16) * (uint32_t)W + (xs[q] & 0xffffu);
                 cl[q] = f + q < n ? __ldg(depth + pix[q]) : 0u;
             }
+#if CR_MATCH_MERGE & 4
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                // Lanes with the same visible pixel sum their colours first.
+                const bool vis = cl[q] != 0u && zs[q] >= crd::uint_to_depth(cl[q]) * a.keep_scale;
+                const unsigned act = __ballot_sync(kFull, vis);
+                if (vis) {
+                    const unsigned peers = __match_any_sync(act, pix[q]);
+                    const uint32_t r = __reduce_add_sync(peers, cs[q] & 0xffu);
+                    const uint32_t g = __reduce_add_sync(peers, (cs[q] >> 8) & 0xffu);
+                    const uint32_t b = __reduce_add_sync(peers, (cs[q] >> 16) & 0xffu);
+                    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1)
+                        hash_add_sums<MV>(hkey, hsum, a, vr, pix[q], xs[q], r, g, b,
+                                          (uint32_t)__popc(peers));
+                }
+            }
+#else
 #pragma unroll
             for (int q = 0; q < 4; ++q)
                 if (cl[q] != 0u && zs[q] >= crd::uint_to_depth(cl[q]) * a.keep_scale)
                     hash_add<MV>(hkey, hsum, a, vr, pix[q], xs[q], cs[q]);
+#endif
         }
     } else {
         for (uint32_t f = threadIdx.x; f < n; f += kThreads) {
@@ -1264,8 +1463,11 @@ __global__ void __launch_bounds__(kThreads) raster_kernel(const __grid_constant_
 
 // The one-view depth passes fit 64 registers without spilling, so four CTAs
 // (and their 32 KB screen tiles) share an SM.
+#ifndef CR_DEPTH_MIN_BLOCKS
+#define CR_DEPTH_MIN_BLOCKS 4
+#endif
 template <int PASS>
-__global__ void __launch_bounds__(kThreads, 4) depth_kernel(const __grid_constant__ RasterArgs a) {
+__global__ void __launch_bounds__(kThreads, CR_DEPTH_MIN_BLOCKS) depth_kernel(const __grid_constant__ RasterArgs a) {
     raster_body<PASS, false>(a);
 }
 
@@ -1370,6 +1572,7 @@ RasterArgs make_args(cr_cloud *cloud, const RasterUniforms &u, const RasterTarge
     a.fcolors = nullptr;
     a.dldimg = nullptr;
     a.fgrad = nullptr;
+    a.status = cloud->ctx->d_status;
     return a;
 }
 
