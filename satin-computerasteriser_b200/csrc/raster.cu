@@ -47,6 +47,9 @@
 #ifndef CR_PACKED_F32X2
 #define CR_PACKED_F32X2 0
 #endif
+#ifndef CR_TILE_REJECT
+#define CR_TILE_REJECT 1
+#endif
 
 namespace {
 
@@ -487,7 +490,7 @@ __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ViewRegsT<M
     const bool in_tile = o.ok && inside, outside = o.ok && !inside;
     const uint32_t pix = (uint32_t)(o.iy * vw<MV>(vr) + o.ix);
     const int l = inside ? ly * c.tw + lx : 0;
-    if (PASS == PASS_DEPTH_FRAG) {
+    if (PASS == PASS_DEPTH_FRAG && CR_TILE_REJECT) {
 #if CR_MATCH_MERGE & 2
         // Lanes on one pixel merge their depths first; every lane of the
         // group tests its fragment against the group's maximum and what the
@@ -720,7 +723,7 @@ __device__ __forceinline__ void tile_init(const RasterArgs &a, const ChunkRec &c
                                           unsigned char *smem) {
     const int n = c.tw * c.th;
     for (int l = threadIdx.x; l < n; l += kThreads) {
-        if (PASS == PASS_DEPTH_FRAG) {
+        if (PASS == PASS_DEPTH_FRAG && CR_TILE_REJECT) {
             // Running maximum and seed: the plane's current value (a lower
             // bound of the final depth; any earlier value of this frame is one).
             constexpr int kPx = TileCfg<PASS_DEPTH_FRAG>::kPx;
@@ -750,7 +753,7 @@ __device__ __forceinline__ void tile_flush(const RasterArgs &a, const ViewRegsT<
     const int n = c.tw * c.th;
     for (int l = threadIdx.x; l < n; l += kThreads) {
         const uint32_t pix = (uint32_t)((c.y0 + l / c.tw) * vw<MV>(vr) + c.x0 + l % c.tw);
-        if (PASS == PASS_DEPTH_FRAG) {
+        if (PASS == PASS_DEPTH_FRAG && CR_TILE_REJECT) {
             constexpr int kPx = TileCfg<PASS_DEPTH_FRAG>::kPx;
             const uint32_t v = reinterpret_cast<const uint32_t *>(smem)[l];
             if (v > reinterpret_cast<const uint32_t *>(smem)[kPx + l])
