@@ -91,6 +91,36 @@ __device__ __forceinline__ f4 mulp2(const float *m, float x, float y, float z) {
     return f4{a.x, a.y, b.x, b.y};
 }
 
+// Three IEEE single-precision quotients a/w, b/w, c/w that share one
+// reciprocal, computed in double precision: r ~ 1/w from the single-precision
+// reciprocal approximation refined by two Newton-Raphson steps in double
+// (relative error below 2^-51), then q = RN32(RN64(a * r)).  The exact
+// quotient of two floats lies at least 2^-49 |q| away from every midpoint
+// between neighbouring floats (a * 2^k - m * w is a nonzero multiple of the
+// unit of m * w for a midpoint m), while RN64(a * r) is within 2^-50 |q| of
+// it, so rounding it to single precision gives the correctly rounded
+// quotient, the same bits as a / w.  Outside |w| in [2^-125, 2^125] (and for
+// NaN or infinite w) the plain divisions are used.
+__device__ __forceinline__ void div3_shared(float a, float b, float c, float w, float &qa,
+                                            float &qb, float &qc) {
+    const float aw = fabsf(w);
+    if (!(aw >= 2.3509887e-38f && aw <= 4.2535296e37f)) {
+        qa = a / w;
+        qb = b / w;
+        qc = c / w;
+        return;
+    }
+    float r0;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(w));
+    const double wd = (double)w;
+    double r = (double)r0;
+    r = __fma_rn(r, __fma_rn(-wd, r, 1.0), r);
+    r = __fma_rn(r, __fma_rn(-wd, r, 1.0), r);
+    qa = __double2float_rn(__dmul_rn((double)a, r));
+    qb = __double2float_rn(__dmul_rn((double)b, r));
+    qc = __double2float_rn(__dmul_rn((double)c, r));
+}
+
 __device__ __forceinline__ void mat4mul(const float *a, const float *b, float *out) {
 #pragma unroll
     for (int c = 0; c < 4; ++c)

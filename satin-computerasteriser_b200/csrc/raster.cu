@@ -50,6 +50,9 @@
 #ifndef CR_TILE_REJECT
 #define CR_TILE_REJECT 1
 #endif
+#ifndef CR_DIV64
+#define CR_DIV64 0
+#endif
 
 namespace {
 
@@ -299,7 +302,12 @@ __device__ __forceinline__ void project_point(const RasterArgs &a, const ViewReg
 #endif
     bool ok = o.ok;
     if (clip.w <= 0.0f) ok = false;
+#if CR_DIV64
+    float nx, ny, nz;
+    crd::div3_shared(clip.x, clip.y, clip.z, clip.w, nx, ny, nz);
+#else
     const float nx = clip.x / clip.w, ny = clip.y / clip.w, nz = clip.z / clip.w;
+#endif
     if (nx < -1.0f || ny < -1.0f || nx > 1.0f || ny > 1.0f || nz > 1.0f) ok = false;
     if (PASS == PASS_NEAREST ? (nz <= 0.0f) : (nz < 0.0f)) ok = false;
     const int W = vw<MV>(vr), H = vh<MV>(vr);
