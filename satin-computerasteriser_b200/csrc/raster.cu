@@ -1185,19 +1185,33 @@ __device__ __forceinline__ uint32_t hash_slot(uint32_t xy) {
     return ((xy & 0xffffu) + 37u * (xy >> 16)) & (kHashSlots - 1u);
 }
 
+#ifndef CR_HASH3
+#define CR_HASH3 0
+#endif
+// Packed table rows: R | count << 20, G, B — exact while the chunk has fewer
+// than 4096 fragments (a count below 2^12, a red sum below 255 * 4096 < 2^20).
+__device__ __forceinline__ bool hash_packed(uint32_t nfrag) { return CR_HASH3 && nfrag < 4096u; }
+
 template <bool MV>
 __device__ __forceinline__ void hash_add_sums(uint32_t *hkey, uint32_t *hsum, const RasterArgs &a,
                                               const ViewRegsT<MV> &vr, uint32_t pix, uint32_t xy,
-                                              uint32_t r, uint32_t g, uint32_t b, uint32_t n) {
+                                              uint32_t r, uint32_t g, uint32_t b, uint32_t n,
+                                              bool p3 = false) {
     uint32_t h = hash_slot(xy);
     for (int probe = 0; probe < kHashProbes; ++probe) {
         uint32_t cur = hkey[h];
         if (cur == kHashEmpty) cur = atomicCAS(hkey + h, kHashEmpty, pix);
         if (cur == kHashEmpty || cur == pix) {
-            atomicAdd(hsum + h, r);
-            atomicAdd(hsum + kHashSlots + h, g);
-            atomicAdd(hsum + 2 * kHashSlots + h, b);
-            atomicAdd(hsum + 3 * kHashSlots + h, n);
+            if (p3) {
+                atomicAdd(hsum + h, r | (n << 20));
+                atomicAdd(hsum + kHashSlots + h, g);
+                atomicAdd(hsum + 2 * kHashSlots + h, b);
+            } else {
+                atomicAdd(hsum + h, r);
+                atomicAdd(hsum + kHashSlots + h, g);
+                atomicAdd(hsum + 2 * kHashSlots + h, b);
+                atomicAdd(hsum + 3 * kHashSlots + h, n);
+            }
             return;
         }
         h = (h + 1u) & (kHashSlots - 1u);
@@ -1208,9 +1222,9 @@ __device__ __forceinline__ void hash_add_sums(uint32_t *hkey, uint32_t *hsum, co
 template <bool MV>
 __device__ __forceinline__ void hash_add(uint32_t *hkey, uint32_t *hsum, const RasterArgs &a,
                                          const ViewRegsT<MV> &vr, uint32_t pix, uint32_t xy,
-                                         uint32_t col) {
+                                         uint32_t col, bool p3) {
     hash_add_sums<MV>(hkey, hsum, a, vr, pix, xy, col & 0xffu, (col >> 8) & 0xffu,
-                      (col >> 16) & 0xffu, 1u);
+                      (col >> 16) & 0xffu, 1u, p3);
 }
 
 // Clears the table (at kernel start).
@@ -1227,6 +1241,7 @@ template <bool MV>
 __device__ __forceinline__ void hash_frags(const RasterArgs &a, const ViewRegsT<MV> &vr,
                                            uint32_t *hkey, uint32_t *hsum, uint32_t n,
                                            uint32_t base, int W, const uint32_t *depth) {
+    const bool p3 = hash_packed(n);
     if ((base & 3u) == 0u) {
         for (uint32_t f = 4u * threadIdx.x; f < n; f += 4u * kThreads) {
             const uint4 xy = __ldcs(reinterpret_cast<const uint4 *>(a.frag_xy + base + f));
@@ -1253,14 +1268,14 @@ __device__ __forceinline__ void hash_frags(const RasterArgs &a, const ViewRegsT<
                     const uint32_t b = __reduce_add_sync(peers, (cs[q] >> 16) & 0xffu);
                     if ((int)(threadIdx.x & 31) == __ffs(peers) - 1)
                         hash_add_sums<MV>(hkey, hsum, a, vr, pix[q], xs[q], r, g, b,
-                                          (uint32_t)__popc(peers));
+                                          (uint32_t)__popc(peers), p3);
                 }
             }
 #else
 #pragma unroll
             for (int q = 0; q < 4; ++q)
                 if (cl[q] != 0u && zs[q] >= crd::uint_to_depth(cl[q]) * a.keep_scale)
-                    hash_add<MV>(hkey, hsum, a, vr, pix[q], xs[q], cs[q]);
+                    hash_add<MV>(hkey, hsum, a, vr, pix[q], xs[q], cs[q], p3);
 #endif
         }
     } else {
@@ -1269,7 +1284,7 @@ __device__ __forceinline__ void hash_frags(const RasterArgs &a, const ViewRegsT<
             const uint32_t pix = (xy >> 16) * (uint32_t)W + (xy & 0xffffu);
             const uint32_t cl = __ldg(depth + pix);
             if (cl != 0u && a.frag_z[base + f] >= crd::uint_to_depth(cl) * a.keep_scale)
-                hash_add<MV>(hkey, hsum, a, vr, pix, xy, a.frag_col[base + f]);
+                hash_add<MV>(hkey, hsum, a, vr, pix, xy, a.frag_col[base + f], p3);
         }
     }
 }
@@ -1280,15 +1295,16 @@ __device__ __forceinline__ void hash_frags(const RasterArgs &a, const ViewRegsT<
 // completes the sums (and after every thread has read the current claim).
 template <bool MV>
 __device__ __forceinline__ void hash_flush(const RasterArgs &a, const ViewRegsT<MV> &vr,
-                                           uint32_t *hkey, uint32_t *hsum,
+                                           uint32_t *hkey, uint32_t *hsum, bool p3,
                                            uint32_t *cursor = nullptr, uint32_t *next = nullptr) {
     uint32_t claimed = 0u;
     if (cursor && threadIdx.x == 0) claimed = atomicAdd(cursor, 1u);
     for (uint32_t i = threadIdx.x; i < kHashSlots; i += kThreads) {
         const uint32_t pix = hkey[i];
         if (pix == kHashEmpty) continue;
-        color_global<MV>(a, vr, pix, hsum[i], hsum[kHashSlots + i], hsum[2 * kHashSlots + i],
-                         hsum[3 * kHashSlots + i]);
+        const uint32_t w0 = hsum[i];
+        color_global<MV>(a, vr, pix, p3 ? (w0 & 0xfffffu) : w0, hsum[kHashSlots + i],
+                         hsum[2 * kHashSlots + i], p3 ? (w0 >> 20) : hsum[3 * kHashSlots + i]);
         hkey[i] = kHashEmpty;
         hsum[i] = hsum[kHashSlots + i] = hsum[2 * kHashSlots + i] = hsum[3 * kHashSlots + i] = 0u;
     }
@@ -1301,10 +1317,10 @@ __device__ __forceinline__ void hash_flush(const RasterArgs &a, const ViewRegsT<
 __device__ __forceinline__ void hash_chunk(const RasterArgs &a, const ViewRegsT<false> &vr,
                                            uint32_t *hkey, uint32_t *hsum, uint32_t k,
                                            uint32_t *cursor = nullptr, uint32_t *next = nullptr) {
-    hash_frags<false>(a, vr, hkey, hsum, __ldg(a.frag_count + k), __ldg(&a.chunks[k].first),
-                      a.u.width, a.t.depth);
+    const uint32_t nfrag = __ldg(a.frag_count + k);
+    hash_frags<false>(a, vr, hkey, hsum, nfrag, __ldg(&a.chunks[k].first), a.u.width, a.t.depth);
     __syncthreads();  // the chunk's sums are complete (and k has been read by all)
-    hash_flush<false>(a, vr, hkey, hsum, cursor, next);
+    hash_flush<false>(a, vr, hkey, hsum, hash_packed(nfrag), cursor, next);
 }
 
 // 1024 slots (about three times a chunk's typical distinct visible pixels)
@@ -1396,11 +1412,12 @@ __global__ void __launch_bounds__(kThreads, 6)
         const uint32_t slot = view * a.chunk_stride + (k - s_vbegin[view]);
         const ViewDesc &vd = a.views[view];
         const ViewRegsT<true> vr{vd.width, vd.height, vd.depth, vd.accum, vd.nearest};
-        hash_frags<true>(a, vr, hkey, hsum, __ldg(a.frag_count + slot),
+        const uint32_t nfrag = __ldg(a.frag_count + slot);
+        hash_frags<true>(a, vr, hkey, hsum, nfrag,
                          (uint32_t)(s_pbegin[view] + __ldg(a.chunk_poff + slot)), vd.width,
                          vd.depth);
         __syncthreads();  // the chunk's sums are complete (and k has been read by all)
-        hash_flush<true>(a, vr, hkey, hsum, cursor, &s_k);
+        hash_flush<true>(a, vr, hkey, hsum, hash_packed(nfrag), cursor, &s_k);
         __syncthreads();  // the next claim and the cleared table
     }
     if (threadIdx.x == 0) {
