@@ -449,14 +449,24 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
             la.col = raw + coff;
         }
     }
-    pack_load<<<grid_for(count), kThreads, 0, s>>>(la, count, sc.pos);
-    CR_CUDA(cudaGetLastError());
+    // Device-resident 16-byte records {x, y, z, rgba8} already have the
+    // layout of the staged positions: read them in place.
+    const bool in_place = on_device && in->positionStrideBytes == 16 &&
+                          in->colorStrideBytes == 16 && in->colorFormat == CR_COLOR_RGBA8 &&
+                          static_cast<const uint8_t *>(in->colors) ==
+                              static_cast<const uint8_t *>(in->positions) + 12 &&
+                          ((uintptr_t)in->positions & 15) == 0;
+    const float4 *pos = in_place ? static_cast<const float4 *>(in->positions) : sc.pos;
+    if (!in_place) {
+        pack_load<<<grid_for(count), kThreads, 0, s>>>(la, count, sc.pos);
+        CR_CUDA(cudaGetLastError());
+    }
 
     // Stage 1: bounds, read back once.
     const uint32_t binit[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
     CR_CUDA(cudaMemcpyAsync(sc.bounds, binit, sizeof(binit), cudaMemcpyHostToDevice, s));
     pack_bounds<<<std::min<unsigned>(grid_for(count), (unsigned)ctx->sm_count * 8), kThreads, 0,
-                  s>>>(sc.pos, count, sc.bounds);
+                  s>>>(pos, count, sc.bounds);
     CR_CUDA(cudaGetLastError());
     uint32_t bflip[6];
     CR_CUDA(cudaMemcpyAsync(bflip, sc.bounds, sizeof(bflip), cudaMemcpyDeviceToHost, s));
@@ -479,7 +489,7 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
     if (wide) {
         auto *k0 = static_cast<unsigned long long *>(sc.keys[0]);
         auto *k1 = static_cast<unsigned long long *>(sc.keys[1]);
-        pack_morton<unsigned long long><<<grid_for(count), kThreads, 0, s>>>(sc.pos, count, ma, k0,
+        pack_morton<unsigned long long><<<grid_for(count), kThreads, 0, s>>>(pos, count, ma, k0,
                                                                              sc.idx[0]);
         CR_CUDA(cudaGetLastError());
         st = radix_sort_pairs<unsigned long long>(k0, sc.idx[0], k1, sc.idx[1], count, 63,
@@ -488,7 +498,7 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
     } else {
         auto *k0 = static_cast<uint32_t *>(sc.keys[0]);
         auto *k1 = static_cast<uint32_t *>(sc.keys[1]);
-        pack_morton<uint32_t><<<grid_for(count), kThreads, 0, s>>>(sc.pos, count, ma, k0, sc.idx[0]);
+        pack_morton<uint32_t><<<grid_for(count), kThreads, 0, s>>>(pos, count, ma, k0, sc.idx[0]);
         CR_CUDA(cudaGetLastError());
         st = radix_sort_pairs<uint32_t>(k0, sc.idx[0], k1, sc.idx[1], count, 30, sc.radix,
                                         ctx->d_status, ctx->sm_count, s, &in_alt);
@@ -500,7 +510,7 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
     const int L = std::max(1, std::min(prm->lodLevels, 8));
     const int divs = std::max(1, prm->coarseVoxelDivisions);
     const uint8_t max_level = (uint8_t)(L - 1);
-    pack_gather<<<grid_for(count), kThreads, 0, s>>>(sc.pos, idx_sorted, count, sc.sorted,
+    pack_gather<<<grid_for(count), kThreads, 0, s>>>(pos, idx_sorted, count, sc.sorted,
                                                      sc.lv_morton, max_level);
     CR_CUDA(cudaGetLastError());
     if (L > 1) {
