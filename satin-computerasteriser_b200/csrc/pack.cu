@@ -13,7 +13,9 @@
 //   5 LOD           per level, coarsest first: dense voxel grid, atomicMin
 //                   of the Morton position claims a voxel for the first
 //                   eligible point in sorted order (the CPU's "first point
-//                   to occupy an empty voxel")
+//                   to occupy an empty voxel"); the claims of a level ride
+//                   in the kernel before (the gather, or the previous
+//                   level's assignment)
 //   6 batches       one CTA per batch: AABB, level histogram, stable
 //                   level-ascending scatter (warp ballots), RasterBatch with
 //                   the cumulative LOD counts
@@ -188,25 +190,61 @@ __device__ __forceinline__ uint64_t lod_cell(const float4 &p, const LodArgs &a) 
 // The points are in Morton order, so neighbouring lanes often share a cell;
 // lanes carry increasing indices, so the lowest lane of each group of lanes
 // with the same cell holds the group's minimum and alone does the atomicMin
-// (the grid ends the same: min is order-independent).
-__global__ void __launch_bounds__(kThreads)
-    pack_lod_claim(const float4 *__restrict__ sorted, const uint8_t *__restrict__ lv, uint64_t n,
-                   LodArgs a, uint32_t *__restrict__ grid) {
-    const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
-    const bool part = i < n && lv[i] == a.max_level;
-    const unsigned act = __ballot_sync(0xffffffffu, part);
-    if (!part) return;
-    const uint64_t cell = lod_cell(sorted[i], a);
-    const unsigned same = __match_any_sync(act, (unsigned long long)cell);
-    if ((int)(__ffs(same) - 1) == (int)(threadIdx.x & 31u)) atomicMin(&grid[cell], (uint32_t)i);
-}
-
+// (the grid ends the same: min is order-independent).  The last level's
+// assignment:
 __global__ void __launch_bounds__(kThreads)
     pack_lod_assign(const float4 *__restrict__ sorted, uint8_t *__restrict__ lv, uint64_t n,
                     LodArgs a, const uint32_t *__restrict__ grid) {
     const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
     if (i >= n || lv[i] != a.max_level) return;
     if (grid[lod_cell(sorted[i], a)] == (uint32_t)i) lv[i] = a.level;
+}
+
+// The claims are fused into the kernels that read the Morton-ordered points
+// anyway: the gather also claims the coarsest level (every point is still
+// unassigned there), and the assignment of level L also claims level L + 1
+// for the points it leaves unassigned (each level has its own grid), so the
+// points are read once per level instead of twice.
+__device__ __forceinline__ void lod_claim_one(bool part, const float4 &p, uint32_t i,
+                                              const LodArgs &a, uint32_t *grid) {
+    const unsigned act = __ballot_sync(0xffffffffu, part);
+    if (!part) return;
+    const uint64_t cell = lod_cell(p, a);
+    const unsigned same = __match_any_sync(act, (unsigned long long)cell);
+    if ((int)(__ffs(same) - 1) == (int)(threadIdx.x & 31u)) atomicMin(&grid[cell], i);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    pack_gather_claim(const float4 *__restrict__ pos, const uint32_t *__restrict__ idx, uint64_t n,
+                      float4 *__restrict__ sorted, uint8_t *__restrict__ lv, uint8_t max_level,
+                      LodArgs a0, uint32_t *__restrict__ grid0) {
+    const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    const bool v = i < n;
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (v) {
+        p = pos[idx[i]];
+        sorted[i] = p;
+        lv[i] = max_level;
+    }
+    lod_claim_one(v, p, (uint32_t)i, a0, grid0);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    pack_lod_assign_claim(const float4 *__restrict__ sorted, uint8_t *__restrict__ lv, uint64_t n,
+                          LodArgs a, const uint32_t *__restrict__ grid, LodArgs next,
+                          uint32_t *__restrict__ grid_next) {
+    const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    const bool v = i < n && lv[i] == a.max_level;
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+    bool left = false;
+    if (v) {
+        p = sorted[i];
+        if (grid[lod_cell(p, a)] == (uint32_t)i)
+            lv[i] = a.level;
+        else
+            left = true;
+    }
+    lod_claim_one(left, p, (uint32_t)i, next, grid_next);
 }
 
 // Stage 6: per batch AABB + stable level bucketing + RasterBatch
@@ -506,18 +544,22 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
     if (st) return st;
     const uint32_t *idx_sorted = sc.idx[in_alt ? 1 : 0];
 
-    // Stage 4-5: gather, LOD levels.
+    // Stage 4-5: gather, LOD levels (each level its own dense grid).
     const int L = std::max(1, std::min(prm->lodLevels, 8));
     const int divs = std::max(1, prm->coarseVoxelDivisions);
     const uint8_t max_level = (uint8_t)(L - 1);
-    pack_gather<<<grid_for(count), kThreads, 0, s>>>(pos, idx_sorted, count, sc.sorted,
-                                                     sc.lv_morton, max_level);
-    CR_CUDA(cudaGetLastError());
-    if (L > 1) {
+    if (L == 1) {
+        pack_gather<<<grid_for(count), kThreads, 0, s>>>(pos, idx_sorted, count, sc.sorted,
+                                                         sc.lv_morton, max_level);
+        CR_CUDA(cudaGetLastError());
+    } else {
         const float longest = std::fmax(ext[0], std::fmax(ext[1], ext[2]));
         const float base_voxel = longest / (float)divs;
+        std::vector<LodArgs> la_(L - 1);
+        std::vector<uint64_t> goff(L);
+        goff[0] = 0;
         for (int level = 0; level < L - 1; ++level) {
-            LodArgs a;
+            LodArgs &a = la_[level];
             const float voxel = base_voxel * std::pow(0.5f, (float)level);
             a.inv = 1.0f / std::fmax(voxel, 0.000001f);
             uint64_t cells = 1;
@@ -534,15 +576,22 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
                                  "LOD grid of " + std::to_string(cells) + " cells exceeds the cap");
             a.max_level = max_level;
             a.level = (uint8_t)level;
-            if ((st = grow(&sc.grid, sc.cap_grid, cells))) return st;
-            CR_CUDA(cudaMemsetAsync(sc.grid, 0xff, cells * 4, s));
-            pack_lod_claim<<<grid_for(count), kThreads, 0, s>>>(sc.sorted, sc.lv_morton, count, a,
-                                                                sc.grid);
-            CR_CUDA(cudaGetLastError());
-            pack_lod_assign<<<grid_for(count), kThreads, 0, s>>>(sc.sorted, sc.lv_morton, count,
-                                                                 a, sc.grid);
+            goff[level + 1] = goff[level] + cells;
+        }
+        if ((st = grow(&sc.grid, sc.cap_grid, goff[L - 1]))) return st;
+        CR_CUDA(cudaMemsetAsync(sc.grid, 0xff, goff[L - 1] * 4, s));
+        pack_gather_claim<<<grid_for(count), kThreads, 0, s>>>(
+            pos, idx_sorted, count, sc.sorted, sc.lv_morton, max_level, la_[0], sc.grid);
+        CR_CUDA(cudaGetLastError());
+        for (int level = 0; level + 1 < L - 1; ++level) {
+            pack_lod_assign_claim<<<grid_for(count), kThreads, 0, s>>>(
+                sc.sorted, sc.lv_morton, count, la_[level], sc.grid + goff[level],
+                la_[level + 1], sc.grid + goff[level + 1]);
             CR_CUDA(cudaGetLastError());
         }
+        pack_lod_assign<<<grid_for(count), kThreads, 0, s>>>(sc.sorted, sc.lv_morton, count,
+                                                             la_[L - 2], sc.grid + goff[L - 2]);
+        CR_CUDA(cudaGetLastError());
     }
 
     // Stage 6-7: batches, final order, quantisation into the pool.
