@@ -604,7 +604,7 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
         count, ppb, sc.perm, idx_sorted, sc.sorted, sc.lv_out, dst_batches,
         cloud->d_low + p0,
         cloud->d_med + p0, cloud->d_high + p0, cloud->d_colors + p0, cloud->d_levels + p0,
-        sc.src_idx);
+        src_idx_host ? sc.src_idx : nullptr);  // source indices only when asked for
     CR_CUDA(cudaGetLastError());
     if (src_idx_host)
         CR_CUDA(cudaMemcpyAsync(src_idx_host, sc.src_idx, count * 4, cudaMemcpyDeviceToHost, s));
