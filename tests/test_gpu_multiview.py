@@ -181,3 +181,37 @@ def test_batched_views_reject_bad_arguments(cr, orc, ctx):
     mv.frames[1] = mv.frames[0]
     with pytest.raises(cr.CRError):
         mv.render(cams)
+
+
+def test_batched_views_match_oracle_directly(cr, orc, ctx):
+    """Every batched view against the CPU oracle itself (not only against the
+    per-view GPU path): RGBA8, float depth, depth plane and R, G, B, count
+    planes, bit for bit, with two clouds (one moved by a model matrix)."""
+    from scenes import oracle_cloud_from_device, oracle_config
+    pos, rgba = lattice_cloud(30, 21)
+    a = make_cloud(cr, orc, ctx, pos, rgba)
+    pos2, rgba2 = blob_cloud(40000, 22)
+    b = make_cloud(cr, orc, ctx, pos2, rgba2, ppb=777)
+    b.position = (0.3, -0.2, 0.1)
+    sizes = [(96, 64), (160, 90), (64, 128)]
+    mv = cr.MultiViewRasteriser(ctx, sizes)
+    mv.addPointCloud(a)
+    mv.addPointCloud(b)
+    cams = cameras(cr, sizes, 9)
+    mv.render(cams)
+    cfg = oracle_config(orc, mv.configuration)
+    for i, (cam, (w, h)) in enumerate(zip(cams, sizes)):
+        clouds = []
+        for c in (a, b):
+            oc = oracle_cloud_from_device(orc, c)
+            vp = cr.matrix_multiply(cam.projectionMatrix, cam.viewMatrix)
+            oc.files = orc.update_files(orc.identity_file(), vp, c.worldMatrix)
+            clouds.append(oc)
+        ref = orc.render(clouds, cfg, cam.viewMatrix, cam.projectionMatrix, w, h)
+        assert np.array_equal(mv.outputRGBA8(i), ref.rgba), f"view {i} rgba"
+        assert np.array_equal(mv.depthTexture(i).view(np.uint32), ref.depthf.view(np.uint32))
+        px = mv.pixels(i)
+        assert np.array_equal(px["depth"], ref.depth), f"view {i} depth"
+        acc = np.stack([px["red"], px["green"], px["blue"], px["count"]], -1)
+        assert np.array_equal(acc, ref.accum), f"view {i} accum"
+        assert ref.accum[..., 3].any()
