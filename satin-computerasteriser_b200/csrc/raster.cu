@@ -53,6 +53,9 @@
 #ifndef CR_DIV64
 #define CR_DIV64 0
 #endif
+#ifndef CR_TILE_PX_PER_POINT
+#define CR_TILE_PX_PER_POINT 1
+#endif
 
 namespace {
 
@@ -1017,7 +1020,8 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
         const bool new_file = file_id != sb.file;
         const uint32_t work = PASS == PASS_COLOR_FRAG ? nfrag : c.count;
         const bool tiled = a.use_tiles && a.radius_zero && c.tw > 0 &&
-                           c.tw * c.th <= TileCfg<PASS>::kPx && c.tw * c.th <= (int)work &&
+                           c.tw * c.th <= TileCfg<PASS>::kPx &&
+                           c.tw * c.th <= CR_TILE_PX_PER_POINT * (int)work &&
                            (!is_color(PASS) || c.count < 4096u);
         if (new_file || tiled) {
             __syncthreads();  // everyone has read sb.file (and the view state)
