@@ -53,44 +53,6 @@ __device__ __forceinline__ f4 mulp(const float *m, float x, float y, float z) {
     return r;
 }
 
-// Packed pairs of FP32 operations (sm_100: one instruction, two lanes).  Each
-// lane is rounded to nearest-even on its own, exactly as the scalar mul.rn /
-// add.rn, and the explicit rounding mode keeps them out of FMA contraction.
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
-    float2 r;
-    asm("{\n\t.reg .b64 pa, pb, pr;\n\t"
-        "mov.b64 pa, {%2, %3};\n\t"
-        "mov.b64 pb, {%4, %5};\n\t"
-        "mul.rn.f32x2 pr, pa, pb;\n\t"
-        "mov.b64 {%0, %1}, pr;\n\t}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-__device__ __forceinline__ float2 add2(float2 a, float2 b) {
-    float2 r;
-    asm("{\n\t.reg .b64 pa, pb, pr;\n\t"
-        "mov.b64 pa, {%2, %3};\n\t"
-        "mov.b64 pb, {%4, %5};\n\t"
-        "add.rn.f32x2 pr, pa, pb;\n\t"
-        "mov.b64 {%0, %1}, pr;\n\t}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-
-// M * (p, 1) for a column-major 4x4 with the rows paired (x, y) and (z, w):
-// per row ((c0*x + c1*y) + c2*z) + c3, every product and sum rounded, the
-// same values as mulp.
-__device__ __forceinline__ f4 mulp2(const float *m, float x, float y, float z) {
-    const float2 xx = make_float2(x, x), yy = make_float2(y, y), zz = make_float2(z, z);
-    float2 a = add2(mul2(make_float2(m[0], m[1]), xx), mul2(make_float2(m[4], m[5]), yy));
-    a = add2(add2(a, mul2(make_float2(m[8], m[9]), zz)), make_float2(m[12], m[13]));
-    float2 b = add2(mul2(make_float2(m[2], m[3]), xx), mul2(make_float2(m[6], m[7]), yy));
-    b = add2(add2(b, mul2(make_float2(m[10], m[11]), zz)), make_float2(m[14], m[15]));
-    return f4{a.x, a.y, b.x, b.y};
-}
-
 // Three IEEE single-precision quotients a/w, b/w, c/w that share one
 // reciprocal, computed in double precision: r ~ 1/w from the single-precision
 // reciprocal approximation refined by two Newton-Raphson steps in double

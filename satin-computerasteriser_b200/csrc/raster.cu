@@ -44,11 +44,8 @@
 #include "cr_internal.h"
 #include "cr_resolve.cuh"
 
-#ifndef CR_PACKED_F32X2
-#define CR_PACKED_F32X2 0
-#endif
 #ifndef CR_TILE_REJECT
-#define CR_TILE_REJECT 1
+#define CR_TILE_REJECT 0
 #endif
 #ifndef CR_DIV64
 #define CR_DIV64 0
@@ -286,23 +283,10 @@ __device__ __forceinline__ void project_point(const RasterArgs &a, const ViewReg
         y = (((lo >> 10) & 1023u) << sl) | (((me >> 10) & 1023u) << sm) | ((hi >> 10) & 1023u);
         z = (((lo >> 20) & 1023u) << sl) | (((me >> 20) & 1023u) << sm) | ((hi >> 20) & 1023u);
     }
-#if CR_PACKED_F32X2 & 2
-    // x and y lanes paired in packed FP32 instructions (identical roundings).
-    const float2 pxy = crd::add2(crd::mul2(make_float2((float)x, (float)y), make_float2(c.qx, c.qy)),
-                                 make_float2(c.minX, c.minY));
-    o.px = pxy.x;
-    o.py = pxy.y;
-    o.pz = (float)z * c.qz + c.minZ;
-#else
     o.px = (float)x * c.qx + c.minX;
     o.py = (float)y * c.qy + c.minY;
     o.pz = (float)z * c.qz + c.minZ;
-#endif
-#if CR_PACKED_F32X2 & 1
-    const crd::f4 clip = crd::mulp2(sb.T, o.px, o.py, o.pz);
-#else
     const crd::f4 clip = crd::mulp(sb.T, o.px, o.py, o.pz);
-#endif
     bool ok = o.ok;
     if (clip.w <= 0.0f) ok = false;
 #if CR_DIV64
@@ -314,16 +298,8 @@ __device__ __forceinline__ void project_point(const RasterArgs &a, const ViewReg
     if (nx < -1.0f || ny < -1.0f || nx > 1.0f || ny > 1.0f || nz > 1.0f) ok = false;
     if (PASS == PASS_NEAREST ? (nz <= 0.0f) : (nz < 0.0f)) ok = false;
     const int W = vw<MV>(vr), H = vh<MV>(vr);
-#if CR_PACKED_F32X2 & 4
-    const float2 sxy = crd::mul2(crd::add2(crd::mul2(make_float2(nx, ny), make_float2(0.5f, 0.5f)),
-                                           make_float2(0.5f, 0.5f)),
-                                 make_float2((float)W, (float)H));
-    o.ix = (int)sxy.x;
-    const int iy = (int)sxy.y;
-#else
     o.ix = (int)((nx * 0.5f + 0.5f) * (float)W);
     const int iy = (int)((ny * 0.5f + 0.5f) * (float)H);
-#endif
     if (o.ix < 0 || o.ix >= W || iy < 0 || iy >= H) ok = false;
     o.iy = H - 1 - iy;
     o.depth = crd::depth_to_uint(nz);
@@ -341,23 +317,6 @@ __device__ __forceinline__ unsigned long long nearest_key(uint32_t depth, uint32
     return ((unsigned long long)depth << 32) | (unsigned long long)(~index);
 }
 
-#ifndef CR_MATCH_MERGE
-#define CR_MATCH_MERGE 0
-#endif
-// Warp pre-merge of 64-bit maxima on the same address: the lanes with
-// `valid` and the same `pix` reduce their keys (high words first, then the
-// low words of the lanes holding the high maximum); returns true on the one
-// lane per group that then updates memory with `k` (the group's maximum).
-__device__ __forceinline__ bool warp_merge_max_u64(bool valid, uint32_t pix,
-                                                   unsigned long long &k) {
-    const unsigned act = __ballot_sync(kFull, valid);
-    if (!valid) return false;
-    const unsigned peers = __match_any_sync(act, pix);
-    const uint32_t hi = __reduce_max_sync(peers, (uint32_t)(k >> 32));
-    const uint32_t lo = __reduce_max_sync(peers, (uint32_t)(k >> 32) == hi ? (uint32_t)k : 0u);
-    k = ((unsigned long long)hi << 32) | lo;
-    return (int)(threadIdx.x & 31) == __ffs(peers) - 1;
-}
 
 // Reductions into the frame planes (global memory).  Written as red.global
 // on explicitly global addresses: the batched-view passes take the plane
@@ -472,12 +431,7 @@ __device__ __forceinline__ void emit_direct(const RasterArgs &a, const ViewRegsT
             grad_store(a, o.pointIndex, g);
         }
     } else {
-#if CR_MATCH_MERGE & 1
-        unsigned long long k = nearest_key(o.depth, o.pointIndex);
-        if (warp_merge_max_u64(o.ok, pix, k)) red_max_u64(&vnearest<MV>(vr)[pix], k);
-#else
         if (o.ok) red_max_u64(&vnearest<MV>(vr)[pix], nearest_key(o.depth, o.pointIndex));
-#endif
     }
 }
 
@@ -502,31 +456,10 @@ __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ViewRegsT<M
     const uint32_t pix = (uint32_t)(o.iy * vw<MV>(vr) + o.ix);
     const int l = inside ? ly * c.tw + lx : 0;
     if (PASS == PASS_DEPTH_FRAG && CR_TILE_REJECT) {
-#if CR_MATCH_MERGE & 2
-        // Lanes on one pixel merge their depths first; every lane of the
-        // group tests its fragment against the group's maximum and what the
-        // tile held before.
-        const unsigned act = __ballot_sync(kFull, o.ok);
-        uint32_t seen = 0u;
-        if (o.ok) {
-            const unsigned peers = __match_any_sync(act, pix);
-            const uint32_t gmax = __reduce_max_sync(peers, o.depth);
-            const int leader = __ffs(peers) - 1;
-            if ((int)(threadIdx.x & 31) == leader) {
-                if (inside)
-                    seen = atomicMax(reinterpret_cast<uint32_t *>(smem) + l, gmax);
-                else
-                    red_max_u32(&vdepth<MV>(vr)[pix], gmax);
-            }
-            seen = max(__shfl_sync(peers, seen, leader), gmax);
-        }
-        o.doomed = o.nz < crd::uint_to_depth(seen) * a.keep_scale;
-#else
         uint32_t seen = 0u;
         if (in_tile) seen = atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
         if (outside) red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
         o.doomed = o.nz < crd::uint_to_depth(seen) * a.keep_scale;
-#endif
     } else if (is_depth(PASS)) {
         if (in_tile) atomicMax(reinterpret_cast<uint32_t *>(smem) + l, o.depth);
         if (outside) red_max_u32(&vdepth<MV>(vr)[pix], o.depth);
@@ -547,15 +480,9 @@ __device__ __forceinline__ void emit_tile(const RasterArgs &a, const ViewRegsT<M
         }
         if (vis && !inside) color_global<MV>(a, vr, pix, r, g, b, 1u);
     } else {
-        unsigned long long k = nearest_key(o.depth, o.pointIndex);
-#if CR_MATCH_MERGE & 1
-        const bool lead = warp_merge_max_u64(o.ok, pix, k);
-        if (lead && inside) atomicMax(reinterpret_cast<unsigned long long *>(smem) + l, k);
-        if (lead && !inside) red_max_u64(&vnearest<MV>(vr)[pix], k);
-#else
+        const unsigned long long k = nearest_key(o.depth, o.pointIndex);
         if (in_tile) atomicMax(reinterpret_cast<unsigned long long *>(smem) + l, k);
         if (outside) red_max_u64(&vnearest<MV>(vr)[pix], k);
-#endif
     }
 }
 
@@ -1259,28 +1186,10 @@ __device__ __forceinline__ void hash_frags(const RasterArgs &a, const ViewRegsT<
                 pix[q] = (xs[q] >> 16) * (uint32_t)W + (xs[q] & 0xffffu);
                 cl[q] = f + q < n ? __ldg(depth + pix[q]) : 0u;
             }
-#if CR_MATCH_MERGE & 4
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                // Lanes with the same visible pixel sum their colours first.
-                const bool vis = cl[q] != 0u && zs[q] >= crd::uint_to_depth(cl[q]) * a.keep_scale;
-                const unsigned act = __ballot_sync(kFull, vis);
-                if (vis) {
-                    const unsigned peers = __match_any_sync(act, pix[q]);
-                    const uint32_t r = __reduce_add_sync(peers, cs[q] & 0xffu);
-                    const uint32_t g = __reduce_add_sync(peers, (cs[q] >> 8) & 0xffu);
-                    const uint32_t b = __reduce_add_sync(peers, (cs[q] >> 16) & 0xffu);
-                    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1)
-                        hash_add_sums<MV>(hkey, hsum, a, vr, pix[q], xs[q], r, g, b,
-                                          (uint32_t)__popc(peers), p3);
-                }
-            }
-#else
 #pragma unroll
             for (int q = 0; q < 4; ++q)
                 if (cl[q] != 0u && zs[q] >= crd::uint_to_depth(cl[q]) * a.keep_scale)
                     hash_add<MV>(hkey, hsum, a, vr, pix[q], xs[q], cs[q], p3);
-#endif
         }
     } else {
         for (uint32_t f = threadIdx.x; f < n; f += kThreads) {
