@@ -736,7 +736,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // in the level array and it has at most kStagePoints points.
 constexpr uint32_t kStagePoints = 2048;
 constexpr uint32_t kStageBytes = kStagePoints * (1 + 4 + 4);
-constexpr uint32_t kStageWaitLimit = 1u << 20;  // polls of an mbarrier before giving up
+constexpr uint32_t kStageWaitLimit = 1u << 16;  // polls of an mbarrier before giving up
 __device__ __forceinline__ bool stage_ok(uint32_t first, uint32_t count) {
     return (first & 15u) == 0u && count <= kStagePoints && count > 0u;
 }
