@@ -223,16 +223,64 @@ __device__ __forceinline__ bool intersects_frustum(const float *m, f3 mn, f3 mx)
     return true;
 }
 
+// The per-file parts of the cull, computed once per file instead of once
+// per batch (the same operations on the same inputs, so the same bits): the
+// six normalised frustum planes of makePlane (nx, ny, nz, offset) and
+// view * world for pixelSizeOnScreen.
+struct FilePre {
+    float plane[6][4];
+    float vw[16];
+};
+__device__ __forceinline__ void plane_of(float x, float y, float z, float w, float *out) {
+    const float len = fmaxf(sqrtf((x * x + y * y) + z * z), 0.000001f);
+    out[0] = x / len;
+    out[1] = y / len;
+    out[2] = z / len;
+    out[3] = w / len;
+}
+// Plane k (0..5) of the frustum matrix m, in intersects_frustum's order.
+__device__ __forceinline__ void frustum_plane(const float *m, int k, float *out) {
+#define M_(c, r) m[(c) * 4 + (r)]
+    switch (k) {
+    case 0: plane_of(M_(0, 3) - M_(0, 0), M_(1, 3) - M_(1, 0), M_(2, 3) - M_(2, 0), M_(3, 3) - M_(3, 0), out); break;
+    case 1: plane_of(M_(0, 3) + M_(0, 0), M_(1, 3) + M_(1, 0), M_(2, 3) + M_(2, 0), M_(3, 3) + M_(3, 0), out); break;
+    case 2: plane_of(M_(0, 3) + M_(0, 1), M_(1, 3) + M_(1, 1), M_(2, 3) + M_(2, 1), M_(3, 3) + M_(3, 1), out); break;
+    case 3: plane_of(M_(0, 3) - M_(0, 1), M_(1, 3) - M_(1, 1), M_(2, 3) - M_(2, 1), M_(3, 3) - M_(3, 1), out); break;
+    case 4: plane_of(M_(0, 3) - M_(0, 2), M_(1, 3) - M_(1, 2), M_(2, 3) - M_(2, 2), M_(3, 3) - M_(3, 2), out); break;
+    default: plane_of(M_(0, 2), M_(1, 2), M_(2, 2), M_(3, 2), out); break;
+    }
+#undef M_
+}
+// intersects_frustum over precomputed planes.
+__device__ __forceinline__ bool intersects_frustum_pre(const FilePre &f, f3 mn, f3 mx) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float nx = f.plane[k][0], ny = f.plane[k][1], nz = f.plane[k][2];
+        const float px = nx > 0.0f ? mx.x : mn.x;
+        const float py = ny > 0.0f ? mx.y : mn.y;
+        const float pz = nz > 0.0f ? mx.z : mn.z;
+        if (((nx * px + ny * py) + nz * pz) + f.plane[k][3] < 0.0f) return false;
+    }
+    return true;
+}
+
 // pixelSizeOnScreen (Common.metal:155-170).
+__device__ __forceinline__ float pixel_size_on_screen_vw(const cr_raster_batch &b, const float *vw,
+                                                         const float *proj, int sw, int sh);
 __device__ __forceinline__ float pixel_size_on_screen(const cr_raster_batch &b, const float *world,
                                                       const float *view, const float *proj,
                                                       int sw, int sh) {
+    float vw[16];
+    mat4mul(view, world, vw);
+    return pixel_size_on_screen_vw(b, vw, proj, sw, sh);
+}
+// pixelSizeOnScreen with view * world given.
+__device__ __forceinline__ float pixel_size_on_screen_vw(const cr_raster_batch &b, const float *vw,
+                                                         const float *proj, int sw, int sh) {
     const float cx = (b.minX + b.maxX) * 0.5f, cy = (b.minY + b.maxY) * 0.5f,
                 cz = (b.minZ + b.maxZ) * 0.5f;
     const float dx = b.minX - b.maxX, dy = b.minY - b.maxY, dz = b.minZ - b.maxZ;
     const float radius = sqrtf((dx * dx + dy * dy) + dz * dz);
-    float vw[16];
-    mat4mul(view, world, vw);
     const f4 vc = mulp(vw, cx, cy, cz);
     const f4 ve{vc.x + radius, vc.y + 0.0f, vc.z + 0.0f, vc.w + 0.0f};
     f4 pc = mulv(proj, vc);

@@ -64,9 +64,11 @@ __device__ __forceinline__ void screen_rect(const cr_raster_batch &b, const floa
 }
 
 // One slot of cullUpdate (Cull/Shaders.metal:28-82).
-// files: the cull's file table (a.files, or the one-view launch's inline copy).
+// files: the cull's file table (a.files, or the one-view launch's inline copy);
+// pre: the per-file planes and view * world of the inline files (or null).
 __device__ __forceinline__ bool cull_slot(const CullArgs &a, const cr_raster_file *files,
-                                          uint32_t gid, CullRec &out) {
+                                          uint32_t gid, CullRec &out,
+                                          const crd::FilePre *pre = nullptr) {
     const cr_raster_batch b = a.batches[gid];
     if (b.state == 0) return false;  // residency gate (:33-36)
     // A fileIndex past the file table is rejected here (the reference would
@@ -74,12 +76,16 @@ __device__ __forceinline__ bool cull_slot(const CullArgs &a, const cr_raster_fil
     if (b.fileIndex >= a.nfiles) return false;
     const cr_raster_file *file = &files[b.fileIndex];
     if (a.u.enableFrustumCulling != 0) {
-        if (!crd::intersects_frustum(file->transformFrustum, crd::f3{b.minX, b.minY, b.minZ},
-                                     crd::f3{b.maxX, b.maxY, b.maxZ}))
+        const crd::f3 mn{b.minX, b.minY, b.minZ}, mx{b.maxX, b.maxY, b.maxZ};
+        if (pre ? !crd::intersects_frustum_pre(pre[b.fileIndex], mn, mx)
+                : !crd::intersects_frustum(file->transformFrustum, mn, mx))
             return false;
     }
     const float px =
-        crd::pixel_size_on_screen(b, file->world, a.u.view, a.u.proj, a.u.width, a.u.height);
+        pre ? crd::pixel_size_on_screen_vw(b, pre[b.fileIndex].vw, a.u.proj, a.u.width,
+                                           a.u.height)
+            : crd::pixel_size_on_screen(b, file->world, a.u.view, a.u.proj, a.u.width,
+                                        a.u.height);
     const int level = crd::precision_level(px);
     // lodThresholdFromPixelSize (Common.metal:185-187); CLOD off -> 99 (:58-60).
     const float thr =
@@ -327,11 +333,24 @@ __global__ void __launch_bounds__(kCullThreads)
     __shared__ uint32_t scan_c[kCullThreads / 32], scan_p[kCullThreads / 32];
     __shared__ CullRec s_rec[kCullThreads];
     __shared__ uint32_t s_cbase[kCullThreads];
+    __shared__ crd::FilePre s_pre[kInlineFiles];
     const uint32_t epoch = *(volatile const uint32_t *)(a.counters + CNT_CULL_EPOCH) + 1u;
     const uint32_t gid = ticket * kCullThreads + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // The inline files' frustum planes and view * world, once per CTA: a
+    // thread per (file, plane) and per (file, view * world).
+    if (ifl.n) {
+        const uint32_t t = threadIdx.x;
+        if (t < 6 * ifl.n) {
+            crd::frustum_plane(ifl.f[t / 6].transformFrustum, (int)(t % 6), s_pre[t / 6].plane[t % 6]);
+        } else if (t >= 32 && t < 32 + ifl.n) {
+            crd::mat4mul(a.u.view, ifl.f[t - 32].world, s_pre[t - 32].vw);
+        }
+        __syncthreads();
+    }
     CullRec rec;
-    const bool keep = gid < a.nbatches && cull_slot(a, ifl.n ? ifl.f : a.files, gid, rec);
+    const bool keep = gid < a.nbatches &&
+                      cull_slot(a, ifl.n ? ifl.f : a.files, gid, rec, ifl.n ? s_pre : nullptr);
     const uint32_t c = keep ? nchunks(rec.vb.activePoints, a.chunk_points) : 0u;
     const uint32_t n = keep ? fragment_span(rec.vb.activePoints, a.chunk_points) : 0u;
     const uint32_t ballot = __ballot_sync(0xffffffffu, keep);
