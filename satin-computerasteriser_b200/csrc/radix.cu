@@ -48,14 +48,27 @@ __device__ __forceinline__ unsigned long long lookback_word(uint32_t epoch, unsi
                                                             unsigned long long count) {
     return ((unsigned long long)epoch << 48) | (flag << 46) | count;
 }
-__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
+// The look-back words carry their data (the counts) in the word itself, so
+// relaxed loads and stores at GPU scope suffice (no other memory is read
+// through them).
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
     unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release64(unsigned long long *p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+__device__ __forceinline__ bool lookback_ready(unsigned long long v, uint32_t epoch) {
+    return (uint32_t)(v >> 48) == epoch && ((v >> 46) & 3ull) != 0ull;
+}
+#ifndef CR_LOOKBACK_BATCH
+#define CR_LOOKBACK_BATCH 8
+#endif
+#ifndef CR_SORT_MIN_BLOCKS
+#define CR_SORT_MIN_BLOCKS 3
+#endif
+constexpr int kLookbackBatch = CR_LOOKBACK_BATCH;  // predecessor words one round loads at once
 
 // Histograms of every 8-bit digit of the keys (grid-stride, per-CTA shared
 // counts added to global memory once per CTA).
@@ -106,7 +119,7 @@ size_t onesweep_smem_bytes() {
 //      digit's global offset: keys of one digit are consecutive in shared
 //      memory and land at consecutive addresses (coalesced runs).
 template <typename K>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
     radix_onesweep(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                    K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, uint64_t n,
                    int shift, const uint32_t *__restrict__ digit_base,
@@ -160,29 +173,50 @@ __global__ void __launch_bounds__(kThreads)
     unsigned long long *my = lookback + (size_t)tile * 256 + dd;
     unsigned long long excl = 0;
     if (tile == 0) {
-        st_release64(my, lookback_word(epoch, kFlagPrefix, total));
+        st_relaxed64(my, lookback_word(epoch, kFlagPrefix, total));
     } else {
-        st_release64(my, lookback_word(epoch, kFlagAgg, total));
-        bool gave_up = false;
-        for (int64_t t = (int64_t)tile - 1; t >= 0; --t) {
-            const unsigned long long *w = lookback + (size_t)t * 256 + dd;
-            unsigned long long v = 0;
-            uint32_t polls = 0;
-            for (;;) {
-                v = ld_acquire64(w);
-                if ((uint32_t)(v >> 48) == epoch && ((v >> 46) & 3ull) != 0ull) break;
-                if (++polls >= kLookbackLimit) break;
-                __nanosleep(32);
+        st_relaxed64(my, lookback_word(epoch, kFlagAgg, total));
+        // Look-back over the tiles before this one, kLookbackBatch words per
+        // round (independent loads), newest first: add counts until a tile's
+        // inclusive prefix; a word not yet published is polled (bounded).
+        bool gave_up = false, done = false;
+        int64_t t = (int64_t)tile - 1;
+        while (!done && t >= 0) {
+            const int n = t + 1 < kLookbackBatch ? (int)(t + 1) : kLookbackBatch;
+            unsigned long long v[kLookbackBatch];
+#pragma unroll
+            for (int k = 0; k < kLookbackBatch; ++k)
+                if (k < n) v[k] = ld_relaxed64(lookback + (size_t)(t - k) * 256 + dd);
+            int used = n;
+#pragma unroll
+            for (int k = 0; k < kLookbackBatch; ++k) {
+                if (k >= used) break;
+                if (!lookback_ready(v[k], epoch)) {
+                    // Poll this predecessor, then carry on from it.
+                    const unsigned long long *w = lookback + (size_t)(t - k) * 256 + dd;
+                    uint32_t polls = 0;
+                    unsigned long long x = ld_relaxed64(w);
+                    while (!lookback_ready(x, epoch) && ++polls < kLookbackLimit) {
+                        __nanosleep(32);
+                        x = ld_relaxed64(w);
+                    }
+                    if (!lookback_ready(x, epoch)) {
+                        gave_up = true;
+                        done = true;
+                        break;
+                    }
+                    v[k] = x;
+                }
+                excl += v[k] & ((1ull << 46) - 1);
+                if (((v[k] >> 46) & 3ull) == kFlagPrefix) {
+                    done = true;
+                    break;
+                }
             }
-            if (polls >= kLookbackLimit) {
-                gave_up = true;
-                break;
-            }
-            excl += v & ((1ull << 46) - 1);
-            if (((v >> 46) & 3ull) == kFlagPrefix) break;
+            t -= n;
         }
         if (gave_up && status) *(volatile uint32_t *)status = kErrSortWait;
-        st_release64(my, lookback_word(epoch, kFlagPrefix, excl + total));
+        st_relaxed64(my, lookback_word(epoch, kFlagPrefix, excl + total));
     }
     offset[dd] = digit_base[dd] + (uint32_t)excl;
     // 3. Exclusive scan of the tile's digit counts (a warp scan per 32
