@@ -542,20 +542,30 @@ def run_ours(args, dist):
     # the host sets the next frame's camera (encode has already captured
     # frame k's), then waits for frame k-1's copy, whose buffer is then
     # complete, and enqueues frame k's.  The clock stops after the last copy.
+    # One untimed frame first creates the copy stream and events, then the
+    # loop runs three times and the median is reported (host-side noise).
     pinned = [cr.HostBuffer((H, W, 4), np.uint8) for _ in range(2)]
-    dist.barrier()
-    ctx.synchronize()
-    t0 = time.perf_counter()
     ras.update(cams[timed[0]])
-    for k in range(len(timed)):
-        frame_encoder.encode()
-        if k + 1 < len(timed):
-            ras.update(cams[timed[k + 1]])
-        ras.waitOutput()
-        ras.outputRGBA8Async(pinned[k & 1].array)
+    frame_encoder.encode()
+    ras.outputRGBA8Async(pinned[0].array)
     ras.waitOutput()
-    e2e_s = time.perf_counter() - t0
-    e2e_max = dist.max(e2e_s)
+
+    def e2e_loop():
+        dist.barrier()
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        ras.update(cams[timed[0]])
+        for k in range(len(timed)):
+            frame_encoder.encode()
+            if k + 1 < len(timed):
+                ras.update(cams[timed[k + 1]])
+            ras.waitOutput()
+            ras.outputRGBA8Async(pinned[k & 1].array)
+        ras.waitOutput()
+        return dist.max(time.perf_counter() - t0)
+
+    e2e_runs = [e2e_loop() for _ in range(3)]
+    e2e_max = statistics.median(e2e_runs)
     last_ok = bool(np.array_equal(pinned[(len(timed) - 1) & 1].array, ras.outputRGBA8()))
     # The same loop with a blocking read-back per frame, for comparison.
     dist.barrier()
@@ -570,6 +580,8 @@ def run_ours(args, dist):
            "unit": "Gpts/s", "h2d_bytes_per_step": 256, "d2h_bytes_per_step": W * H * 4,
            "ms_per_step": round(e2e_max * 1e3 / args.steps, 4),
            "readback": "asynchronous, overlapped with the next frame (2 pinned buffers)",
+           "timing": "wall clock, median of 3 runs of the timed poses (max over ranks)",
+           "runs_ms_per_step": [round(x * 1e3 / args.steps, 4) for x in e2e_runs],
            "last_image_matches_blocking_read": last_ok,
            "blocking_readback": {
                "value": round(units * args.steps / blocking_max / 1e9, 4),

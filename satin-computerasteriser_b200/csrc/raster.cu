@@ -86,11 +86,8 @@ struct TileCfg<PASS_NEAREST> {
 template <>
 struct TileCfg<PASS_DEPTH_FRAG> {
     static constexpr int kPx = 4096;
-#if CR_BULK_STAGE
-    static constexpr int kBytes = kPx * 8 + 2 * 2048 * 9;  // + two bulk stage buffers
-#else
-    static constexpr int kBytes = kPx * 8;
-#endif
+    static constexpr int kTileBytes = kPx * (CR_TILE_REJECT ? 8 : 4);
+    static constexpr int kBytes = kTileBytes + (CR_BULK_STAGE ? 2 * 2048 * 9 : 0);  // + stage buffers
 };
 template <>
 struct TileCfg<PASS_COLOR_FRAG> : TileCfg<PASS_COLOR> {};
@@ -875,7 +872,7 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
     __shared__ uint32_t s_k[2], s_kview[2], s_kslot[2];  // per record buffer
     constexpr bool kStage = CR_BULK_STAGE && PASS == PASS_DEPTH_FRAG && !MV;
     __shared__ __align__(8) uint64_t s_mbar[2];
-    unsigned char *stage_base = smem + TileCfg<PASS>::kPx * 8;
+    unsigned char *stage_base = smem + TileCfg<PASS_DEPTH_FRAG>::kTileBytes;
     uint32_t stage_phase = 0u;  // per buffer: the parity of its next completion
     auto finish = [&]() {
         if (threadIdx.x == 0) {
