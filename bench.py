@@ -1098,6 +1098,22 @@ def run_multiview(args, cr, ctx, torch, dist):
     ev1.record(stream)
     ev1.synchronize()
     per_view_ms = ev0.elapsed_time(ev1) / args.mv_reps
+    # Pass times of the per-view renders (a separate run with a CUDA event
+    # around every pass): the depth and colour work is the same in both
+    # forms, so (all passes) / (depth + colour) bounds what batching can gain.
+    ctx.set_profiling(True)
+    per_view()
+    ctx.synchronize()
+    pt = ctx.pass_times(len(cams))
+    ctx.set_profiling(False)
+    names = list(PASS_NAMES)
+    work = float(pt[:, names.index("depth")].sum() + pt[:, names.index("color")].sum())
+    by_size = {}
+    for w, h in MV_SIZES:
+        idx = [i for i, sz in enumerate(sizes) if sz == (w, h)]
+        if idx:
+            by_size[f"{w}x{h}"] = {n: round(float(pt[idx, k].mean()), 4)
+                                   for k, n in enumerate(names) if pt[idx, k].any()}
 
     mv = cr.MultiViewRasteriser(ctx, sizes)
     mv.addPointCloud(cloud)
@@ -1132,6 +1148,10 @@ def run_multiview(args, cr, ctx, torch, dist):
             "sizes": {f"{w}x{h}": sizes.count((w, h)) for w, h in MV_SIZES},
             "per_view_ms": round(per_view_ms, 4), "batched_ms": round(batched_ms, 4),
             "speedup": round(per_view_ms / batched_ms, 3),
+            "per_view_pass_ms": by_size,
+            "ceiling": {"value": round(float(pt.sum()) / max(work, 1e-9), 3),
+                        "why": "per-view pass time over its depth + colour time: the "
+                               "per-(point, view) work that batching cannot share"},
             "batched_gpts_per_s": round(n * args.mv_points / (batched_ms / 1e3) / 1e9, 2),
             "bit_exact": bool(exact), "tuning": tuned,
             "timing": "CUDA events on the library stream, mean of --mv-reps repetitions "
