@@ -110,11 +110,12 @@ size_t onesweep_smem_bytes() {
 //   1. each warp takes 512 consecutive keys, 16 per lane in warp-striped order
 //      (key j*32 + lane), and ranks them among equal digits with
 //      __match_any_sync against running per-warp digit counts, in input order;
-//   2. thread d: the tile's count of digit d and the exclusive bases of the
-//      warps; the count is published, the counts of the tiles before it are
-//      summed (look-back), the inclusive prefix is published;
+//   2. thread d: the tile's count of digit d (published at once) and the
+//      exclusive bases of the warps;
 //   3. exclusive scan over the digits gives each key its slot in a tile
-//      sorted by digit; keys and values move there in shared memory;
+//      sorted by digit; keys and values move there in shared memory; then
+//      thread d sums the counts of the tiles before it (look-back) and
+//      publishes the inclusive prefix;
 //   4. threads read the sorted tile in order and write each key to its
 //      digit's global offset: keys of one digit are consecutive in shared
 //      memory and land at consecutive addresses (coalesced runs).
@@ -160,8 +161,7 @@ __global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
         __syncwarp();
     }
     __syncthreads();
-    // 2. Digit d = thread: the tile's count, the warps' exclusive bases, the
-    //    look-back over the tiles before this one.
+    // 2. Digit d = thread: the tile's count and the warps' exclusive bases.
     const uint32_t dd = threadIdx.x;
     uint32_t total = 0;
 #pragma unroll
@@ -171,23 +171,46 @@ __global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
         total += c;
     }
     unsigned long long *my = lookback + (size_t)tile * 256 + dd;
+    // Publish the tile's count first (tile 0: its prefix), so that the tiles
+    // after it can go on while this one sorts its keys.
+    st_relaxed64(my, lookback_word(epoch, tile == 0 ? kFlagPrefix : kFlagAgg, total));
+    // 3. Exclusive scan of the tile's digit counts (a warp scan per 32
+    //    digits, then over the warps).
+    const uint32_t incl = warp_inclusive(total, lane);
+    if (lane == 31) misc[1 + warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w)
+        if (w < warp) wbase += misc[1 + w];
+    tbase[dd] = wbase + incl - total;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kKeysPerLane; ++j) {
+        const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
+        if (li < tile_n) {
+            const uint32_t d = rd[j] >> 16;
+            const uint32_t slot = tbase[d] + wcnt[warp * 256 + d] + (rd[j] & 0xffffu);
+            skey[slot] = keys_in[tile0 + li];
+            sval[slot] = vals_in[tile0 + li];
+        }
+    }
+    // The look-back (thread d, digit d) over the tiles before this one, after
+    // the tile-local work so that its waits overlap it.
     unsigned long long excl = 0;
-    if (tile == 0) {
-        st_relaxed64(my, lookback_word(epoch, kFlagPrefix, total));
-    } else {
-        st_relaxed64(my, lookback_word(epoch, kFlagAgg, total));
+    if (tile != 0) {
         // Look-back over the tiles before this one, kLookbackBatch words per
         // round (independent loads), newest first: add counts until a tile's
         // inclusive prefix; a word not yet published is polled (bounded).
         bool gave_up = false, done = false;
         int64_t t = (int64_t)tile - 1;
         while (!done && t >= 0) {
-            const int n = t + 1 < kLookbackBatch ? (int)(t + 1) : kLookbackBatch;
+            const int nb = t + 1 < kLookbackBatch ? (int)(t + 1) : kLookbackBatch;
             unsigned long long v[kLookbackBatch];
 #pragma unroll
             for (int k = 0; k < kLookbackBatch; ++k)
-                if (k < n) v[k] = ld_relaxed64(lookback + (size_t)(t - k) * 256 + dd);
-            int used = n;
+                if (k < nb) v[k] = ld_relaxed64(lookback + (size_t)(t - k) * 256 + dd);
+            const int used = nb;
 #pragma unroll
             for (int k = 0; k < kLookbackBatch; ++k) {
                 if (k >= used) break;
@@ -213,34 +236,13 @@ __global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
                     break;
                 }
             }
-            t -= n;
+            t -= nb;
         }
         if (gave_up && status) *(volatile uint32_t *)status = kErrSortWait;
         st_relaxed64(my, lookback_word(epoch, kFlagPrefix, excl + total));
     }
     offset[dd] = digit_base[dd] + (uint32_t)excl;
-    // 3. Exclusive scan of the tile's digit counts (a warp scan per 32
-    //    digits, then over the warps).
-    const uint32_t incl = warp_inclusive(total, lane);
-    if (lane == 31) misc[1 + warp] = incl;
-    __syncthreads();
-    uint32_t wbase = 0;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w)
-        if (w < warp) wbase += misc[1 + w];
-    tbase[dd] = wbase + incl - total;
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kKeysPerLane; ++j) {
-        const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
-        if (li < tile_n) {
-            const uint32_t d = rd[j] >> 16;
-            const uint32_t slot = tbase[d] + wcnt[warp * 256 + d] + (rd[j] & 0xffffu);
-            skey[slot] = keys_in[tile0 + li];
-            sval[slot] = vals_in[tile0 + li];
-        }
-    }
-    __syncthreads();
+    __syncthreads();  // every digit's offset; the sorted tile complete
     // 4. Coalesced runs per digit to the global output.
     for (uint32_t i = threadIdx.x; i < tile_n; i += kThreads) {
         const K k = skey[i];
