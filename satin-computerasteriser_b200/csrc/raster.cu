@@ -50,9 +50,6 @@
 #ifndef CR_DIV64
 #define CR_DIV64 0
 #endif
-#ifndef CR_TRIM_OPS
-#define CR_TRIM_OPS 0
-#endif
 #ifndef CR_TILE_PX_PER_POINT
 #define CR_TILE_PX_PER_POINT 1
 #endif
@@ -295,25 +292,17 @@ __device__ __forceinline__ void project_point(const RasterArgs &a, const ViewReg
 #else
     const float nx = clip.x / clip.w, ny = clip.y / clip.w, nz = clip.z / clip.w;
 #endif
-#if CR_TRIM_OPS
     // |x| > 1 is x < -1 || x > 1 for every float (false for NaN either way).
     if (fabsf(nx) > 1.0f || fabsf(ny) > 1.0f || nz > 1.0f) ok = false;
-#else
-    if (nx < -1.0f || ny < -1.0f || nx > 1.0f || ny > 1.0f || nz > 1.0f) ok = false;
-#endif
     if (PASS == PASS_NEAREST ? (nz <= 0.0f) : (nz < 0.0f)) ok = false;
     const int W = vw<MV>(vr), H = vh<MV>(vr);
     o.ix = (int)((nx * 0.5f + 0.5f) * (float)W);
     const int iy = (int)((ny * 0.5f + 0.5f) * (float)H);
     if (o.ix < 0 || o.ix >= W || iy < 0 || iy >= H) ok = false;
     o.iy = H - 1 - iy;
-#if CR_TRIM_OPS
     // depth_to_uint without its clamps: the saturating conversion already
     // maps z * 2^32 to 0 for z <= 0 or NaN and to 0xFFFFFFFF for z >= 1.
     o.depth = __float2uint_rz(nz * 4294967296.0f);
-#else
-    o.depth = crd::depth_to_uint(nz);
-#endif
     o.nz = nz;
     o.ok = ok;
     if (PASS == PASS_COLOR || PASS == PASS_DEPTH_FRAG) {  // ColorPass/Shaders.metal:95-100
