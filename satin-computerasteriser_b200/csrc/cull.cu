@@ -288,12 +288,6 @@ __device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-#ifndef CR_CULL_PREFETCH
-#define CR_CULL_PREFETCH 0
-#endif
-#ifndef CR_CULL_SLEEP_NS
-#define CR_CULL_SLEEP_NS 100
-#endif
 // The one-view cull in one pass: every CTA classifies its 256 slots,
 // publishes its survivor, chunk and point counts (flag = this launch's
 // epoch + 1, after a release), sums the counts of the CTAs before it and
@@ -317,7 +311,6 @@ __global__ void __launch_bounds__(kCullThreads)
     crd::grid_wait();          // the previous frame's passes have finished with the planes
     crd::launch_dependents();  // the depth pass waits for this grid itself
     __shared__ uint32_t s_ticket;
-#if CR_CULL_PREFETCH
     // Tickets mostly follow block order: start bringing this block's likely
     // batch records towards L2 while the ticket is claimed.
     {
@@ -325,7 +318,6 @@ __global__ void __launch_bounds__(kCullThreads)
         if (g < a.nbatches)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(a.batches + g));
     }
-#endif
     if (threadIdx.x == 0) s_ticket = atomicInc(a.counters + CNT_CULL_TICKET, gridDim.x - 1u);
     __syncthreads();
     const uint32_t ticket = s_ticket;
@@ -403,7 +395,7 @@ __global__ void __launch_bounds__(kCullThreads)
                 published = true;
                 break;
             }
-            __nanosleep(CR_CULL_SLEEP_NS);
+            __nanosleep(20);
         }
         if (!published) {
             gave_up = true;
