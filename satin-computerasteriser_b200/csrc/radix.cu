@@ -65,9 +65,6 @@ __device__ __forceinline__ bool lookback_ready(unsigned long long v, uint32_t ep
 #ifndef CR_LOOKBACK_BATCH
 #define CR_LOOKBACK_BATCH 8
 #endif
-#ifndef CR_SORT_KEYS_IN_REGS
-#define CR_SORT_KEYS_IN_REGS 0
-#endif
 #ifndef CR_SORT_MIN_BLOCKS
 #define CR_SORT_MIN_BLOCKS 3
 #endif
@@ -150,26 +147,11 @@ __global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
     //    (from L1 / L2) when they move.
     uint32_t rd[kKeysPerLane];
     uint32_t *wc = wcnt + warp * 256;
-#if CR_SORT_KEYS_IN_REGS
-    // All of the lane's keys are loaded before any is ranked, so the loads'
-    // latencies overlap (the ranking's warp barriers would otherwise order
-    // each load after the previous key's ranking), and kept for the move.
-    K kv[kKeysPerLane];
-#pragma unroll
-    for (int j = 0; j < kKeysPerLane; ++j) {
-        const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
-        kv[j] = li < tile_n ? keys_in[tile0 + li] : K(0);
-    }
-#endif
 #pragma unroll
     for (int j = 0; j < kKeysPerLane; ++j) {
         const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
         const bool v = li < tile_n;
-#if CR_SORT_KEYS_IN_REGS
-        const K key = kv[j];
-#else
         const K key = v ? keys_in[tile0 + li] : K(0);
-#endif
         const uint32_t d = v ? ((uint32_t)(key >> shift) & 0xffu) : 256u;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const uint32_t before = v ? wc[d] : 0u;
@@ -209,11 +191,7 @@ __global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
         if (li < tile_n) {
             const uint32_t d = rd[j] >> 16;
             const uint32_t slot = tbase[d] + wcnt[warp * 256 + d] + (rd[j] & 0xffffu);
-#if CR_SORT_KEYS_IN_REGS
-            skey[slot] = kv[j];
-#else
             skey[slot] = keys_in[tile0 + li];
-#endif
             sval[slot] = vals_in[tile0 + li];
         }
     }
