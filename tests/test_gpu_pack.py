@@ -245,3 +245,26 @@ def test_lattice_1m_pack_bit_exact(cr, orc, ctx):
     assert ref.batchCount == 98
     check_region(cloud, ref, 0, 10240, src)
     cloud.close()
+
+
+@pytest.mark.parametrize("bits", [10, 21])
+def test_constant_and_single_digit_keys(cr, orc, ctx, bits):
+    """Edge cases of the radix sort's digit skipping: every point at the same
+    position (every digit of every key the same: no pass runs, the input
+    order stands) and points that differ along one axis only (most digits
+    constant), at sizes around the 4096-key tile."""
+    for n in (1, 4095, 4096, 4097, 9000):
+        pos = np.tile(np.array([[0.25, -0.5, 1.0]], np.float32), (n, 1))
+        rgba = np.arange(n, dtype=np.uint32) | np.uint32(0xff000000)
+        ref = orc.pack(pos, colors_rgba8=rgba, pointsPerBatch=1000, morton_bits=bits)
+        cloud, src = gpu_pack(cr, ctx, pos, rgba=rgba, ppb=1000, bits=bits)
+        check_region(cloud, ref, 0, 1000, src)
+        cloud.close()
+    n = 20000
+    pos = np.zeros((n, 3), np.float32)
+    pos[:, 1] = np.random.default_rng(3).integers(0, 7, n).astype(np.float32)
+    rgba = np.arange(n, dtype=np.uint32)
+    ref = orc.pack(pos, colors_rgba8=rgba, pointsPerBatch=512, morton_bits=bits)
+    cloud, src = gpu_pack(cr, ctx, pos, rgba=rgba, ppb=512, bits=bits)
+    check_region(cloud, ref, 0, 512, src)
+    cloud.close()
