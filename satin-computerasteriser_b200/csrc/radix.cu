@@ -12,8 +12,8 @@
 //                     the rest into digit bases (exclusive scans);
 //   radix_onesweep    per pass, 4096-key tiles taken in ticket order: a tile
 //                     ranks its keys among equal digits in input order (warp
-//                     multisplit with __match_any_sync, then scans over warps
-//                     and digits), publishes its per-digit counts, sums the
+//                     multisplit with ballots, then scans over warps and
+//                     digits), publishes its per-digit counts, sums the
 //                     counts of the tiles before it per digit (look-back over
 //                     their published counts and inclusive prefixes, a
 //                     thread per digit), sorts the tile by digit in shared
@@ -34,7 +34,7 @@
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 256;  // one thread per digit in the per-digit phases
 constexpr int kWarps = kThreads / 32;
 constexpr int kKeysPerLane = 16;
 constexpr int kTileKeys = kThreads * kKeysPerLane;  // 4096
@@ -65,10 +65,11 @@ __device__ __forceinline__ bool lookback_ready(unsigned long long v, uint32_t ep
 #ifndef CR_LOOKBACK_BATCH
 #define CR_LOOKBACK_BATCH 8
 #endif
-#ifndef CR_SORT_MIN_BLOCKS
-#define CR_SORT_MIN_BLOCKS 3
-#endif
 constexpr int kLookbackBatch = CR_LOOKBACK_BATCH;  // predecessor words one round loads at once
+// Per-warp digit counts and bases (at most kTileKeys) in 16 bits: 55.4 KB of
+// shared memory and at most 64 registers let four sort CTAs share an SM.
+using WarpCount = uint16_t;
+constexpr int kSortBlocksPerSM = 4;
 
 // Histograms of every 8-bit digit of the keys (grid-stride, per-CTA shared
 // counts added to global memory once per CTA).
@@ -103,13 +104,13 @@ __device__ __forceinline__ uint32_t warp_inclusive(uint32_t x, int lane) {
 template <typename K>
 size_t onesweep_smem_bytes() {
     return (size_t)kTileKeys * (sizeof(K) + sizeof(uint32_t)) +
-           ((size_t)kWarps * 256 + 256 + 256 + 32) * sizeof(uint32_t);
+           (size_t)kWarps * 256 * sizeof(WarpCount) + (256 + 256 + 32) * sizeof(uint32_t);
 }
 
 // One pass: a tile of kTileKeys keys per CTA, in ticket order.
 //   1. each warp takes 512 consecutive keys, 16 per lane in warp-striped order
-//      (key j*32 + lane), and ranks them among equal digits with
-//      __match_any_sync against running per-warp digit counts, in input order;
+//      (key j*32 + lane), and ranks them among equal digits (peer lanes found
+//      by ballots) against running per-warp digit counts, in input order;
 //   2. thread d: the tile's count of digit d (published at once) and the
 //      exclusive bases of the warps;
 //   3. exclusive scan over the digits gives each key its slot in a tile
@@ -120,7 +121,7 @@ size_t onesweep_smem_bytes() {
 //      digit's global offset: keys of one digit are consecutive in shared
 //      memory and land at consecutive addresses (coalesced runs).
 template <typename K>
-__global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, kSortBlocksPerSM)
     radix_onesweep(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                    K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, uint64_t n,
                    int shift, const uint32_t *__restrict__ digit_base,
@@ -129,8 +130,10 @@ __global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
     extern __shared__ __align__(16) unsigned char smem[];
     K *skey = reinterpret_cast<K *>(smem);
     uint32_t *sval = reinterpret_cast<uint32_t *>(skey + kTileKeys);
-    uint32_t *wcnt = sval + kTileKeys;       // [kWarps][256]: counts, then warp bases
-    uint32_t *offset = wcnt + kWarps * 256;  // global offset of the tile's run of each digit
+    // [kWarps][256]: per-warp digit counts, then the warps' digit bases.
+    WarpCount *wcnt = reinterpret_cast<WarpCount *>(sval + kTileKeys);
+    // Global offset of the tile's run of each digit.
+    uint32_t *offset = reinterpret_cast<uint32_t *>(wcnt + kWarps * 256);
     uint32_t *tbase = offset + 256;          // tile-local digit base
     uint32_t *misc = tbase + 256;            // [0] ticket, [1..8] warp sums of the digit scan
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -146,18 +149,27 @@ __global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
     //    (< 512) and digit are kept packed, the key and value are read again
     //    (from L1 / L2) when they move.
     uint32_t rd[kKeysPerLane];
-    uint32_t *wc = wcnt + warp * 256;
+    WarpCount *wc = wcnt + warp * 256;
 #pragma unroll
     for (int j = 0; j < kKeysPerLane; ++j) {
         const uint32_t li = (uint32_t)warp * (32 * kKeysPerLane) + (uint32_t)j * 32 + lane;
         const bool v = li < tile_n;
         const K key = v ? keys_in[tile0 + li] : K(0);
         const uint32_t d = v ? ((uint32_t)(key >> shift) & 0xffu) : 256u;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        // Lanes with the same digit (9 bits: the digit and the no-key flag):
+        // the intersection, over the bits, of the lanes that agree with this
+        // lane's bit.  (Nine ballots cost less than __match_any_sync when a
+        // warp holds many distinct digits.)
+        uint32_t peers = 0xffffffffu;
+#pragma unroll
+        for (int b = 0; b < 9; ++b) {
+            const uint32_t m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? m : ~m;
+        }
         const uint32_t before = v ? wc[d] : 0u;
         rd[j] = (before + __popc(peers & lt)) | (d << 16);
         __syncwarp();
-        if (v && (peers & lt) == 0u) wc[d] = before + __popc(peers);
+        if (v && (peers & lt) == 0u) wc[d] = (WarpCount)(before + __popc(peers));
         __syncwarp();
     }
     __syncthreads();
@@ -167,7 +179,7 @@ __global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
         const uint32_t c = wcnt[w * 256 + dd];
-        wcnt[w * 256 + dd] = total;
+        wcnt[w * 256 + dd] = (WarpCount)total;
         total += c;
     }
     unsigned long long *my = lookback + (size_t)tile * 256 + dd;
@@ -202,41 +214,51 @@ __global__ void __launch_bounds__(kThreads, CR_SORT_MIN_BLOCKS)
         // Look-back over the tiles before this one, kLookbackBatch words per
         // round (independent loads), newest first: add counts until a tile's
         // inclusive prefix; a word not yet published is polled (bounded).
-        bool gave_up = false, done = false;
+        constexpr unsigned long long kCountMask = (1ull << 46) - 1ull;
+        bool gave_up = false;
         int64_t t = (int64_t)tile - 1;
-        while (!done && t >= 0) {
+        while (t >= 0) {
             const int nb = t + 1 < kLookbackBatch ? (int)(t + 1) : kLookbackBatch;
             unsigned long long v[kLookbackBatch];
 #pragma unroll
             for (int k = 0; k < kLookbackBatch; ++k)
                 if (k < nb) v[k] = ld_relaxed64(lookback + (size_t)(t - k) * 256 + dd);
-            const int used = nb;
+            // Add the batch's counts up to the first inclusive prefix (pf)
+            // or the first word not yet published (nr).
+            int nr = -1;
+            bool pf = false;
 #pragma unroll
             for (int k = 0; k < kLookbackBatch; ++k) {
-                if (k >= used) break;
-                if (!lookback_ready(v[k], epoch)) {
-                    // Poll this predecessor, then carry on from it.
-                    const unsigned long long *w = lookback + (size_t)(t - k) * 256 + dd;
-                    uint32_t polls = 0;
-                    unsigned long long x = ld_relaxed64(w);
-                    while (!lookback_ready(x, epoch) && ++polls < kLookbackLimit) {
-                        __nanosleep(32);
-                        x = ld_relaxed64(w);
+                if (k < nb && nr < 0 && !pf) {
+                    if (!lookback_ready(v[k], epoch)) {
+                        nr = k;
+                    } else {
+                        excl += v[k] & kCountMask;
+                        pf = ((v[k] >> 46) & 3ull) == kFlagPrefix;
                     }
-                    if (!lookback_ready(x, epoch)) {
-                        gave_up = true;
-                        done = true;
-                        break;
-                    }
-                    v[k] = x;
-                }
-                excl += v[k] & ((1ull << 46) - 1);
-                if (((v[k] >> 46) & 3ull) == kFlagPrefix) {
-                    done = true;
-                    break;
                 }
             }
-            t -= nb;
+            if (pf) break;
+            if (nr < 0) {
+                t -= nb;
+                continue;
+            }
+            // Poll the unpublished predecessor, then carry on from the one
+            // before it.
+            const unsigned long long *w = lookback + (size_t)(t - nr) * 256 + dd;
+            uint32_t polls = 0;
+            unsigned long long x = ld_relaxed64(w);
+            while (!lookback_ready(x, epoch) && ++polls < kLookbackLimit) {
+                __nanosleep(32);
+                x = ld_relaxed64(w);
+            }
+            if (!lookback_ready(x, epoch)) {
+                gave_up = true;
+                break;
+            }
+            excl += x & kCountMask;
+            if (((x >> 46) & 3ull) == kFlagPrefix) break;
+            t -= nr + 1;
         }
         if (gave_up && status) *(volatile uint32_t *)status = kErrSortWait;
         st_relaxed64(my, lookback_word(epoch, kFlagPrefix, excl + total));

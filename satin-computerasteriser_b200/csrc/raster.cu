@@ -40,6 +40,7 @@
 // predicated single instructions rather than branches around code.
 // Integer max and sum are associative and commutative: the planes are
 // bit-identical to a per-point atomic order either way.
+#include "cr_bulk.cuh"
 #include "cr_device.cuh"
 #include "cr_internal.h"
 #include "cr_resolve.cuh"
@@ -740,41 +741,10 @@ constexpr uint32_t kStageWaitLimit = 1u << 16;  // polls of an mbarrier before g
 __device__ __forceinline__ bool stage_ok(uint32_t first, uint32_t count) {
     return (first & 15u) == 0u && count <= kStagePoints && count > 0u;
 }
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
-                                         uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-// Bounded wait for the mbarrier phase `parity`; false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
-    for (uint32_t i = 0; i < limit; ++i) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(smem_u32(bar)), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
+using crb::bulk_g2s;
+using crb::mbar_expect_tx;
+using crb::mbar_init;
+using crb::mbar_wait;
 // Thread 0: the bulk copies of one chunk's level bytes, coarse words and
 // colours into a stage buffer, completing on `bar`.
 __device__ __forceinline__ void stage_issue(unsigned char *stage, uint64_t *bar,
@@ -782,7 +752,7 @@ __device__ __forceinline__ void stage_issue(unsigned char *stage, uint64_t *bar,
                                             const uint32_t *colors, uint32_t first,
                                             uint32_t count) {
     const uint32_t nl = (count + 15u) & ~15u, nw = ((count + 3u) & ~3u) * 4u;
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    crb::fence_proxy_async_smem();
     mbar_expect_tx(bar, nl + 2u * nw);
     bulk_g2s(stage, levels + first, nl, bar);
     bulk_g2s(stage + kStagePoints, low + first, nw, bar);
@@ -920,7 +890,7 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
     if (kStage && threadIdx.x == 0) {
         mbar_init(&s_mbar[0], 1u);
         mbar_init(&s_mbar[1], 1u);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        crb::mbar_init_fence();
     }
     if (threadIdx.x == 0) {
         claim(0);
