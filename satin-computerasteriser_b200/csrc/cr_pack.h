@@ -20,13 +20,15 @@ struct RadixScratch {
 void radix_scratch_free(RadixScratch &r);
 
 // Stable sort of n (key, value) pairs by the low key_bits bits of the keys;
-// the result is in (keys_alt, vals_alt) when *result_in_alt.  Synchronises
-// once (the histograms are read back to skip constant digits).  A bounded
-// wait that gives up stores kErrSortWait into *status.
+// the result is in (keys_alt, vals_alt) when *result_in_alt.  With
+// vals_iota the values are the keys' input positions and `vals` is not read
+// (the first pass makes them).  Synchronises once (the histograms are read
+// back to skip constant digits).  A bounded wait that gives up stores
+// kErrSortWait into *status.
 template <typename K>
 cr_status radix_sort_pairs(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, uint64_t n,
-                           int key_bits, RadixScratch &rs, uint32_t *status, int sm_count,
-                           cudaStream_t s, bool *result_in_alt);
+                           int key_bits, bool vals_iota, RadixScratch &rs, uint32_t *status,
+                           int sm_count, cudaStream_t s, bool *result_in_alt);
 
 // Grow-only device scratch of the packer, owned by the context (the
 // reference's PackScratch, GPUPacker.swift:453-484).

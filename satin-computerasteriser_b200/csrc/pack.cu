@@ -8,7 +8,8 @@
 //   2 morton        10 bits/axis (30-bit key) or 21 bits/axis (63-bit key)
 //   3 sort          stable LSD radix of (key, input index), one read of the
 //                   keys for every digit's histogram, then one single-sweep
-//                   pass per digit (decoupled look-back)         [radix.cu]
+//                   pass per digit (decoupled look-back; the first pass
+//                   makes the input indices)                     [radix.cu]
 //   4 gather        positions in Morton order, levels = maxLevel
 //   5 LOD           per level, coarsest first: dense voxel grid, atomicMin
 //                   of the Morton position claims a voxel for the first
@@ -16,9 +17,10 @@
 //                   to occupy an empty voxel"); the claims of a level ride
 //                   in the kernel before (the gather, or the previous
 //                   level's assignment)
-//   6 batches       one CTA per batch: AABB, level histogram, stable
-//                   level-ascending scatter (warp ballots), RasterBatch with
-//                   the cumulative LOD counts
+//   6 batches       one CTA per batch, a contiguous segment per warp:
+//                   AABB, level counts, stable level-ascending scatter (warp
+//                   ballots, no block barrier), RasterBatch with the
+//                   cumulative LOD counts
 //   7 emit          gather in final order, 30-bit quantisation into three
 //                   10-bit/axis words, colours, levels, source indices.
 // Host-side float math (scale, voxel sizes, grid dims) is compiled without
@@ -140,11 +142,12 @@ struct MortonArgs {
     float top;
 };
 
-// Stage 2: Morton key + identity index (packMorton, GPUPacker/Shaders.metal:109-126).
+// Stage 2: Morton key (packMorton, GPUPacker/Shaders.metal:109-126); the
+// identity index the reference writes beside it is made by the sort's first
+// pass instead.
 template <typename K>
 __global__ void __launch_bounds__(kThreads)
-    pack_morton(const float4 *__restrict__ pos, uint64_t n, MortonArgs m, K *__restrict__ keys,
-                uint32_t *__restrict__ idx) {
+    pack_morton(const float4 *__restrict__ pos, uint64_t n, MortonArgs m, K *__restrict__ keys) {
     const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
     const float4 p = pos[i];
@@ -155,7 +158,6 @@ __global__ void __launch_bounds__(kThreads)
         keys[i] = (K)((spread21(qx) << 2) | (spread21(qy) << 1) | spread21(qz));
     else
         keys[i] = (K)((spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz));
-    idx[i] = (uint32_t)i;
 }
 
 // Stage 4: gather into Morton order, all levels at maxLevel (packLODInit).
@@ -249,53 +251,98 @@ __global__ void __launch_bounds__(kThreads)
 
 // Stage 6: per batch AABB + stable level bucketing + RasterBatch
 // (packBatchAABB + packBucketLOD, GPUPacker/Shaders.metal:243-284, 383-414).
+// One CTA per batch; each warp owns a contiguous segment of the batch's
+// points.  Pass 1: the AABB and the warp's per-level counts (ballots).  The
+// counts give every warp its first slot per level (the batch's exclusive
+// level prefix plus the counts of the warps before it), so pass 2 needs no
+// block barrier: each warp walks its segment in order, 32 points a round,
+// placing each point after the earlier points of its level (ballot rank).
+// Both passes load four rounds ahead.
+constexpr int kBatchRounds = 4;
 __global__ void __launch_bounds__(kThreads)
     pack_batches(const float4 *__restrict__ sorted, const uint8_t *__restrict__ lv, uint64_t n,
                  uint32_t ppb, uint32_t first_slot, cr_raster_batch *__restrict__ batches,
                  uint32_t *__restrict__ perm, uint8_t *__restrict__ lv_out) {
-    __shared__ uint32_t red[6][kThreads / 32];
-    __shared__ uint32_t cnt[8];
-    __shared__ uint32_t running[8];
-    __shared__ uint32_t wl[kThreads / 32][8];
+    constexpr int kWarps = kThreads / 32;
+    constexpr unsigned kFull = 0xffffffffu;
+    __shared__ uint32_t red[6][kWarps];
+    __shared__ uint32_t wcnt[kWarps][8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
     const uint64_t start = (uint64_t)blockIdx.x * ppb;
     const uint64_t end = (start + ppb < n) ? start + ppb : n;
-    if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
-    __syncthreads();
+    const uint32_t total = (uint32_t)(end - start);
+    const uint32_t seg = (total + kWarps - 1u) / kWarps;
+    const uint64_t s0 = start + min((uint64_t)total, (uint64_t)warp * seg);
+    const uint64_t s1 = start + min((uint64_t)total, (uint64_t)(warp + 1) * seg);
+    // 1. AABB and level counts of the warp's segment.
     uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
-    for (uint64_t i = start + threadIdx.x; i < end; i += kThreads) {
-        const float4 p = sorted[i];
-        const uint32_t f[3] = {flip(p.x), flip(p.y), flip(p.z)};
+    uint32_t c[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+    for (uint64_t r0 = s0; r0 < s1; r0 += 32u * kBatchRounds) {
+        float4 p[kBatchRounds];
+        uint32_t l[kBatchRounds];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            mn[k] = min(mn[k], f[k]);
-            mx[k] = max(mx[k], f[k]);
+        for (int k = 0; k < kBatchRounds; ++k) {
+            const uint64_t i = r0 + 32u * k + lane;
+            l[k] = i < s1 ? (lv[i] & 7u) : 8u;
+            p[k] = i < s1 ? sorted[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        atomicAdd(&cnt[lv[i] & 7u], 1u);
+#pragma unroll
+        for (int k = 0; k < kBatchRounds; ++k) {
+            if (l[k] < 8u) {
+                const uint32_t f[3] = {flip(p[k].x), flip(p[k].y), flip(p[k].z)};
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    mn[a] = min(mn[a], f[a]);
+                    mx[a] = max(mx[a], f[a]);
+                }
+            }
+#pragma unroll
+            for (int L = 0; L < 8; ++L) c[L] += __popc(__ballot_sync(kFull, l[k] == (uint32_t)L));
+        }
     }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const uint32_t a = __reduce_min_sync(0xffffffffu, mn[k]);
-        const uint32_t b = __reduce_max_sync(0xffffffffu, mx[k]);
+    for (int a = 0; a < 3; ++a) {
+        const uint32_t x = __reduce_min_sync(kFull, mn[a]);
+        const uint32_t y = __reduce_max_sync(kFull, mx[a]);
         if (lane == 0) {
-            red[k][warp] = a;
-            red[3 + k][warp] = b;
+            red[a][warp] = x;
+            red[3 + a][warp] = y;
         }
+    }
+    if (lane < 8) {
+        uint32_t mine = 0;
+#pragma unroll
+        for (int L = 0; L < 8; ++L)
+            if (lane == L) mine = c[L];
+        wcnt[warp][lane] = mine;
     }
     __syncthreads();
+    // 2. This warp's first slot (from the batch start) per level.
+    uint32_t run[8], cum[8];
+    {
+        uint32_t acc = 0;
+#pragma unroll
+        for (int L = 0; L < 8; ++L) {
+            uint32_t tot = 0, before = 0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) {
+                const uint32_t x = wcnt[w][L];
+                tot += x;
+                if (w < warp) before += x;
+            }
+            run[L] = acc + before;
+            acc += tot;
+            cum[L] = acc;
+        }
+    }
     if (threadIdx.x == 0) {
         uint32_t m[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-        for (int w = 0; w < kThreads / 32; ++w)
-            for (int k = 0; k < 3; ++k) {
-                m[k] = min(m[k], red[k][w]);
-                m[3 + k] = max(m[3 + k], red[3 + k][w]);
+        for (int w = 0; w < kWarps; ++w)
+            for (int a = 0; a < 3; ++a) {
+                m[a] = min(m[a], red[a][w]);
+                m[3 + a] = max(m[3 + a], red[3 + a][w]);
             }
-        uint32_t cum[8], acc = 0;
-        for (int l = 0; l < 8; ++l) {
-            running[l] = acc;
-            acc += cnt[l];
-            cum[l] = acc;
-        }
         cr_raster_batch rb;
         rb.state = 1;
         rb.minX = unflip(m[0]);
@@ -304,7 +351,7 @@ __global__ void __launch_bounds__(kThreads)
         rb.maxX = unflip(m[3]);
         rb.maxY = unflip(m[4]);
         rb.maxZ = unflip(m[5]);
-        rb.numPoints = (uint32_t)(end - start);
+        rb.numPoints = total;
         rb.firstPoint = (first_slot + blockIdx.x) * ppb;
         rb.fileIndex = 0;
         rb.lodCum01 = cum[0] | (cum[1] << 16);
@@ -315,36 +362,31 @@ __global__ void __launch_bounds__(kThreads)
         rb.padding8 = 0;
         batches[blockIdx.x] = rb;
     }
-    __syncthreads();
-    const uint32_t lt = (1u << lane) - 1u;
-    for (uint64_t r0 = start; r0 < end; r0 += kThreads) {
-        const uint64_t i = r0 + threadIdx.x;
-        const bool v = i < end;
-        const uint32_t l = v ? (lv[i] & 7u) : 8u;
-        uint32_t my_rank = 0;
+    // 3. Stable bucketing of the warp's segment.
+    for (uint64_t r0 = s0; r0 < s1; r0 += 32u * kBatchRounds) {
+        uint32_t raw[kBatchRounds];
 #pragma unroll
-        for (uint32_t L = 0; L < 8; ++L) {
-            const uint32_t b = __ballot_sync(0xffffffffu, l == L);
-            if (lane == 0) wl[warp][L] = __popc(b);
-            if (l == L) my_rank = __popc(b & lt);
+        for (int k = 0; k < kBatchRounds; ++k) {
+            const uint64_t i = r0 + 32u * k + lane;
+            raw[k] = i < s1 ? (uint32_t)lv[i] : 0xffu;
         }
-        __syncthreads();
-        if (v) {
-            uint32_t before = running[l];
-            for (int w = 0; w < warp; ++w) before += wl[w][l];
-            const uint64_t dst = start + before + my_rank;
-            if (dst < end) {  // always true: the ranks come from the same levels
-                perm[dst] = (uint32_t)i;
-                lv_out[dst] = lv[i];
+#pragma unroll
+        for (int k = 0; k < kBatchRounds; ++k) {
+            const uint64_t i = r0 + 32u * k + lane;
+            const bool v = i < s1;
+            const uint32_t l = v ? (raw[k] & 7u) : 8u;
+            uint32_t dst = 0;
+#pragma unroll
+            for (int L = 0; L < 8; ++L) {
+                const uint32_t b = __ballot_sync(kFull, l == (uint32_t)L);
+                if (l == (uint32_t)L) dst = run[L] + __popc(b & lt);
+                run[L] += __popc(b);
+            }
+            if (v && dst < total) {  // always true: the ranks come from the same levels
+                perm[start + dst] = (uint32_t)i;
+                lv_out[start + dst] = (uint8_t)raw[k];
             }
         }
-        __syncthreads();
-        if (threadIdx.x < 8) {
-            uint32_t s = 0;
-            for (int w = 0; w < kThreads / 32; ++w) s += wl[w][threadIdx.x];
-            running[threadIdx.x] += s;
-        }
-        __syncthreads();
     }
 }
 
@@ -527,18 +569,17 @@ cr_status pack_run(cr_context *ctx, cr_cloud *cloud, const cr_pack_input *in, ui
     if (wide) {
         auto *k0 = static_cast<unsigned long long *>(sc.keys[0]);
         auto *k1 = static_cast<unsigned long long *>(sc.keys[1]);
-        pack_morton<unsigned long long><<<grid_for(count), kThreads, 0, s>>>(pos, count, ma, k0,
-                                                                             sc.idx[0]);
+        pack_morton<unsigned long long><<<grid_for(count), kThreads, 0, s>>>(pos, count, ma, k0);
         CR_CUDA(cudaGetLastError());
-        st = radix_sort_pairs<unsigned long long>(k0, sc.idx[0], k1, sc.idx[1], count, 63,
+        st = radix_sort_pairs<unsigned long long>(k0, sc.idx[0], k1, sc.idx[1], count, 63, true,
                                                   sc.radix, ctx->d_status, ctx->sm_count, s,
                                                   &in_alt);
     } else {
         auto *k0 = static_cast<uint32_t *>(sc.keys[0]);
         auto *k1 = static_cast<uint32_t *>(sc.keys[1]);
-        pack_morton<uint32_t><<<grid_for(count), kThreads, 0, s>>>(pos, count, ma, k0, sc.idx[0]);
+        pack_morton<uint32_t><<<grid_for(count), kThreads, 0, s>>>(pos, count, ma, k0);
         CR_CUDA(cudaGetLastError());
-        st = radix_sort_pairs<uint32_t>(k0, sc.idx[0], k1, sc.idx[1], count, 30, sc.radix,
+        st = radix_sort_pairs<uint32_t>(k0, sc.idx[0], k1, sc.idx[1], count, 30, true, sc.radix,
                                         ctx->d_status, ctx->sm_count, s, &in_alt);
     }
     if (st) return st;

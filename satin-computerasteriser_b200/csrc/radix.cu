@@ -91,6 +91,12 @@ __global__ void __launch_bounds__(kThreads)
         if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
+// The values of a sort that ran no pass: their input positions.
+__global__ void __launch_bounds__(kThreads) radix_iota(uint32_t *__restrict__ vals, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (i < n) vals[i] = (uint32_t)i;
+}
+
 // Inclusive warp scan.
 __device__ __forceinline__ uint32_t warp_inclusive(uint32_t x, int lane) {
 #pragma unroll
@@ -120,7 +126,7 @@ size_t onesweep_smem_bytes() {
 //   4. threads read the sorted tile in order and write each key to its
 //      digit's global offset: keys of one digit are consecutive in shared
 //      memory and land at consecutive addresses (coalesced runs).
-template <typename K>
+template <typename K, bool kIota>
 __global__ void __launch_bounds__(kThreads, kSortBlocksPerSM)
     radix_onesweep(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                    K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, uint64_t n,
@@ -204,7 +210,7 @@ __global__ void __launch_bounds__(kThreads, kSortBlocksPerSM)
             const uint32_t d = rd[j] >> 16;
             const uint32_t slot = tbase[d] + wcnt[warp * 256 + d] + (rd[j] & 0xffffu);
             skey[slot] = keys_in[tile0 + li];
-            sval[slot] = vals_in[tile0 + li];
+            sval[slot] = kIota ? (uint32_t)(tile0 + li) : vals_in[tile0 + li];
         }
     }
     // The look-back (thread d, digit d) over the tiles before this one, after
@@ -288,10 +294,13 @@ void radix_scratch_free(RadixScratch &r) {
 
 template <typename K>
 cr_status radix_sort_pairs(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, uint64_t n,
-                           int key_bits, RadixScratch &rs, uint32_t *status, int sm_count,
-                           cudaStream_t s, bool *result_in_alt) {
+                           int key_bits, bool vals_iota, RadixScratch &rs, uint32_t *status,
+                           int sm_count, cudaStream_t s, bool *result_in_alt) {
     *result_in_alt = false;
-    if (n <= 1) return CR_OK;
+    if (n <= 1) {
+        if (vals_iota && n == 1) CR_CUDA(cudaMemsetAsync(vals, 0, sizeof(uint32_t), s));
+        return CR_OK;
+    }
     if (n >= (1ull << 32)) return cri::fail(CR_ERR_CAPACITY, "radix sort: at most 2^32 - 1 keys");
     const int passes = (key_bits + 7) / 8;
     const uint64_t ntiles = (n + kTileKeys - 1) / kTileKeys;
@@ -333,8 +342,12 @@ cr_status radix_sort_pairs(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_
     CR_CUDA(cudaMemcpyAsync(rs.bases, bases.data(), passes * 256 * sizeof(uint32_t),
                             cudaMemcpyHostToDevice, s));
     const size_t smem = onesweep_smem_bytes<K>();
-    CR_CUDA(cudaFuncSetAttribute(radix_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
+    for (auto *f : {radix_onesweep<K, false>, radix_onesweep<K, true>})
+        CR_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (run.empty() && vals_iota) {
+        radix_iota<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(vals, n);
+        CR_CUDA(cudaGetLastError());
+    }
     K *kin = keys, *kout = keys_alt;
     uint32_t *vin = vals, *vout = vals_alt;
     for (int p : run) {
@@ -345,9 +358,12 @@ cr_status radix_sort_pairs(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_
                                     rs.cap_tiles * 256 * sizeof(unsigned long long), s));
             rs.epoch = 1;
         }
-        radix_onesweep<K><<<(unsigned)ntiles, kThreads, smem, s>>>(
-            kin, vin, kout, vout, n, 8 * p, rs.bases + p * 256, rs.lookback, rs.epoch,
-            rs.tiles + p, status);
+        // The first pass of an index sort makes the indices (kIota).
+        auto *kern = vals_iota && p == run.front() ? radix_onesweep<K, true>
+                                                   : radix_onesweep<K, false>;
+        kern<<<(unsigned)ntiles, kThreads, smem, s>>>(kin, vin, kout, vout, n, 8 * p,
+                                                     rs.bases + p * 256, rs.lookback, rs.epoch,
+                                                     rs.tiles + p, status);
         CR_CUDA(cudaGetLastError());
         std::swap(kin, kout);
         std::swap(vin, vout);
@@ -357,9 +373,9 @@ cr_status radix_sort_pairs(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_
 }
 
 template cr_status radix_sort_pairs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *,
-                                              uint64_t, int, RadixScratch &, uint32_t *, int,
-                                              cudaStream_t, bool *);
+                                              uint64_t, int, bool, RadixScratch &, uint32_t *,
+                                              int, cudaStream_t, bool *);
 template cr_status radix_sort_pairs<unsigned long long>(unsigned long long *, uint32_t *,
                                                         unsigned long long *, uint32_t *, uint64_t,
-                                                        int, RadixScratch &, uint32_t *, int,
+                                                        int, bool, RadixScratch &, uint32_t *, int,
                                                         cudaStream_t, bool *);
