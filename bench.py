@@ -525,6 +525,13 @@ def run_ours(args, dist):
                 "bytes_per_launch": int(dom_bytes.mean()),
                 "launch_ms": round(float(dom_ms.mean()), 4),
                 "traffic": ncu_traffic(config_dict(args)["workload"], PASS_NAMES[dom])}
+    # The whole frame against the same peak: both point passes' algorithmic
+    # bytes plus 48 B per pixel (clear 20, resolve read 20, RGBA8 write 4,
+    # float depth write 4) over the device-timed frame.
+    frame_bytes = float((b_depth + b_color).mean()) + 48.0 * W * H
+    frame_gbs = frame_bytes / (ms_max / len(timed) / 1e3) / 1e9
+    roofline["frame"] = {"bytes_per_frame": int(frame_bytes), "achieved": round(frame_gbs, 1),
+                         "frac": round(frame_gbs / peak, 4)}
     # The instruction-issue bound and the L2 atomic rate of the same kernel,
     # from its small-case ncu capture (instructions per survivor point, the
     # fraction of the SMs' issue slots used, L2 reduction/atomic throughput
