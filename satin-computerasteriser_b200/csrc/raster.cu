@@ -546,13 +546,56 @@ __device__ __forceinline__ void emit_fragment(const RasterArgs &a, uint32_t fbas
     }
 }
 
+// A point's fragment, held back so that several points of a thread are
+// appended with one shared-memory atomic per warp.  Two points per atomic:
+// the one-view depth pass 212 -> 207 µs on the 100M-point 1080p frames;
+// four spill registers and were slower, and so does the batched-view kernel
+// with two.
+struct Frag {
+    bool keep;
+    uint32_t xy;
+    float z;
+    uint32_t col;
+};
+#ifndef CR_FRAG_BATCH
+#define CR_FRAG_BATCH 2
+#endif
+
+// Appends N fragments per lane: one ballot per fragment, one atomic per warp.
+template <int N>
+__device__ __forceinline__ void emit_fragments(const RasterArgs &a, uint32_t fbase,
+                                               const Frag (&f)[N]) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t b[N], tot = 0;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        b[k] = __ballot_sync(kFull, f[k].keep);
+        tot += __popc(b[k]);
+    }
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&s_frag_count, tot);
+    base = __shfl_sync(kFull, base, 0);
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        if (f[k].keep) {
+            const uint32_t i = fbase + base + __popc(b[k] & lt);
+            a.frag_xy[i] = f[k].xy;
+            a.frag_z[i] = f[k].z;
+            a.frag_col[i] = f[k].col;
+        }
+        base += __popc(b[k]);
+    }
+}
+
 // One point; every lane of the warp calls this (warp-uniform early outs).
+// With fo, the depth pass's fragment is returned there instead of appended.
 template <int PASS, bool MV>
 __device__ __forceinline__ void do_point(const RasterArgs &a, const ViewRegsT<MV> &vr, const BatchShared &sb,
                                          unsigned char *smem, const ChunkRec &c, bool tiled,
                                          bool valid, uint32_t local, uint32_t lvl, uint32_t lo,
                                          uint32_t me, uint32_t hi, uint32_t color, uint32_t fbase,
-                                         bool emit, bool all_keep) {
+                                         bool emit, bool all_keep, Frag *fo = nullptr) {
     PointOut o;
     o.pointIndex = c.first + local;
     o.color = color;
@@ -571,7 +614,16 @@ __device__ __forceinline__ void do_point(const RasterArgs &a, const ViewRegsT<MV
         emit_tile<PASS, MV>(a, vr, c, smem, o);
     else
         emit_direct<PASS, MV>(a, vr, o);
-    if (PASS == PASS_DEPTH_FRAG && emit) emit_fragment(a, fbase, o);
+    if (PASS == PASS_DEPTH_FRAG && emit) {
+        if (fo) {
+            fo->keep = o.ok && !o.doomed;
+            fo->xy = (uint32_t)o.ix | ((uint32_t)o.iy << 16);
+            fo->z = o.nz;
+            fo->col = o.color;
+        } else {
+            emit_fragment(a, fbase, o);
+        }
+    }
 }
 
 // One fragment of the colour pass (PASS_COLOR_FRAG); every lane calls this.
@@ -1026,6 +1078,26 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                         co4 = __ldg(reinterpret_cast<const uint4 *>(a.colors + base));
                 }
                 const uint32_t l0 = 4u * q;
+                if (CR_FRAG_BATCH > 1 && PASS == PASS_DEPTH_FRAG && !MV && emit) {
+                    // The fragments of CR_FRAG_BATCH points per atomic (one
+                    // view: the batched-view kernel has no registers to
+                    // spare for them).
+                    constexpr int kB = CR_FRAG_BATCH > 1 ? CR_FRAG_BATCH : 1;
+                    Frag f[kB];
+                    const uint32_t lvs[4] = {lv4 & 0xffu, (lv4 >> 8) & 0xffu, (lv4 >> 16) & 0xffu,
+                                             lv4 >> 24};
+                    const uint32_t los[4] = {lo4.x, lo4.y, lo4.z, lo4.w};
+                    const uint32_t mes[4] = {me4.x, me4.y, me4.z, me4.w};
+                    const uint32_t his[4] = {hi4.x, hi4.y, hi4.z, hi4.w};
+                    const uint32_t cos[4] = {co4.x, co4.y, co4.z, co4.w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + j < c.count,
+                                           l0 + j, lvs[j], los[j], mes[j], his[j], cos[j], fbase,
+                                           emit, all_keep, &f[j % kB]);
+                        if (j % kB == kB - 1) emit_fragments<kB>(a, fbase, f);
+                    }
+                } else {
                 do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 0 < c.count, l0 + 0,
                                lv4 & 0xffu, lo4.x, me4.x, hi4.x, co4.x, fbase, emit, all_keep);
                 do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 1 < c.count, l0 + 1,
@@ -1034,6 +1106,7 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                                (lv4 >> 16) & 0xffu, lo4.z, me4.z, hi4.z, co4.z, fbase, emit, all_keep);
                 do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 3 < c.count, l0 + 3,
                                lv4 >> 24, lo4.w, me4.w, hi4.w, co4.w, fbase, emit, all_keep);
+                }
             }
         } else {
             // Unaligned start (pointsPerBatch not a multiple of 4): one point per thread.
