@@ -97,8 +97,7 @@ void free_cloud_buffers(cr_cloud *c) {
     dfree(c->d_chunks);
     c->chunk_cap = 0;
     dfree(c->d_frag_xy);
-    dfree(c->d_frag_z);
-    dfree(c->d_frag_col);
+    dfree(c->d_frag_zc);
     dfree(c->d_frag_count);
     dfree(c->d_counters);
     dfree(c->d_disp);
@@ -229,8 +228,7 @@ cr_status allocate_cloud(cr_cloud *c, cr_capacity cap, const cr_raster_file *fil
     c->chunk_cap = chunk_capacity(cap, kMinChunkPoints);
     if ((st = dalloc(&c->d_chunks, c->chunk_cap * sizeof(ChunkRec))) ||
         (st = dalloc(&c->d_frag_count, c->chunk_cap * sizeof(uint32_t))) ||
-        (st = dalloc(&c->d_frag_xy, pts * 4)) || (st = dalloc(&c->d_frag_z, pts * 4)) ||
-        (st = dalloc(&c->d_frag_col, pts * 4)))
+        (st = dalloc(&c->d_frag_xy, pts * 4)) || (st = dalloc(&c->d_frag_zc, pts * 8)))
         return st;
     c->d_files_cap = (uint32_t)c->files.size();
     if ((st = dalloc(&c->d_files, c->d_files_cap * sizeof(cr_raster_file)))) return st;

@@ -195,8 +195,7 @@ struct cr_cloud {
     // Fragments of the last depth pass, in pool point index space: a chunk
     // starting at point p keeps its n kept points compacted at [p, p + n).
     uint32_t *d_frag_xy = nullptr;     // pixel x | row << 16
-    float *d_frag_z = nullptr;         // NDC z
-    uint32_t *d_frag_col = nullptr;    // RGBA8 (after the colorize options)
+    uint2 *d_frag_zc = nullptr;        // NDC z bits, RGBA8 (after the colorize options)
     uint32_t *d_frag_count = nullptr;  // kept points per chunk record
     // Per-point float4 attributes of the colour variants, written by user
     // kernels (lazy, zeroed on allocation): displacement, the previous
@@ -437,8 +436,7 @@ static_assert(sizeof(ViewDesc) == 192, "ViewDesc is 192 bytes");
 // pass when the spans exceed cap (the colour pass then decodes the points).
 struct ViewsFragments {
     uint32_t *xy;
-    float *z;
-    uint32_t *col;
+    uint2 *zc;
     uint32_t *count;
     const uint32_t *poff;
     unsigned long long cap;

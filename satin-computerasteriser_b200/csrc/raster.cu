@@ -115,9 +115,8 @@ struct RasterArgs {
     float keep_scale;  // 1 - depthTolerance
     int radius_zero;   // every footprint is a single pixel
     int use_tiles;
-    uint32_t *frag_xy;
-    float *frag_z;
-    uint32_t *frag_col;
+    uint32_t *frag_xy;  // pixel x | row << 16
+    uint2 *frag_zc;     // NDC z bits, RGBA8: two stores per fragment
     uint32_t *frag_count;
     // Differentiable colours: learnable colours, dL/dpixel, gradient (3 floats each).
     const float *fcolors;
@@ -541,8 +540,7 @@ __device__ __forceinline__ void emit_fragment(const RasterArgs &a, uint32_t fbas
     if (keep) {
         const uint32_t i = fbase + base + __popc(ballot & ((1u << lane) - 1u));
         a.frag_xy[i] = (uint32_t)o.ix | ((uint32_t)o.iy << 16);
-        a.frag_z[i] = o.nz;
-        a.frag_col[i] = o.color;
+        a.frag_zc[i] = make_uint2(__float_as_uint(o.nz), o.color);
     }
 }
 
@@ -581,8 +579,7 @@ __device__ __forceinline__ void emit_fragments(const RasterArgs &a, uint32_t fba
         if (f[k].keep) {
             const uint32_t i = fbase + base + __popc(b[k] & lt);
             a.frag_xy[i] = f[k].xy;
-            a.frag_z[i] = f[k].z;
-            a.frag_col[i] = f[k].col;
+            a.frag_zc[i] = make_uint2(__float_as_uint(f[k].z), f[k].col);
         }
         base += __popc(b[k]);
     }
@@ -1028,8 +1025,12 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                     float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (q < nquads) {
                         xy4 = __ldcs(reinterpret_cast<const uint4 *>(a.frag_xy + base));
-                        z4 = __ldcs(reinterpret_cast<const float4 *>(a.frag_z + base));
-                        co4 = __ldcs(reinterpret_cast<const uint4 *>(a.frag_col + base));
+                        const uint4 zc01 = __ldcs(reinterpret_cast<const uint4 *>(a.frag_zc + base));
+                        const uint4 zc23 =
+                            __ldcs(reinterpret_cast<const uint4 *>(a.frag_zc + base + 2));
+                        z4 = make_float4(__uint_as_float(zc01.x), __uint_as_float(zc01.z),
+                                         __uint_as_float(zc23.x), __uint_as_float(zc23.z));
+                        co4 = make_uint4(zc01.y, zc01.w, zc23.y, zc23.w);
                     }
                     const uint32_t nv = q < nquads ? min(4u, nfrag - 4u * q) : 0u;
                     color_quad<MV>(a, vr, smem, c, tiled, nv, xy4, z4, co4);
@@ -1039,8 +1040,9 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                     const uint32_t l = l0 + threadIdx.x;
                     const bool v = l < nfrag;
                     const uint32_t i = fbase + (v ? l : 0u);
-                    do_fragment<MV>(a, vr, smem, c, tiled, v, v ? a.frag_xy[i] : 0u, v ? a.frag_z[i] : 0.f,
-                                v ? a.frag_col[i] : 0u);
+                    const uint2 zc = v ? a.frag_zc[i] : make_uint2(0u, 0u);
+                    do_fragment<MV>(a, vr, smem, c, tiled, v, v ? a.frag_xy[i] : 0u,
+                                    __uint_as_float(zc.x), zc.y);
                 }
             }
         } else if ((c.first & 3u) == 0u) {
@@ -1219,10 +1221,12 @@ __device__ __forceinline__ void hash_frags(const RasterArgs &a, const ViewRegsT<
     if ((base & 3u) == 0u) {
         for (uint32_t f = 4u * threadIdx.x; f < n; f += 4u * kThreads) {
             const uint4 xy = __ldcs(reinterpret_cast<const uint4 *>(a.frag_xy + base + f));
-            const float4 z = __ldcs(reinterpret_cast<const float4 *>(a.frag_z + base + f));
-            const uint4 co = __ldcs(reinterpret_cast<const uint4 *>(a.frag_col + base + f));
-            const uint32_t xs[4] = {xy.x, xy.y, xy.z, xy.w}, cs[4] = {co.x, co.y, co.z, co.w};
-            const float zs[4] = {z.x, z.y, z.z, z.w};
+            const uint4 zc01 = __ldcs(reinterpret_cast<const uint4 *>(a.frag_zc + base + f));
+            const uint4 zc23 = __ldcs(reinterpret_cast<const uint4 *>(a.frag_zc + base + f + 2));
+            const uint32_t xs[4] = {xy.x, xy.y, xy.z, xy.w},
+                           cs[4] = {zc01.y, zc01.w, zc23.y, zc23.w};
+            const float zs[4] = {__uint_as_float(zc01.x), __uint_as_float(zc01.z),
+                                 __uint_as_float(zc23.x), __uint_as_float(zc23.z)};
             uint32_t pix[4], cl[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -1239,8 +1243,9 @@ __device__ __forceinline__ void hash_frags(const RasterArgs &a, const ViewRegsT<
             const uint32_t xy = a.frag_xy[base + f];
             const uint32_t pix = (xy >> 16) * (uint32_t)W + (xy & 0xffffu);
             const uint32_t cl = __ldg(depth + pix);
-            if (cl != 0u && a.frag_z[base + f] >= crd::uint_to_depth(cl) * a.keep_scale)
-                hash_add<MV>(hkey, hsum, a, vr, pix, xy, a.frag_col[base + f], p3);
+            const uint2 zc = a.frag_zc[base + f];
+            if (cl != 0u && __uint_as_float(zc.x) >= crd::uint_to_depth(cl) * a.keep_scale)
+                hash_add<MV>(hkey, hsum, a, vr, pix, xy, zc.y, p3);
         }
     }
 }
@@ -1394,8 +1399,8 @@ __global__ void __launch_bounds__(kThreads, 6)
 // three; the re-run is rare and its speed does not matter.
 struct RedoCloud {
     const ChunkRec *chunks;
-    const uint32_t *counters, *frag_count, *frag_xy, *frag_col;
-    const float *frag_z;
+    const uint32_t *counters, *frag_count, *frag_xy;
+    const uint2 *frag_zc;
 };
 constexpr uint32_t kRedoMaxClouds = 32;
 struct RedoArgs {
@@ -1423,8 +1428,7 @@ __global__ void __launch_bounds__(kThreads) hqs_redo_kernel(RedoArgs r) {
         a.chunks = r.clouds[ci].chunks;
         a.frag_count = const_cast<uint32_t *>(r.clouds[ci].frag_count);
         a.frag_xy = const_cast<uint32_t *>(r.clouds[ci].frag_xy);
-        a.frag_z = const_cast<float *>(r.clouds[ci].frag_z);
-        a.frag_col = const_cast<uint32_t *>(r.clouds[ci].frag_col);
+        a.frag_zc = const_cast<uint2 *>(r.clouds[ci].frag_zc);
         const ViewRegsT<false> vr(a);
         const uint32_t nchunks = r.clouds[ci].counters[CNT_CHUNKS];
         for (uint32_t k = 0; k < nchunks; ++k) {
@@ -1543,8 +1547,7 @@ RasterArgs make_args(cr_cloud *cloud, const RasterUniforms &u, const RasterTarge
     a.radius_zero = fmaxf(u.minimumPointSize, u.maximumPointSize) <= 1.0f ? 1 : 0;
     a.use_tiles = cloud->ctx->use_tiles ? 1 : 0;
     a.frag_xy = cloud->d_frag_xy;
-    a.frag_z = cloud->d_frag_z;
-    a.frag_col = cloud->d_frag_col;
+    a.frag_zc = cloud->d_frag_zc;
     a.frag_count = cloud->d_frag_count;
     a.views = nullptr;
     a.nviews = 0;
@@ -1602,7 +1605,7 @@ cr_status launch_hqs_redo(cr_frame *f, cr_cloud *const *clouds, uint32_t nclouds
     r.a = make_args(clouds[0], u, t);
     for (uint32_t i = 0; i < nclouds; ++i)
         r.clouds[i] = RedoCloud{clouds[i]->d_chunks,   clouds[i]->d_counters, clouds[i]->d_frag_count,
-                                clouds[i]->d_frag_xy, clouds[i]->d_frag_col, clouds[i]->d_frag_z};
+                                clouds[i]->d_frag_xy, clouds[i]->d_frag_zc};
     r.nclouds = nclouds;
     r.redo = t.redo;
     r.rgba = f->d_rgba[0];
@@ -1670,8 +1673,7 @@ cr_status launch_raster_views(cr_cloud *cloud, RasterPass pass, const RasterUnif
     a.chunk_stride = chunk_stride;
     if (frags) {
         a.frag_xy = frags->xy;
-        a.frag_z = frags->z;
-        a.frag_col = frags->col;
+        a.frag_zc = frags->zc;
         a.frag_count = frags->count;
         a.chunk_poff = frags->poff;
         a.frag_cap = frags->cap;

@@ -69,8 +69,8 @@ struct ViewsCloud {
     uint32_t *counters = nullptr;         // nviews * CNT_COUNT
     uint32_t *chunk_poff = nullptr;       // nviews * chunk_stride
     uint32_t *frag_count = nullptr;       // nviews * chunk_stride
-    uint32_t *frag_xy = nullptr, *frag_col = nullptr;  // frag_cap each
-    float *frag_z = nullptr;
+    uint32_t *frag_xy = nullptr;  // frag_cap each
+    uint2 *frag_zc = nullptr;
     uint32_t *frag_overflow = nullptr;
     unsigned long long frag_cap = 0;
     uint32_t nslots = 0, ctas = 0, nfiles = 0;
@@ -126,8 +126,7 @@ void views_free(ViewsState *s) {
         dfree(c.chunk_poff);
         dfree(c.frag_count);
         dfree(c.frag_xy);
-        dfree(c.frag_z);
-        dfree(c.frag_col);
+        dfree(c.frag_zc);
         dfree(c.frag_overflow);
     }
     s->clouds.clear();
@@ -290,8 +289,7 @@ cr_status views_alloc(cr_context *ctx, ViewsState *s, cr_frame *const *frames, u
             const size_t slots = (size_t)nviews * vc.chunk_stride;
             if ((st = dalloc(&vc.chunk_poff, slots * 4)) || (st = dalloc(&vc.frag_count, slots * 4)) ||
                 (st = dalloc(&vc.frag_xy, vc.frag_cap * 4)) ||
-                (st = dalloc(&vc.frag_z, vc.frag_cap * 4)) ||
-                (st = dalloc(&vc.frag_col, vc.frag_cap * 4)) ||
+                (st = dalloc(&vc.frag_zc, vc.frag_cap * 8)) ||
                 (st = dalloc(&vc.frag_overflow, 16)))
                 return st;
             CR_CUDA(cudaMemsetAsync(vc.frag_overflow, 0, 16, ctx->stream));
@@ -337,8 +335,7 @@ cr_status views_enqueue(cr_context *ctx, ViewsState *s, int b, cr_cloud *const *
                 (size_t)v0 * vc.nfiles;
             const size_t slot0 = (size_t)v0 * vc.chunk_stride;
             const ViewsFragments fr{vc.frag_xy,
-                                    vc.frag_z,
-                                    vc.frag_col,
+                                    vc.frag_zc,
                                     vc.frag_count ? vc.frag_count + slot0 : nullptr,
                                     vc.chunk_poff ? vc.chunk_poff + slot0 : nullptr,
                                     vc.frag_cap,
