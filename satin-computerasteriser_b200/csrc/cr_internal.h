@@ -51,8 +51,9 @@ struct ViewsState;
 void views_destroy(ViewsState *s);
 
 // One survivor of the cull with the per-batch values the point passes need
-// (cull_classify output, 64 bytes).
-struct CullRec {
+// (cull_classify output, 64 bytes; 16-byte aligned so that it moves as four
+// 16-byte words).
+struct alignas(16) CullRec {
     cr_visible_batch vb;
     float minX, minY, minZ;  // batch min
     float qx, qy, qz;        // batchSize / steps of the survivor's precision level
@@ -62,8 +63,9 @@ struct CullRec {
 };
 
 // One unit of point-pass work: up to `chunkPoints` consecutive survivor points
-// of one batch (64 bytes, written by cull_compact in survivor order).
-struct ChunkRec {
+// of one batch (64 bytes, 16-byte aligned; written by the cull in survivor
+// order).
+struct alignas(16) ChunkRec {
     uint32_t first;  // absolute index of the chunk's first point
     uint32_t count;
     int32_t level;

@@ -44,8 +44,11 @@ __device__ __forceinline__ void screen_rect(const cr_raster_batch &b, const floa
         const crd::f4 clip = crd::mulp(T, (c & 1) ? b.maxX : b.minX, (c & 2) ? b.maxY : b.minY,
                                        (c & 4) ? b.maxZ : b.minZ);
         if (!(clip.w > 0.000001f) || !isfinite(clip.x) || !isfinite(clip.y)) front = false;
-        const float fx = (clip.x / clip.w * 0.5f + 0.5f) * (float)W;
-        const float fy = (clip.y / clip.w * 0.5f + 0.5f) * (float)H;
+        // Approximate quotients: the rectangle only decides which points
+        // take the shared-memory tile (the others take global atomics, with
+        // the same result), and its 2-pixel margin covers their error.
+        const float fx = (__fdividef(clip.x, clip.w) * 0.5f + 0.5f) * (float)W;
+        const float fy = (__fdividef(clip.y, clip.w) * 0.5f + 0.5f) * (float)H;
         xmin = fminf(xmin, fx);
         xmax = fmaxf(xmax, fx);
         ymin = fminf(ymin, fy);
@@ -340,6 +343,7 @@ __global__ void __launch_bounds__(kCullThreads)
     __shared__ uint32_t scan_c[kCullThreads / 32], scan_p[kCullThreads / 32];
     __shared__ CullRec s_rec[kCullThreads];
     __shared__ uint32_t s_cbase[kCullThreads];
+    __shared__ uint4 s_out[kCullThreads / 32][128];  // a warp's 32 chunk records
     __shared__ crd::FilePre s_pre[kInlineFiles];
     const uint32_t epoch = *(volatile const uint32_t *)(a.counters + CNT_CULL_EPOCH) + 1u;
     const uint32_t gid = ticket * kCullThreads + threadIdx.x;
@@ -443,35 +447,54 @@ __global__ void __launch_bounds__(kCullThreads)
                 a.chunk_poff[off_c + lbase + j] = pbase + j * round4(a.chunk_points);
     }
     __syncthreads();
-    for (uint32_t r = threadIdx.x; r < total_chunks; r += kCullThreads) {
-        uint32_t lo = 0, hi = total;  // survivors' first records ascend (each has one at least)
-        while (hi - lo > 1u) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_cbase[mid] <= r)
-                lo = mid;
-            else
-                hi = mid;
+    // A warp's 32 records go through shared memory so that they leave as
+    // contiguous 16-byte words (one record per lane would store 64-byte
+    // strided words).
+    uint4 *stage = s_out[warp];
+    uint4 *dst4 = reinterpret_cast<uint4 *>(a.chunks + off_c);
+    for (uint32_t r0 = 0; r0 < total_chunks; r0 += kCullThreads) {
+        const uint32_t r = r0 + threadIdx.x;
+        if (r < total_chunks) {
+            // The survivors' first records ascend (each has one at least).
+            uint32_t lo = 0, hi = total;
+            while (hi - lo > 1u) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (s_cbase[mid] <= r)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const CullRec &sr = s_rec[lo];
+            const uint32_t j = r - s_cbase[lo];
+            ChunkRec k;
+            k.first = sr.first + j * a.chunk_points;
+            k.count = min(a.chunk_points, sr.vb.activePoints - j * a.chunk_points);
+            k.level = sr.vb.level;
+            k.thr = sr.vb.lodThreshold;
+            k.batchIndex = sr.vb.batchIndex;
+            k.file = sr.file;
+            k.minX = sr.minX;
+            k.minY = sr.minY;
+            k.minZ = sr.minZ;
+            k.qx = sr.qx;
+            k.qy = sr.qy;
+            k.qz = sr.qz;
+            k.x0 = sr.x0;
+            k.y0 = sr.y0;
+            k.tw = sr.tw;
+            k.th = sr.th;
+            const uint4 *kv = reinterpret_cast<const uint4 *>(&k);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) stage[4 * lane + q] = kv[q];
         }
-        const CullRec &sr = s_rec[lo];
-        const uint32_t j = r - s_cbase[lo];
-        ChunkRec k;
-        k.first = sr.first + j * a.chunk_points;
-        k.count = min(a.chunk_points, sr.vb.activePoints - j * a.chunk_points);
-        k.level = sr.vb.level;
-        k.thr = sr.vb.lodThreshold;
-        k.batchIndex = sr.vb.batchIndex;
-        k.file = sr.file;
-        k.minX = sr.minX;
-        k.minY = sr.minY;
-        k.minZ = sr.minZ;
-        k.qx = sr.qx;
-        k.qy = sr.qy;
-        k.qz = sr.qz;
-        k.x0 = sr.x0;
-        k.y0 = sr.y0;
-        k.tw = sr.tw;
-        k.th = sr.th;
-        a.chunks[off_c + r] = k;
+        __syncwarp();
+        const uint32_t wrec = r0 + 32u * warp;  // the warp's first record
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const uint32_t w = 32u * m + lane;  // 16-byte word of the warp's records
+            if (wrec + w / 4u < total_chunks) dst4[4u * wrec + w] = stage[w];
+        }
+        __syncwarp();
     }
     if (ticket == cull_ctas - 1 && threadIdx.x == 0) {
         // cullFinalizeUpdate (CullFinalize/Shaders.metal:3-14): {count, 1, 1}.
