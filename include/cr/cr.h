@@ -439,6 +439,11 @@ CR_API cr_status cr_frame_read_nearest_index(cr_frame *frame, uint32_t *out /* w
 CR_API cr_status cr_frame_read_rgba8_async(cr_frame *frame, uint8_t *out /* w*h*4 */);
 /* Waits for the frame's enqueued asynchronous read-backs. */
 CR_API cr_status cr_frame_read_wait(cr_frame *frame);
+/* Waits until at most the `keep` most recent asynchronous read-backs of the
+ * frame may still be in flight (keep 0..3; 0 is cr_frame_read_wait), so that
+ * a render loop can use frame k's image while frame k+1's copy travels and
+ * frame k+2 renders.  No counterpart in the reference. */
+CR_API cr_status cr_frame_read_wait_keep(cr_frame *frame, int keep);
 /* Rows [row0, row0+nrows) of the nearest index plane (pick band read-back). */
 CR_API cr_status cr_frame_read_nearest_index_rows(cr_frame *frame, int row0, int nrows,
                                                   uint32_t *out);

@@ -784,9 +784,11 @@ class _Frame:
         self._pending.append(out)
         return out
 
-    def wait(self):
-        N.check(N.lib().cr_frame_read_wait(self._h))
-        self._pending.clear()
+    def wait(self, keep: int = 0):
+        """Waits until at most the `keep` most recent read-backs may still be
+        in flight (0: all done); the arrays of the finished ones are released."""
+        N.check(N.lib().cr_frame_read_wait_keep(self._h, int(keep)))
+        del self._pending[:len(self._pending) - int(keep) if keep else None]
 
     def depth_f32(self) -> np.ndarray:
         out = np.zeros((self.height, self.width), np.float32)
@@ -999,9 +1001,10 @@ class ComputeRasteriser:
         that reads every frame keeps the GPU busy while the images travel."""
         return self._require_frame().rgba8_async(out)
 
-    def waitOutput(self):
-        """Waits for every read-back enqueued by outputRGBA8Async."""
-        self._require_frame().wait()
+    def waitOutput(self, keep: int = 0):
+        """Waits for the read-backs enqueued by outputRGBA8Async: all of them,
+        or all but the `keep` (at most 3) most recent."""
+        self._require_frame().wait(keep)
 
     def depthTexture(self) -> np.ndarray:
         f = self._require_frame()

@@ -151,6 +151,7 @@ PROTOTYPES = {
     "cr_frame_read_rgba8": (C.c_int, [P, P]),
     "cr_frame_read_rgba8_async": (C.c_int, [P, P]),
     "cr_frame_read_wait": (C.c_int, [P]),
+    "cr_frame_read_wait_keep": (C.c_int, [P, C.c_int]),
     "cr_frame_read_depth_f32": (C.c_int, [P, P]),
     "cr_frame_read_pixels": (C.c_int, [P, P]),
     "cr_frame_read_nearest_depth": (C.c_int, [P, P]),

@@ -881,6 +881,8 @@ CR_API cr_status cr_frame_destroy(cr_frame *f) {
         cudaEventSynchronize(f->ev_copied);
         cudaEventDestroy(f->ev_copied);
     }
+    for (cudaEvent_t e : f->ev_copy_ring)
+        if (e) cudaEventDestroy(e);
     if (f->ev_rendered) cudaEventDestroy(f->ev_rendered);
     dfree(f->d_depth);
     dfree(f->d_accum);
@@ -1120,6 +1122,10 @@ CR_API cr_status cr_frame_read_rgba8_async(cr_frame *f, uint8_t *out) {
     CR_CUDA(cudaMemcpyAsync(out, f->d_rgba[f->final_rgba], (size_t)f->width * f->height * 4,
                             cudaMemcpyDeviceToHost, ctx->copy_stream));
     CR_CUDA(cudaEventRecord(f->ev_copied, ctx->copy_stream));
+    cudaEvent_t &slot = f->ev_copy_ring[f->copies % cr_frame::kCopyRing];
+    if (!slot) CR_CUDA(cudaEventCreateWithFlags(&slot, cudaEventDisableTiming));
+    CR_CUDA(cudaEventRecord(slot, ctx->copy_stream));
+    ++f->copies;
     f->copy_pending = true;
     return CR_OK;
 }
@@ -1129,6 +1135,21 @@ CR_API cr_status cr_frame_read_wait(cr_frame *f) {
     if (!f->ev_copied) return CR_OK;
     DeviceGuard g(f->ctx->device);
     CR_CUDA(cudaEventSynchronize(f->ev_copied));
+    return device_status(f->ctx);
+}
+
+CR_API cr_status cr_frame_read_wait_keep(cr_frame *f, int keep) {
+    if (!f) return fail(CR_ERR_INVALID_ARGUMENT, "frame is null");
+    if (keep < 0 || keep >= cr_frame::kCopyRing)
+        return fail(CR_ERR_INVALID_ARGUMENT,
+                    "keep must be 0.." + std::to_string(cr_frame::kCopyRing - 1));
+    if (keep == 0) return cr_frame_read_wait(f);
+    if (f->copies <= (uint64_t)keep) return CR_OK;
+    DeviceGuard g(f->ctx->device);
+    // The copy stream runs the read-backs in order: once read-back
+    // copies - 1 - keep has finished, every earlier one has too.
+    const uint64_t n = f->copies - 1 - (uint64_t)keep;
+    CR_CUDA(cudaEventSynchronize(f->ev_copy_ring[n % cr_frame::kCopyRing]));
     return device_status(f->ctx);
 }
 

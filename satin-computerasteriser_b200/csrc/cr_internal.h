@@ -231,6 +231,11 @@ struct cr_frame {
     // and waited on by the next write of the RGBA8 planes.
     cudaEvent_t ev_rendered = nullptr, ev_copied = nullptr;
     bool copy_pending = false;
+    // The last kCopyRing read-backs' completion events (copy n in slot
+    // n % kCopyRing) and the number of read-backs enqueued so far.
+    static constexpr int kCopyRing = 4;
+    cudaEvent_t ev_copy_ring[kCopyRing] = {};
+    uint64_t copies = 0;
 };
 
 // Asynchronous uploads: wait for and publish every upload in flight; free

@@ -67,8 +67,32 @@ def test_pipelined_readback_matches_blocking(cr, orc, ctx, hole_fill):
         ras.outputRGBA8Async(ring[k & 1].array)
     ras.waitOutput()
     assert np.array_equal(ring[(frames - 1) & 1].array, expect[-1])
+
+    # Three buffers, waiting only until frame k-2's copy is done (keep=1:
+    # frame k-1's may still travel) before enqueueing frame k's.
+    ring = bufs[:3]
+    for k in range(frames):
+        ras.update(camera(cr, k, w / h))
+        ras.encode()
+        ras.waitOutput(keep=1)
+        if k >= 2:
+            assert np.array_equal(ring[(k - 2) % 3].array, expect[k - 2]), f"ring3 frame {k - 2}"
+        ras.outputRGBA8Async(ring[k % 3].array)
+    ras.waitOutput()
+    for k in (frames - 2, frames - 1):
+        assert np.array_equal(ring[k % 3].array, expect[k]), f"ring3 frame {k}"
     for b in bufs:
         b.close()
+
+
+def test_wait_keep_is_validated(cr, ctx):
+    ras = cr.ComputeRasteriser(ctx)
+    ras.resize((64, 48))
+    ras.waitOutput(keep=3)  # nothing enqueued: returns at once
+    with pytest.raises(cr.CRError):
+        ras.waitOutput(keep=4)
+    with pytest.raises(cr.CRError):
+        ras.waitOutput(keep=-1)
 
 
 def test_readback_then_batched_views_render(cr, orc, ctx):
