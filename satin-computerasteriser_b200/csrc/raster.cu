@@ -1100,14 +1100,18 @@ __device__ __forceinline__ void raster_body(const RasterArgs &a) {
                         if (j % kB == kB - 1) emit_fragments<kB>(a, fbase, f);
                     }
                 } else {
-                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 0 < c.count, l0 + 0,
-                               lv4 & 0xffu, lo4.x, me4.x, hi4.x, co4.x, fbase, emit, all_keep);
-                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 1 < c.count, l0 + 1,
-                               (lv4 >> 8) & 0xffu, lo4.y, me4.y, hi4.y, co4.y, fbase, emit, all_keep);
-                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 2 < c.count, l0 + 2,
-                               (lv4 >> 16) & 0xffu, lo4.z, me4.z, hi4.z, co4.z, fbase, emit, all_keep);
-                do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 3 < c.count, l0 + 3,
-                               lv4 >> 24, lo4.w, me4.w, hi4.w, co4.w, fbase, emit, all_keep);
+                    do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 0 < c.count, l0 + 0,
+                                       lv4 & 0xffu, lo4.x, me4.x, hi4.x, co4.x, fbase, emit,
+                                       all_keep);
+                    do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 1 < c.count, l0 + 1,
+                                       (lv4 >> 8) & 0xffu, lo4.y, me4.y, hi4.y, co4.y, fbase,
+                                       emit, all_keep);
+                    do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 2 < c.count, l0 + 2,
+                                       (lv4 >> 16) & 0xffu, lo4.z, me4.z, hi4.z, co4.z, fbase,
+                                       emit, all_keep);
+                    do_point<PASS, MV>(a, vr, sb, smem, c, tiled, qv && l0 + 3 < c.count, l0 + 3,
+                                       lv4 >> 24, lo4.w, me4.w, hi4.w, co4.w, fbase, emit,
+                                       all_keep);
                 }
             }
         } else {
