@@ -248,6 +248,22 @@ public final class ComputeRasteriser {
         return out
     }
 
+    /// Enqueues the read-back of the frame's image into `out` (w*h*4 bytes,
+    /// page-locked memory keeps the copy asynchronous) and returns at once;
+    /// the copy overlaps the next encode() up to its resolve.  The caller
+    /// keeps `out` alive until waitOutput covers this read-back.
+    public func outputRGBA8Async(into out: UnsafeMutablePointer<UInt8>) throws {
+        guard let frame else { return }
+        try check(cr_frame_read_rgba8_async(frame, out))
+    }
+
+    /// Waits for the read-backs enqueued by outputRGBA8Async: all of them
+    /// (keep 0), or all but the `keep` (at most 3) most recent.
+    public func waitOutput(keep: Int = 0) throws {
+        guard let frame else { return }
+        try check(cr_frame_read_wait_keep(frame, Int32(keep)))
+    }
+
     /// pickPointIndex(atNDC:in:camera:searchRadius:): the global packed point
     /// index under ndc (y up), or nil.  Blocks until the GPU has finished.
     public func pickPointIndex(atNDC ndc: (Float, Float), in cloud: ComputeRasteriserPointCloud,
